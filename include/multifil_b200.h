@@ -1,0 +1,161 @@
+/*
+ * multifil_b200 -- C ABI of the B200 (sm_100a) half-sarcomere timestep engine.
+ *
+ * The reference (travistune3/multifil_jax) has no FFI: its seam is the Python
+ * call run(topology, duration_ms, dt, pCa, z_line, lattice_spacing, K_lat, nu,
+ * dynamic_params, static_params, replicates, rng_seed, ...) -> SimulationResult
+ * (multifil_jax/simulation.py:754-771), which dispatches the jitted
+ * _run_sim_kernel(topology, batched_params, z_batched, pCa_batched,
+ * ls_batched, rng_keys, dt, ..., n_cg_steps, n_newton_steps) -> 52 metrics of
+ * shape [batch, time] (simulation.py:584-747).  The entry points below replace
+ * that kernel; the Python package multifil_jax_b200 keeps the run() API on
+ * top of them through ctypes.
+ *
+ * Conventions
+ *   - Every function returns 0 on success or a negative MF_ERR_* code; the
+ *     message of the last failure on a context is mf_last_error(ctx).
+ *   - No exceptions cross this boundary; no device trap is ever raised.
+ *   - "device" pointers are CUDA device addresses owned by the caller; the
+ *     library never frees them.  "host" pointers are read during the call.
+ *   - A context is driven by one host thread at a time.  Several contexts
+ *     may coexist.  Outputs are valid once the given stream has synchronised.
+ */
+#ifndef MULTIFIL_B200_H
+#define MULTIFIL_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MF_ABI_VERSION 1
+
+/* error codes */
+#define MF_OK 0
+#define MF_ERR_INVALID (-1)   /* bad argument / shape */
+#define MF_ERR_CUDA (-2)      /* a CUDA runtime call failed */
+#define MF_ERR_NOMEM (-3)     /* device memory exhausted / admission refused */
+#define MF_ERR_NOTFOUND (-4)  /* unknown topology id or request id */
+#define MF_ERR_TIMEOUT (-5)   /* a bounded device wait gave up */
+#define MF_ERR_BUSY (-6)      /* request still running */
+
+/* per-condition status bits written to status_out */
+#define MF_STATUS_NONFINITE 1      /* a Newton update or residual was not finite */
+#define MF_STATUS_NOT_CONVERGED 2  /* residual above solver_residual_tol at some step */
+#define MF_STATUS_BOUNDS 4         /* an index was out of range (debug checks) */
+#define MF_STATUS_MULTIBIND 8      /* a site carried 3+ bound heads (sum order differs) */
+
+/* batch flags */
+#define MF_FLAG_DYNAMIC_LS 1       /* lattice spacing solved as an unknown (K_lat given) */
+#define MF_FLAG_PRECISE 2          /* displacement formulation + FP64 residual test/squaring */
+#define MF_FLAG_ORIGINAL_PRNG 4    /* pre-0.5 jax.random counter layout */
+#define MF_FLAG_PLAIN 8            /* one condition per launch, one launch per step */
+#define MF_FLAG_NO_GRAPH 16        /* batched path without CUDA-graph capture */
+
+#define MF_N_PARAMS 44
+#define MF_N_METRICS 52
+
+typedef struct mf_ctx mf_ctx;
+
+/* Lattice arrays as produced by SarcTopology.create
+ * (reference core/sarc_geometry.py:112-176, 379-645).  Host pointers. */
+typedef struct {
+    int32_t n_thick, n_crowns, n_thin, n_sites;
+    int32_t n_xb_per_crown, max_sites_per_face, n_xb_bins;
+    const int32_t* xb_to_thin_id;      /* [n_thick*n_crowns*n_xb_per_crown] */
+    const int32_t* xb_to_thin_face;    /* same */
+    const uint8_t* xb_valid;           /* same */
+    const int32_t* face_to_sites;      /* [n_thin*3*max_sites_per_face], -1 padded */
+    const int32_t* n_sites_per_face;   /* [n_thin*3] */
+    const int32_t* tm_prev_neighbor;   /* [n_thin*n_sites] */
+    const int32_t* tm_next_neighbor;   /* [n_thin*n_sites] */
+    const float* crown_offsets;        /* [n_thick*n_crowns] */
+    const float* crown_rests;          /* [n_thick*n_crowns] */
+    const float* binding_offsets;      /* [n_thin*n_sites] */
+    const float* binding_rests;        /* [n_thin*n_sites] */
+    const float* thin_rest_cumsum;     /* [n_thin*n_sites] cumsum(binding_rests) per filament */
+    const float* xb_bin_edges;         /* [n_xb_bins+1] */
+    const float* xb_bin_centers;       /* [n_xb_bins] */
+} mf_topo_desc;
+
+/* One batch of independent conditions (one row of the reference's vmap each). */
+typedef struct {
+    int32_t B;              /* number of conditions */
+    int32_t T_max;          /* row stride of the per-step arrays */
+    const int32_t* topo_id; /* [B] host: lattice of each condition (mf_upload_topology ids) */
+    const float* params;    /* [B*44] device: DynamicParams rows, reference field order */
+    const float* z;         /* [B*T_max] device: z_line trace */
+    const float* pCa;       /* [B*T_max] device */
+    const float* ls;        /* [B*T_max] device: lattice_spacing trace (driver / d_ref basis) */
+    const int32_t* n_steps; /* [B] device: steps of each condition (<= T_max) */
+    const uint32_t* keys;   /* [B*2] device: jax.random key of each condition */
+    const float* K_lat;     /* [B] device: lattice stiffness already x n_thick (dynamic LS) */
+    const float* nu;        /* [B] device: Poisson exponent (dynamic LS) */
+    const float* dt;        /* [B] device: timestep (ms) of each condition */
+    int32_t n_newton;       /* StaticParams.n_newton_steps (4) */
+    int32_t n_cg;           /* StaticParams.n_cg_steps (6) */
+    int32_t flags;          /* MF_FLAG_* */
+    int32_t chunk_steps;    /* steps per launch in the batched path (0 = all) */
+    float residual_warn;    /* StaticParams.solver_residual_tol (status bit only) */
+    float* metrics_out;     /* [B*52*T_max] device */
+    int32_t* status_out;    /* [B] device */
+    uint32_t* keys_out;     /* [B*2] device or NULL: key after the last step */
+    /* test hooks (NULL in production) */
+    const float* u_thin;    /* [B*T_max*n_sites_total] injected uniforms or NULL */
+    const float* u_xb;      /* [B*T_max*total_xbs] injected uniforms or NULL */
+    float* x_trace;         /* [B*T_max*max_dof] node positions after each step or NULL */
+    int8_t* state_trace;    /* [B*T_max*(max_xbs + max_sites)] xb then tm states or NULL */
+    int32_t* bound_trace;   /* [B*T_max*(max_xbs + max_sites)] xb then thin bound_to or NULL */
+} mf_batch;
+
+int mf_abi_version(void);
+int mf_create(int device, mf_ctx** out);
+int mf_destroy(mf_ctx* ctx);
+const char* mf_last_error(mf_ctx* ctx);
+
+/* Copy a lattice to the device; the library owns the copy until mf_destroy. */
+int mf_upload_topology(mf_ctx* ctx, const mf_topo_desc* desc, int32_t* topo_id);
+
+/* Run every condition of the batch to its n_steps.  Batched path: one CTA per
+ * condition, whole time loop resident in shared memory, launches of
+ * chunk_steps steps replayed from a captured CUDA graph.  With MF_FLAG_PLAIN:
+ * one condition per launch and one launch per step (the baseline form). */
+int mf_run_batch(mf_ctx* ctx, const mf_batch* batch, void* stream);
+
+/* Device bytes the library needs for a batch (admission control). */
+int mf_workspace_bytes(mf_ctx* ctx, const mf_batch* batch, uint64_t* bytes);
+
+/* jax.random on the host: key = PRNGKey(seed); keys_out[2*i..] = split(key, n)[i].
+ * partitionable=1: JAX >= 0.5 layout; 0: original layout. */
+int mf_prng_split(uint32_t k0, uint32_t k1, int32_t n, int32_t partitionable, uint32_t* keys_out);
+/* uniform(key, (n,)) float32 on the host (for tests of the device generator). */
+int mf_prng_uniform(uint32_t k0, uint32_t k1, int32_t n, int32_t partitionable, float* out);
+
+/* ---- continuous-batching server (serving form) ------------------------ */
+typedef struct {
+    int32_t topo_id;
+    int32_t n_steps;
+    float dt;
+    uint32_t key[2];
+    float params[MF_N_PARAMS];
+    float pCa, z_line, lattice_spacing;   /* constant drivers */
+} mf_request;
+
+/* Start a server on ctx with a device-memory budget (bytes) for resident
+ * slots and a chunk of steps per scheduling tick. */
+int mf_server_start(mf_ctx* ctx, uint64_t mem_budget, int32_t chunk_steps, int32_t max_slots);
+/* Queue a request; returns its id.  MF_ERR_NOMEM if it can never fit. */
+int mf_server_submit(mf_ctx* ctx, const mf_request* req, uint64_t* req_id);
+/* Run up to max_ticks scheduling ticks (admit, launch one chunk, retire). */
+int mf_server_step(mf_ctx* ctx, int32_t max_ticks, int32_t* n_active, int32_t* n_queued);
+/* Fetch a finished request's metrics (host [52*n_steps]); MF_ERR_BUSY if not done. */
+int mf_server_poll(mf_ctx* ctx, uint64_t req_id, float* metrics_host, int32_t* status, double* t_submit,
+                   double* t_done);
+int mf_server_cancel(mf_ctx* ctx, uint64_t req_id);
+int mf_server_stop(mf_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MULTIFIL_B200_H */

@@ -1,0 +1,509 @@
+// C ABI of the engine (include/multifil_b200.h): contexts, lattice upload,
+// batched / plain execution, host-side jax.random, and the serving loop.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/multifil_b200.h"
+#include "mf_kernel.cuh"
+
+using namespace mf;
+
+namespace {
+
+struct TopoHost {
+  TopoDev dev{};          // host copy with device pointers
+  TopoDev* d_struct = nullptr;
+  std::vector<void*> allocs;
+  size_t smem_local = 0;  // bytes with CG vectors in smem (at chosen NT)
+  int threads = 0;        // chosen CTA size
+  bool vec_global = false;
+};
+
+struct Request;
+
+struct Server;
+
+}  // namespace
+
+struct mf_ctx {
+  int device = 0;
+  std::string err;
+  std::vector<std::unique_ptr<TopoHost>> topos;
+  char* ws = nullptr;
+  size_t ws_bytes = 0;
+  CondDesc* d_cond = nullptr;
+  size_t cond_cap = 0;
+  int smem_optin = 0;
+  int num_sms = 0;
+  Server* server = nullptr;
+};
+
+static int fail(mf_ctx* c, int code, const char* fmt, ...) {
+  if (c) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    c->err = buf;
+  }
+  return code;
+}
+
+#define CK(call)                                                                        \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return fail(ctx, e_ == cudaErrorMemoryAllocation ? MF_ERR_NOMEM : MF_ERR_CUDA,     \
+                  "%s failed: %s", #call, cudaGetErrorString(e_));                      \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// kernel dispatch by CTA size
+// ---------------------------------------------------------------------------
+template <int NT>
+static cudaError_t launch_nt(const StepArgs& a, int grid, int base, size_t smem, cudaStream_t st) {
+  static bool attr_set = false;
+  static size_t attr_bytes = 0;
+  if (!attr_set || smem > attr_bytes) {
+    cudaError_t e = cudaFuncSetAttribute(step_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+    attr_bytes = smem;
+  }
+  step_kernel<NT><<<grid, NT, smem, st>>>(a, base);
+  return cudaGetLastError();
+}
+
+static cudaError_t launch(int nt, const StepArgs& a, int grid, int base, size_t smem, cudaStream_t st) {
+  switch (nt) {
+    case 128: return launch_nt<128>(a, grid, base, smem, st);
+    case 256: return launch_nt<256>(a, grid, base, smem, st);
+    case 512: return launch_nt<512>(a, grid, base, smem, st);
+    default: return launch_nt<1024>(a, grid, base, smem, st);
+  }
+}
+
+static int default_threads(const TopoDev& t) {
+  if (t.n_dof <= 1200) return 256;
+  if (t.n_dof <= 4000) return 512;
+  return 1024;
+}
+
+extern "C" {
+
+int mf_abi_version(void) { return MF_ABI_VERSION; }
+
+int mf_create(int device, mf_ctx** out) {
+  if (!out) return MF_ERR_INVALID;
+  mf_ctx* ctx = new mf_ctx();
+  ctx->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) {
+    *out = nullptr;
+    delete ctx;
+    return MF_ERR_CUDA;
+  }
+  cudaDeviceGetAttribute(&ctx->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+  *out = ctx;
+  return MF_OK;
+}
+
+int mf_server_stop(mf_ctx* ctx);
+
+int mf_destroy(mf_ctx* ctx) {
+  if (!ctx) return MF_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  if (ctx->server) mf_server_stop(ctx);
+  for (auto& t : ctx->topos) {
+    for (void* p : t->allocs) cudaFree(p);
+    if (t->d_struct) cudaFree(t->d_struct);
+  }
+  if (ctx->ws) cudaFree(ctx->ws);
+  if (ctx->d_cond) cudaFree(ctx->d_cond);
+  delete ctx;
+  return MF_OK;
+}
+
+const char* mf_last_error(mf_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int mf_upload_topology(mf_ctx* ctx, const mf_topo_desc* d, int32_t* topo_id) {
+  if (!ctx || !d || !topo_id) return fail(ctx, MF_ERR_INVALID, "null argument");
+  CK(cudaSetDevice(ctx->device));
+  const int nth = d->n_thick, ncr = d->n_crowns, nthin = d->n_thin, ns = d->n_sites;
+  const int nxb = d->n_xb_per_crown, width = d->max_sites_per_face, nb = d->n_xb_bins;
+  if (nth < 1 || ncr < 2 || nthin < 1 || ns < 2 || nxb < 1 || width < 1 || nb < 1)
+    return fail(ctx, MF_ERR_INVALID, "bad lattice sizes");
+  if (ncr > 128 || ns > 128) return fail(ctx, MF_ERR_INVALID, "filaments longer than 128 nodes");
+  const long X = (long)nth * ncr * nxb, S = (long)nthin * ns;
+  if (X > 32767 || S > 32767) return fail(ctx, MF_ERR_INVALID, "lattice too large for int16 indices");
+  auto t = std::make_unique<TopoHost>();
+  TopoDev& td = t->dev;
+  td.n_thick = nth; td.n_crowns = ncr; td.n_thin = nthin; td.n_sites = ns;
+  td.nxb = nxb; td.width = width; td.n_bins = nb;
+  td.total_xbs = (int)X; td.n_sites_total = (int)S; td.n_thick_nodes = nth * ncr;
+  td.n_dof = nth * ncr + (int)S;
+  td.plan_thick = make_scan_plan(ncr);
+  td.plan_thin = make_scan_plan(ns);
+  std::vector<int16_t> xb_face(X), face_sites((size_t)nthin * 3 * width), tm_prev(S), tm_next(S);
+  std::vector<uint8_t> valid(X), face_n(nthin * 3);
+  for (long i = 0; i < X; ++i) {
+    const int th = d->xb_to_thin_id[i], fc = d->xb_to_thin_face[i];
+    if (th < 0 || th >= nthin || fc < 0 || fc > 2) return fail(ctx, MF_ERR_INVALID, "bad xb target");
+    xb_face[i] = (int16_t)(th * 3 + fc);
+    valid[i] = d->xb_valid[i] ? 1 : 0;
+  }
+  for (int f = 0; f < nthin * 3; ++f) {
+    const int n = d->n_sites_per_face[f];
+    if (n < 0 || n > width) return fail(ctx, MF_ERR_INVALID, "bad face site count");
+    face_n[f] = (uint8_t)n;
+    const int first = n > 0 ? d->face_to_sites[(size_t)f * width] : 0;
+    for (int k = 0; k < width; ++k) {
+      int v = k < n ? d->face_to_sites[(size_t)f * width + k] : first;
+      if (v < 0 || v >= ns) return fail(ctx, MF_ERR_INVALID, "bad face site index");
+      face_sites[(size_t)f * width + k] = (int16_t)v;
+    }
+  }
+  for (long g = 0; g < S; ++g) {
+    const int p = d->tm_prev_neighbor[g], q = d->tm_next_neighbor[g];
+    if (p < 0 || p >= ns || q < 0 || q >= ns) return fail(ctx, MF_ERR_INVALID, "bad chain neighbour");
+    tm_prev[g] = (int16_t)p;
+    tm_next[g] = (int16_t)q;
+  }
+  std::vector<float> thick_c((size_t)nth * ncr), thin_c(S);
+  float cmin = INFINITY, cmax = -INFINITY;
+  for (int a = 0; a < nth; ++a)
+    for (int c = 0; c < ncr; ++c) {
+      const size_t i = (size_t)a * ncr + c;
+      const double prev = c > 0 ? (double)d->crown_offsets[i - 1] : 0.0;
+      thick_c[i] = (float)(((double)d->crown_offsets[i] - prev) - (double)d->crown_rests[i]);
+      cmin = std::min(cmin, d->crown_offsets[i]);
+      cmax = std::max(cmax, d->crown_offsets[i]);
+    }
+  for (int a = 0; a < nthin; ++a)
+    for (int j = 0; j < ns; ++j) {
+      const size_t g = (size_t)a * ns + j;
+      const double nxt = j + 1 < ns ? (double)d->binding_offsets[g + 1] : 0.0;
+      thin_c[g] = (float)(((double)d->binding_offsets[g] - nxt) - (double)d->binding_rests[g]);
+    }
+  td.crown_min = cmin;
+  td.crown_max = cmax;
+  auto up = [&](const void* src, size_t bytes, const void** dst) -> int {
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes < 16 ? 16 : bytes);
+    if (e != cudaSuccess) return fail(ctx, MF_ERR_NOMEM, "cudaMalloc(topology): %s", cudaGetErrorString(e));
+    t->allocs.push_back(p);
+    e = cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail(ctx, MF_ERR_CUDA, "cudaMemcpy(topology): %s", cudaGetErrorString(e));
+    *dst = p;
+    return 0;
+  };
+  int rc = 0;
+  rc |= up(xb_face.data(), X * 2, (const void**)&td.xb_face);
+  rc |= up(valid.data(), X, (const void**)&td.xb_valid);
+  rc |= up(face_sites.data(), face_sites.size() * 2, (const void**)&td.face_sites);
+  rc |= up(face_n.data(), face_n.size(), (const void**)&td.face_n);
+  rc |= up(tm_prev.data(), S * 2, (const void**)&td.tm_prev);
+  rc |= up(tm_next.data(), S * 2, (const void**)&td.tm_next);
+  rc |= up(d->crown_offsets, (size_t)nth * ncr * 4, (const void**)&td.crown_off);
+  rc |= up(d->crown_rests, (size_t)nth * ncr * 4, (const void**)&td.crown_rest);
+  rc |= up(d->binding_offsets, S * 4, (const void**)&td.bind_off);
+  rc |= up(d->binding_rests, S * 4, (const void**)&td.bind_rest);
+  rc |= up(d->thin_rest_cumsum, S * 4, (const void**)&td.thin_cum);
+  rc |= up(d->xb_bin_edges, (size_t)(nb + 1) * 4, (const void**)&td.edges);
+  rc |= up(d->xb_bin_centers, (size_t)nb * 4, (const void**)&td.centers);
+  rc |= up(thick_c.data(), thick_c.size() * 4, (const void**)&td.thick_c);
+  rc |= up(thin_c.data(), thin_c.size() * 4, (const void**)&td.thin_c);
+  if (rc) {
+    for (void* p : t->allocs) cudaFree(p);
+    return rc < 0 ? rc : MF_ERR_CUDA;
+  }
+  CK(cudaMalloc(&t->d_struct, sizeof(TopoDev)));
+  CK(cudaMemcpy(t->d_struct, &td, sizeof(TopoDev), cudaMemcpyHostToDevice));
+  t->threads = default_threads(td);
+  size_t sm = smem_bytes(td, t->threads, false);
+  t->vec_global = sm + 256 > (size_t)ctx->smem_optin;
+  t->smem_local = smem_bytes(td, t->threads, t->vec_global);
+  if (t->smem_local + 256 > (size_t)ctx->smem_optin)
+    return fail(ctx, MF_ERR_INVALID, "lattice needs %zu B shared memory (limit %d)", t->smem_local,
+                ctx->smem_optin);
+  ctx->topos.push_back(std::move(t));
+  *topo_id = (int32_t)ctx->topos.size() - 1;
+  return MF_OK;
+}
+
+// Choose the CTA size of a lattice (autotuner hook).  threads in {128,256,512,1024}.
+int mf_tune_threads(mf_ctx* ctx, int32_t topo_id, int32_t threads) {
+  if (!ctx || topo_id < 0 || topo_id >= (int)ctx->topos.size())
+    return fail(ctx, MF_ERR_NOTFOUND, "unknown topology");
+  if (threads != 128 && threads != 256 && threads != 512 && threads != 1024)
+    return fail(ctx, MF_ERR_INVALID, "threads must be 128, 256, 512 or 1024");
+  TopoHost& t = *ctx->topos[topo_id];
+  size_t sm = smem_bytes(t.dev, threads, false);
+  bool vg = sm > (size_t)ctx->smem_optin;
+  sm = smem_bytes(t.dev, threads, vg);
+  if (sm > (size_t)ctx->smem_optin) return fail(ctx, MF_ERR_INVALID, "does not fit");
+  t.threads = threads;
+  t.vec_global = vg;
+  t.smem_local = sm;
+  return MF_OK;
+}
+
+static size_t slot_bytes(const TopoDev& t) {
+  const CoefLayout cl = coef_layout(t);
+  return slot_layout(t.n_dof, t.total_xbs, t.n_sites_total, t.n_bins, cl.total).total;
+}
+
+int mf_workspace_bytes(mf_ctx* ctx, const mf_batch* bt, uint64_t* bytes) {
+  if (!ctx || !bt || !bytes) return fail(ctx, MF_ERR_INVALID, "null argument");
+  uint64_t tot = 0;
+  for (int i = 0; i < bt->B; ++i) {
+    const int id = bt->topo_id[i];
+    if (id < 0 || id >= (int)ctx->topos.size()) return fail(ctx, MF_ERR_NOTFOUND, "unknown topology %d", id);
+    tot += slot_bytes(ctx->topos[id]->dev);
+  }
+  *bytes = tot + sizeof(CondDesc) * (uint64_t)bt->B;
+  return MF_OK;
+}
+
+static int ensure_ws(mf_ctx* ctx, size_t bytes) {
+  if (bytes <= ctx->ws_bytes) return MF_OK;
+  if (ctx->ws) cudaFree(ctx->ws);
+  ctx->ws = nullptr;
+  ctx->ws_bytes = 0;
+  size_t want = std::max(bytes, ctx->ws_bytes * 3 / 2);
+  cudaError_t e = cudaMalloc(&ctx->ws, want);
+  if (e != cudaSuccess) {
+    e = cudaMalloc(&ctx->ws, bytes);
+    if (e != cudaSuccess) return fail(ctx, MF_ERR_NOMEM, "workspace of %zu B: %s", bytes, cudaGetErrorString(e));
+    want = bytes;
+  }
+  ctx->ws_bytes = want;
+  return MF_OK;
+}
+
+static int ensure_cond(mf_ctx* ctx, size_t n) {
+  if (n <= ctx->cond_cap) return MF_OK;
+  if (ctx->d_cond) cudaFree(ctx->d_cond);
+  ctx->d_cond = nullptr;
+  size_t cap = std::max(n, ctx->cond_cap * 2);
+  cudaError_t e = cudaMalloc(&ctx->d_cond, cap * sizeof(CondDesc));
+  if (e != cudaSuccess) return fail(ctx, MF_ERR_NOMEM, "condition table: %s", cudaGetErrorString(e));
+  ctx->cond_cap = cap;
+  return MF_OK;
+}
+
+static StepArgs make_args(const mf_batch* bt, const CondDesc* dc, int flags, int max_dof, int max_x,
+                          int max_s) {
+  StepArgs a{};
+  a.cond = dc;
+  a.T = bt->T_max;
+  a.n_newton = bt->n_newton;
+  a.n_cg = bt->n_cg;
+  a.flags = flags;
+  a.resid_warn = bt->residual_warn;
+  a.sq64_from = (flags & FLAG_PRECISE) ? 8 : 1 << 20;
+  a.u_thin = bt->u_thin;
+  a.u_xb = bt->u_xb;
+  a.x_trace = bt->x_trace;
+  a.st_trace = bt->state_trace;
+  a.bd_trace = bt->bound_trace;
+  a.max_dof = max_dof;
+  a.max_xbs = max_x;
+  a.max_sites = max_s;
+  return a;
+}
+
+int mf_run_batch(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
+  if (!ctx || !bt) return fail(ctx, MF_ERR_INVALID, "null argument");
+  if (bt->B < 0 || bt->T_max < 0) return fail(ctx, MF_ERR_INVALID, "negative batch shape");
+  if (bt->B == 0) return MF_OK;
+  if (!bt->topo_id || !bt->params || !bt->z || !bt->pCa || !bt->ls || !bt->n_steps || !bt->keys ||
+      !bt->metrics_out)
+    return fail(ctx, MF_ERR_INVALID, "missing required array");
+  if (bt->n_newton < 0 || bt->n_cg < 0) return fail(ctx, MF_ERR_INVALID, "negative solver caps");
+  if ((bt->flags & MF_FLAG_DYNAMIC_LS) && (!bt->K_lat || !bt->nu))
+    return fail(ctx, MF_ERR_INVALID, "dynamic lattice spacing needs K_lat and nu");
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t st = (cudaStream_t)stream_v;
+  const int B = bt->B;
+  // group conditions by CTA configuration; one launch per group
+  std::vector<int> n_steps(B);
+  std::vector<float> h_K(B, 0.f), h_nu(B, 0.f), h_dt(B, 1.0f);
+  CK(cudaMemcpy(n_steps.data(), bt->n_steps, sizeof(int) * B, cudaMemcpyDeviceToHost));
+  if (bt->K_lat) CK(cudaMemcpy(h_K.data(), bt->K_lat, sizeof(float) * B, cudaMemcpyDeviceToHost));
+  if (bt->nu) CK(cudaMemcpy(h_nu.data(), bt->nu, sizeof(float) * B, cudaMemcpyDeviceToHost));
+  if (bt->dt) CK(cudaMemcpy(h_dt.data(), bt->dt, sizeof(float) * B, cudaMemcpyDeviceToHost));
+  std::vector<CondDesc> hc(B);
+  size_t off = 0;
+  int max_dof = 0, max_x = 0, max_s = 0;
+  for (int i = 0; i < B; ++i) {
+    const int id = bt->topo_id[i];
+    if (id < 0 || id >= (int)ctx->topos.size()) return fail(ctx, MF_ERR_NOTFOUND, "unknown topology %d", id);
+    if (n_steps[i] < 0 || n_steps[i] > bt->T_max) return fail(ctx, MF_ERR_INVALID, "n_steps out of range");
+    const TopoDev& td = ctx->topos[id]->dev;
+    max_dof = std::max(max_dof, td.n_dof);
+    max_x = std::max(max_x, td.total_xbs);
+    max_s = std::max(max_s, td.n_sites_total);
+    off += slot_bytes(td);
+  }
+  int rc = ensure_ws(ctx, off);
+  if (rc) return rc;
+  // order: group by (threads, vec_global), longest work first inside a group
+  std::vector<int> order(B);
+  for (int i = 0; i < B; ++i) order[i] = i;
+  auto key_of = [&](int i) {
+    const TopoHost& t = *ctx->topos[bt->topo_id[i]];
+    return std::make_pair(t.threads * 2 + (t.vec_global ? 1 : 0), -(long)n_steps[i] * t.dev.n_dof);
+  };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key_of(a) < key_of(b); });
+  off = 0;
+  for (int k = 0; k < B; ++k) {
+    const int i = order[k];
+    const TopoHost& t = *ctx->topos[bt->topo_id[i]];
+    hc[k].topo = t.d_struct;
+    hc[k].ws = ctx->ws + off;
+    hc[k].n_steps = n_steps[i];
+    hc[k].index = i;
+    hc[k].T = bt->T_max;
+    hc[k].t0 = 0;
+    hc[k].t1 = n_steps[i];
+    hc[k].params = bt->params + (size_t)i * MF_N_PARAMS;
+    hc[k].z = bt->z + (size_t)i * bt->T_max;
+    hc[k].pCa = bt->pCa + (size_t)i * bt->T_max;
+    hc[k].ls = bt->ls + (size_t)i * bt->T_max;
+    hc[k].key = bt->keys + 2 * (size_t)i;
+    hc[k].metrics = bt->metrics_out + (size_t)i * MF_N_METRICS * bt->T_max;
+    hc[k].status = bt->status_out ? bt->status_out + i : nullptr;
+    hc[k].key_out = bt->keys_out ? bt->keys_out + 2 * (size_t)i : nullptr;
+    hc[k].K_lat = h_K[i];
+    hc[k].nu = h_nu[i];
+    hc[k].dt = h_dt[i];
+    off += slot_bytes(t.dev);
+  }
+  int base_flags = 0;
+  if (bt->flags & MF_FLAG_DYNAMIC_LS) base_flags |= FLAG_DYN;
+  if (bt->flags & MF_FLAG_PRECISE) base_flags |= FLAG_PRECISE;
+  if (bt->flags & MF_FLAG_ORIGINAL_PRNG) base_flags |= FLAG_ORIG_PRNG;
+  int T = 0;
+  for (int i = 0; i < B; ++i) T = std::max(T, n_steps[i]);
+  // groups
+  struct Group { int begin, end, threads; bool vg; size_t smem; };
+  std::vector<Group> groups;
+  for (int k = 0; k < B;) {
+    const TopoHost& t0 = *ctx->topos[bt->topo_id[order[k]]];
+    Group g{k, k, t0.threads, t0.vec_global, 0};
+    while (g.end < B) {
+      const TopoHost& tk = *ctx->topos[bt->topo_id[order[g.end]]];
+      if (tk.threads != g.threads || tk.vec_global != g.vg) break;
+      g.smem = std::max(g.smem, tk.smem_local);
+      ++g.end;
+    }
+    groups.push_back(g);
+    k = g.end;
+  }
+  const bool plain = (bt->flags & MF_FLAG_PLAIN) != 0;
+  if (plain) {
+    // One condition per launch, one launch per step: every step reloads the
+    // condition from its resident workspace and stores it back.  The step
+    // range of each launch is baked into its own descriptor row.
+    size_t n_rows = 0;
+    for (int k = 0; k < B; ++k) n_rows += (size_t)std::max(hc[k].n_steps, 1);
+    rc = ensure_cond(ctx, n_rows + B);
+    if (rc) return rc;
+    std::vector<CondDesc> rows;
+    rows.reserve(n_rows);
+    std::vector<std::pair<int, int>> launches;  // (row, group)
+    for (size_t gi = 0; gi < groups.size(); ++gi)
+      for (int k = groups[gi].begin; k < groups[gi].end; ++k)
+        for (int t = 0; t < std::max(hc[k].n_steps, 1); ++t) {
+          CondDesc c = hc[k];
+          c.t0 = t;
+          c.t1 = t + 1;
+          launches.emplace_back((int)rows.size(), (int)gi);
+          rows.push_back(c);
+        }
+    CK(cudaMemcpyAsync(ctx->d_cond, rows.data(), sizeof(CondDesc) * rows.size(), cudaMemcpyHostToDevice, st));
+    for (auto& lr : launches) {
+      const Group& g = groups[lr.second];
+      StepArgs a = make_args(bt, ctx->d_cond, base_flags | (g.vg ? 64 : 0), max_dof, max_x, max_s);
+      cudaError_t e = launch(g.threads, a, 1, lr.first, g.smem, st);
+      if (e != cudaSuccess) return fail(ctx, MF_ERR_CUDA, "plain launch: %s", cudaGetErrorString(e));
+    }
+    CK(cudaStreamSynchronize(st));  // the host staging vector dies here
+    return MF_OK;
+  }
+  const int chunk = bt->chunk_steps > 0 ? bt->chunk_steps : std::max(T, 1);
+  const int n_chunks = (std::max(T, 1) + chunk - 1) / chunk;
+  // one descriptor table per chunk (step ranges differ), uploaded once
+  rc = ensure_cond(ctx, (size_t)B * n_chunks);
+  if (rc) return rc;
+  std::vector<CondDesc> tab((size_t)B * n_chunks);
+  for (int c = 0; c < n_chunks; ++c)
+    for (int k = 0; k < B; ++k) {
+      CondDesc d = hc[k];
+      d.t0 = c * chunk;
+      d.t1 = std::min(c * chunk + chunk, d.n_steps);
+      tab[(size_t)c * B + k] = d;
+    }
+  CK(cudaMemcpyAsync(ctx->d_cond, tab.data(), sizeof(CondDesc) * tab.size(), cudaMemcpyHostToDevice, st));
+  const bool use_graph = !(bt->flags & MF_FLAG_NO_GRAPH) && n_chunks > 1;
+  cudaGraph_t graph = nullptr;
+  if (use_graph) CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  for (int c = 0; c < n_chunks; ++c) {
+    for (const Group& g : groups) {
+      StepArgs a = make_args(bt, ctx->d_cond + (size_t)c * B, base_flags | (g.vg ? 64 : 0), max_dof,
+                             max_x, max_s);
+      cudaError_t e = launch(g.threads, a, g.end - g.begin, g.begin, g.smem, st);
+      if (e != cudaSuccess) {
+        if (use_graph) {
+          cudaStreamEndCapture(st, &graph);
+          if (graph) cudaGraphDestroy(graph);
+        }
+        return fail(ctx, MF_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
+      }
+    }
+  }
+  if (use_graph) {
+    CK(cudaStreamEndCapture(st, &graph));
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(ctx, MF_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    e = cudaGraphLaunch(exec, st);
+    cudaGraphExecDestroy(exec);
+    if (e != cudaSuccess) return fail(ctx, MF_ERR_CUDA, "graph launch: %s", cudaGetErrorString(e));
+  }
+  CK(cudaStreamSynchronize(st));  // the host descriptor table dies here
+  return MF_OK;
+}
+
+int mf_prng_split(uint32_t k0, uint32_t k1, int32_t n, int32_t partitionable, uint32_t* out) {
+  if (n < 0 || (!out && n > 0)) return MF_ERR_INVALID;
+  for (int i = 0; i < n; ++i) {
+    if (partitionable) split_part(k0, k1, (uint32_t)i, out[2 * i], out[2 * i + 1]);
+    else split_orig(k0, k1, (uint32_t)n, (uint32_t)i, out[2 * i], out[2 * i + 1]);
+  }
+  return MF_OK;
+}
+
+int mf_prng_uniform(uint32_t k0, uint32_t k1, int32_t n, int32_t partitionable, float* out) {
+  if (n < 0 || (!out && n > 0)) return MF_ERR_INVALID;
+  for (int i = 0; i < n; ++i) out[i] = bits_to_uniform(bits32(partitionable != 0, k0, k1, (uint32_t)n, (uint32_t)i));
+  return MF_OK;
+}
+
+}  // extern "C"
+
+#include "mf_server.inc"

@@ -1,0 +1,505 @@
+// Kernel body: per-CTA set-up, the initial equilibrium, the step loop and the
+// fused metrics epilogue.  See mf_step.cuh for the per-phase device code.
+#pragma once
+#include "mf_step.cuh"
+
+namespace mf {
+
+// Shared-memory bytes needed by one condition of this lattice with NT threads.
+__host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, bool vec_global) {
+  const int N = t.n_dof, X = t.total_xbs, S = t.n_sites_total;
+  const int nw = nt / 32;
+  const int scan = t.plan_thin.total > t.plan_thick.total ? t.plan_thin.total : t.plan_thick.total;
+  const CoefLayout cl = coef_layout(t);
+  size_t o = 0;
+  auto add = [&](size_t bytes) { o = align_up(o + bytes, 16); };
+  add(sizeof(double) * 64);                // redd
+  add(sizeof(float) * 32 * 24);            // red
+  if (!vec_global) add(sizeof(float) * 5 * N);  // x r dx pv zz
+  add(sizeof(float) * 3 * X);              // fxb fdx xb_ax
+  add(sizeof(float) * S);                  // site / win1
+  add(sizeof(int) * S);                    // win2
+  add(sizeof(int16_t) * 2 * X);            // xb_bound xb_near
+  add(sizeof(int16_t) * S);                // thin_bound
+  add(X);                                  // xb_state
+  add(2 * S);                              // tm tm_new
+  add(sizeof(float) * 27 * 16);            // cum_tm
+  add(sizeof(float) * cl.total);           // coef
+  add(sizeof(float) * nw * scan);          // scan
+  add(sizeof(float) * kNParams);           // P
+  add(sizeof(float) * 4 * t.n_thick);      // tvec
+  return o;
+}
+
+template <int NT>
+__device__ void carve(Sim<NT>& m, char* base, bool vec_global) {
+  const TopoDev& t = m.T;
+  const int N = t.n_dof, X = t.total_xbs, S = t.n_sites_total;
+  const int scan = t.plan_thin.total > t.plan_thick.total ? t.plan_thin.total : t.plan_thick.total;
+  size_t o = 0;
+  auto take = [&](size_t bytes) { char* p = base + o; o = align_up(o + bytes, 16); return p; };
+  m.s.redd = (double*)take(sizeof(double) * 64);
+  m.s.red = (float*)take(sizeof(float) * 32 * 24);
+  float* v5 = vec_global ? reinterpret_cast<float*>(m.ws + m.L.vec) : (float*)take(sizeof(float) * 5 * N);
+  m.s.x = v5; m.s.r = v5 + N; m.s.dx = v5 + 2 * N; m.s.pv = v5 + 3 * N; m.s.zz = v5 + 4 * N;
+  float* v3 = (float*)take(sizeof(float) * 3 * X);
+  m.s.fxb = v3; m.s.fdx = v3 + X; m.s.xb_ax = v3 + 2 * X;
+  m.s.site = (float*)take(sizeof(float) * S);
+  m.s.win2 = (int*)take(sizeof(int) * S);
+  int16_t* i2 = (int16_t*)take(sizeof(int16_t) * 2 * X);
+  m.s.xb_bound = i2; m.s.xb_near = i2 + X;
+  m.s.thin_bound = (int16_t*)take(sizeof(int16_t) * S);
+  m.s.xb_state = (int8_t*)take(X);
+  int8_t* t2 = (int8_t*)take(2 * S);
+  m.s.tm = t2; m.s.tm_new = t2 + S;
+  m.s.cum_tm = (float*)take(sizeof(float) * 27 * 16);
+  m.s.coef = (float*)take(sizeof(float) * m.cl.total);
+  m.s.scan = (float*)take(sizeof(float) * NT / 32 * scan);
+  m.s.P = (float*)take(sizeof(float) * kNParams);
+  m.s.tvec = (float*)take(sizeof(float) * 4 * t.n_thick);
+}
+
+// ---------------------------------------------------------------------------
+// metrics epilogue (metrics_fn.py:154-417), written to metrics[b][k][t]
+// ---------------------------------------------------------------------------
+template <int NT>
+__device__ void metrics(Sim<NT>& m, int t, float zl, float pCa, float new_ls, float force,
+                        double resid, int iters, const float* old_x_thick, const int8_t* old_xb,
+                        const int8_t* old_tm_unused, const int16_t* old_near, const float* old_ax,
+                        const int8_t* old_tm, float* Mo) {
+  const TopoDev& T = m.T;
+  const int X = T.total_xbs, S = T.n_sites_total, NTN = T.n_thick_nodes;
+  const int tid = m.tid;
+  const float* pabs = reinterpret_cast<const float*>(m.ws + m.L.pabs);
+  // integer counts: 6 xb states, bound, 4 tm, overlap n/n2/n3, atp, newly
+  int ci[15] = {0};
+  float cf[4] = {0.f, 0.f, 0.f, 0.f};  // thick disp sum, thin disp sum, dx sum, atp_p
+  float tear = 0.f;
+  float tmin = INFINITY, tmax = -INFINITY, nmin = INFINITY, nmax = -INFINITY;
+  const float near_b = T.crown_min - 13.0f, far_b = T.crown_max + 13.0f;
+  for (int i = tid; i < X; i += NT) {
+    const int sn = m.s.xb_state[i], so = old_xb[i];
+    ci[sn] += 1;
+    ci[6] += (sn >= 1 && sn <= 3);
+    ci[13] += (so == 3) && (sn == 4 || sn == 0);
+    ci[14] += (so == 0) && (sn == 1);
+    if (so >= 2 && so <= 3) {
+      // P_abs on the pre-step geometry (metrics_fn.py:297-338)
+      const int thin = m.thin_of(i);
+      const int near = old_near[i];
+      const int site = near < 0 ? 0 : (near > T.n_sites - 1 ? T.n_sites - 1 : near);
+      const bool perm = (old_tm[thin * T.n_sites + site] == 3) && T.xb_valid[i];
+      const int key = (perm ? T.n_bins : 0) + m.bin_of(old_ax[i]);
+      if (so == 3) cf[3] += pabs[key * 3 + 0];
+      tear += pabs[key * 3 + (so == 2 ? 1 : 2)];
+    }
+  }
+  for (int g = tid; g < S; g += NT) {
+    const int st = m.s.tm[g];
+    ci[7 + st] += 1;
+    float xa;
+    if (!m.precise) xa = m.s.x[NTN + g];
+    else xa = (float)((m.zref - (double)T.bind_off[g]) + (double)m.s.x[NTN + g]);
+    const bool ov = xa >= near_b && xa <= far_b && xa > 0.0f;
+    ci[11] += ov;
+    ci[12] += ov && st == 2;
+    // n3 overlap stored after: reuse ci[14]? keep separate below
+  }
+  int c3o = 0;
+  for (int g = tid; g < S; g += NT) {
+    float xa;
+    if (!m.precise) xa = m.s.x[NTN + g];
+    else xa = (float)((m.zref - (double)T.bind_off[g]) + (double)m.s.x[NTN + g]);
+    const bool ov = xa >= near_b && xa <= far_b && xa > 0.0f;
+    c3o += ov && m.s.tm[g] == 3;
+  }
+  // displacements
+  for (int i = tid; i < NTN; i += NT) {
+    const float dsp = m.precise ? m.s.x[i] : m.s.x[i] - T.crown_off[i];
+    cf[0] += dsp;
+    tmin = fminf(tmin, dsp);
+    tmax = fmaxf(tmax, dsp);
+    cf[2] += m.s.x[i] - old_x_thick[i];
+  }
+  for (int g = tid; g < S; g += NT) {
+    float dsp;
+    if (!m.precise) dsp = m.s.x[NTN + g] - T.thin_cum[g];
+    else dsp = (float)((m.zref - (double)T.bind_off[g]) + (double)m.s.x[NTN + g] - (double)T.thin_cum[g]);
+    cf[1] += dsp;
+    nmin = fminf(nmin, dsp);
+    nmax = fmaxf(nmax, dsp);
+  }
+  int cnt[16];
+#pragma unroll
+  for (int k = 0; k < 15; ++k) cnt[k] = ci[k];
+  cnt[15] = c3o;
+  m.template bsum_ki<16>(cnt);
+  float sums[5] = {cf[0], cf[1], cf[2], cf[3], tear};
+  m.template bsum_k<5>(sums);
+  tmin = m.bmin(tmin);
+  tmax = m.bmax(tmax);
+  nmin = m.bmin(nmin);
+  nmax = m.bmax(nmax);
+  const float tmean = sums[0] / (float)NTN, nmean = sums[1] / (float)S;
+  float sq[2] = {0.f, 0.f};
+  for (int i = tid; i < NTN; i += NT) {
+    const float dsp = m.precise ? m.s.x[i] : m.s.x[i] - T.crown_off[i];
+    const float c = dsp - tmean;
+    sq[0] += c * c;
+  }
+  for (int g = tid; g < S; g += NT) {
+    float dsp;
+    if (!m.precise) dsp = m.s.x[NTN + g] - T.thin_cum[g];
+    else dsp = (float)((m.zref - (double)T.bind_off[g]) + (double)m.s.x[NTN + g] - (double)T.thin_cum[g]);
+    const float c = dsp - nmean;
+    sq[1] += c * c;
+  }
+  m.template bsum_k<2>(sq);
+  if (tid == 0) {
+    const float nx = (float)X, nt = (float)S;
+    const float* P = m.s.P;
+    auto put = [&](int k, float v) { Mo[(size_t)k * m.Tstride + t] = v; };
+    put(M_AXIAL_FORCE, force);
+    put(M_SOLVER_RESIDUAL, (float)resid);
+    put(M_Z_LINE, zl);
+    put(M_PCA, pCa);
+    put(M_LATTICE_SPACING, new_ls);
+    const float nb = (float)cnt[6];
+    put(M_N_BOUND, nb);
+    for (int k = 0; k < 6; ++k) put(M_N_XB_DRX + k, (float)cnt[k]);
+    put(M_FRAC_XB_BOUND, nb / nx);
+    for (int k = 0; k < 6; ++k) put(M_FRAC_XB_DRX + k, (float)cnt[k] / nx);
+    for (int k = 0; k < 4; ++k) put(M_N_TM_0 + k, (float)cnt[7 + k]);
+    for (int k = 0; k < 4; ++k) put(M_FRAC_TM_0 + k, (float)cnt[7 + k] / nt);
+    put(M_ACTIN_PERM, (float)cnt[10] / nt);
+    const float nov = (float)cnt[11];
+    const float n2 = (float)cnt[12], n3 = (float)cnt[15];
+    put(M_FRAC_TM_2_OV, n2 / nov);
+    put(M_FRAC_TM_3_OV, n3 / nov);
+    put(M_FRAC_TM_AVAIL_OV, (n2 + n3) / nov);
+    put(M_N_OVERLAP, nov);
+    put(M_ATP_CONSUMED, (float)cnt[13]);
+    put(M_NEWLY_BOUND, (float)cnt[14]);
+    put(M_THICK_D_MEAN, tmean);
+    put(M_THICK_D_MAX, tmax);
+    put(M_THICK_D_MIN, tmin);
+    put(M_THICK_D_STD, sqrtf(sq[0] / (float)NTN));
+    put(M_THIN_D_MEAN, nmean);
+    put(M_THIN_D_MAX, nmax);
+    put(M_THIN_D_MIN, nmin);
+    put(M_THIN_D_STD, sqrtf(sq[1] / (float)S));
+    // energies over thick filaments (sequential, small)
+    float e_new = 0.f, e_delta = 0.f, te_new = 0.f, te_delta = 0.f;
+    const float k = P[THICK_K];
+    for (int th = 0; th < T.n_thick; ++th) {
+      const int n0 = th * T.n_crowns;
+      const float u_new = m.precise ? m.s.x[n0] : m.s.x[n0] - T.crown_off[n0];
+      const float u_old = m.precise ? old_x_thick[n0] : old_x_thick[n0] - T.crown_off[n0];
+      const float en = 0.5f * k * (u_new * u_new);
+      const float eo = 0.5f * k * (u_old * u_old);
+      e_new += en;
+      e_delta += en - eo;
+      const int nl = n0 + T.n_crowns - 1;
+      float ad_new, ad_old;
+      if (!m.precise) {
+        ad_new = zl - m.s.x[nl];
+        ad_old = zl - old_x_thick[nl];
+      } else {
+        const float zc = (float)((double)zl - (double)T.crown_off[nl]);
+        ad_new = zc - m.s.x[nl];
+        ad_old = zc - old_x_thick[nl];
+      }
+      const float a = P[TITIN_A], bb = P[TITIN_B], r0 = P[TITIN_REST];
+      const float Ln = sqrtf(ad_new * ad_new + new_ls * new_ls);
+      const float Lo = sqrtf(ad_old * ad_old + new_ls * new_ls);
+      const float tn = (a / bb) * (expf(bb * (Ln - r0)) - 1.0f);
+      const float to = (a / bb) * (expf(bb * (Lo - r0)) - 1.0f);
+      te_new += tn;
+      te_delta += tn - to;
+    }
+    const float fth = (float)T.n_thick;
+    put(M_THICK_E_AVG, e_new / fth);
+    put(M_THICK_E_DELTA, e_delta / fth);
+    put(M_TITIN_E_AVG, te_new / fth);
+    put(M_TITIN_E_DELTA, te_delta / fth);
+    const float work = force * (sums[2] / (float)NTN);
+    put(M_WORK_THICK, work);
+    put(M_WORK_THICK_MEAN, work / (float)NTN);
+    put(M_ATP_EXPECTED_P, sums[3]);
+    put(M_XB_TEAR, sums[4]);
+    put(M_WORK_PER_ATP, sums[3] > 0.01f ? work / sums[3] : 0.0f);
+    put(M_NEWTON_ITERS, (float)iters);
+  }
+  (void)old_tm_unused;
+}
+
+// ---------------------------------------------------------------------------
+// one CTA = one condition, steps [t_begin, t_end)
+// ---------------------------------------------------------------------------
+template <int NT>
+__device__ void run_condition(const StepArgs& A, int ci) {
+  extern __shared__ __align__(16) char smem_raw[];
+  const CondDesc cd = A.cond[ci];
+  const TopoDev& T = *cd.topo;
+  Sim<NT> m(T, A);
+  m.tid = threadIdx.x;
+  m.lane = m.tid & 31;
+  m.warp = m.tid >> 5;
+  m.b = cd.index;
+  m.ws = cd.ws;
+  m.cl = coef_layout(T);
+  m.L = slot_layout(T.n_dof, T.total_xbs, T.n_sites_total, T.n_bins, m.cl.total);
+  m.dyn = (A.flags & FLAG_DYN) != 0;
+  m.precise = (A.flags & FLAG_PRECISE) != 0;
+  m.part = (A.flags & FLAG_ORIG_PRNG) == 0;
+  m.status = 0;
+  m.Tstride = cd.T;
+  carve(m, smem_raw, (A.flags & 64) != 0);
+  const int b = m.b;
+  const int N = T.n_dof, X = T.total_xbs, S = T.n_sites_total, NTN = T.n_thick_nodes;
+  double* misc = reinterpret_cast<double*>(m.ws + m.L.misc);
+  float* xg = reinterpret_cast<float*>(m.ws + m.L.x);
+  int8_t* xbs_g = reinterpret_cast<int8_t*>(m.ws + m.L.xb_state);
+  int16_t* xbb_g = reinterpret_cast<int16_t*>(m.ws + m.L.xb_bound);
+  int16_t* xbn_g = reinterpret_cast<int16_t*>(m.ws + m.L.xb_near);
+  float* xba_g = reinterpret_cast<float*>(m.ws + m.L.xb_ax);
+  int8_t* tm_g = reinterpret_cast<int8_t*>(m.ws + m.L.tm);
+  int16_t* tb_g = reinterpret_cast<int16_t*>(m.ws + m.L.thin_bound);
+  float* cum_tm_g = reinterpret_cast<float*>(m.ws + m.L.cum_tm);
+  float* coef_g = reinterpret_cast<float*>(m.ws + m.L.coef);
+
+  for (int i = m.tid; i < kNParams; i += NT) m.s.P[i] = cd.params[i];
+  m.Kl = cd.K_lat;
+  m.nu_c = cd.nu;
+  m.dtm = cd.dt;
+  const float* zt = cd.z;
+  const float* pt = cd.pCa;
+  const float* lt = cd.ls;
+  const int n_steps = cd.n_steps;
+  const int t0 = cd.t0;
+  const int t1 = cd.t1 < n_steps ? cd.t1 : n_steps;
+  if (t0 >= t1 && t0 > 0) return;
+  __syncthreads();
+
+  __shared__ uint32_t key_s[2];
+  __shared__ float ls_s;
+  if (t0 == 0) {
+    // ---- realize_state + initial equilibrium with the constants (A1) ----
+    m.zref = (double)zt[0];
+    for (int i = m.tid; i < N; i += NT) {
+      if (i < NTN) m.s.x[i] = m.precise ? 0.f : T.crown_off[i];
+      else m.s.x[i] = m.precise ? 0.f : zt[0] - T.bind_off[i - NTN];
+    }
+    for (int i = m.tid; i < X; i += NT) {
+      m.s.xb_state[i] = 0;
+      m.s.xb_bound[i] = -1;
+    }
+    for (int g = m.tid; g < S; g += NT) {
+      m.s.tm[g] = 0;
+      m.s.thin_bound[g] = -1;
+    }
+    m.build_precond_coef(coef_g);
+    __syncthreads();
+    __threadfence_block();
+    for (int i = m.tid; i < m.cl.total; i += NT) m.s.coef[i] = coef_g[i];
+    __syncthreads();
+    m.nearest(m.s.P[LATTICE_SPACING]);
+    __syncthreads();
+    double resid;
+    int it;
+    float d0 = m.s.P[LATTICE_SPACING];
+    const bool dyn_save = m.dyn;
+    m.dyn = false;
+    m.solve(m.s.P[Z_LINE], d0, resid, it, 0.f);
+    m.dyn = dyn_save;
+    if (m.tid == 0) {
+      key_s[0] = cd.key[0];
+      key_s[1] = cd.key[1];
+      ls_s = lt[0];
+      misc[MS_TAB_PCA] = NAN;
+      misc[MS_TAB_D] = NAN;
+      misc[MS_ABS_PCA] = NAN;
+      misc[MS_ABS_D] = NAN;
+      misc[MS_L0] = (double)zt[0];
+    }
+    __syncthreads();
+  } else {
+    // ---- resume a condition from its resident workspace ----
+    m.zref = misc[MS_ZREF];
+    for (int i = m.tid; i < N; i += NT) m.s.x[i] = xg[i];
+    for (int i = m.tid; i < X; i += NT) {
+      m.s.xb_state[i] = xbs_g[i];
+      m.s.xb_bound[i] = xbb_g[i];
+      m.s.xb_near[i] = xbn_g[i];
+      m.s.xb_ax[i] = xba_g[i];
+    }
+    for (int g = m.tid; g < S; g += NT) {
+      m.s.tm[g] = tm_g[g];
+      m.s.thin_bound[g] = tb_g[g];
+    }
+    for (int i = m.tid; i < m.cl.total; i += NT) m.s.coef[i] = coef_g[i];
+    for (int i = m.tid; i < 27 * 16; i += NT) m.s.cum_tm[i] = cum_tm_g[i];
+    if (m.tid == 0) {
+      const uint32_t* kk = reinterpret_cast<const uint32_t*>(misc + MS_KEY);
+      key_s[0] = kk[0];
+      key_s[1] = kk[1];
+      ls_s = (float)misc[MS_CUR_LS];
+      m.status = (int)misc[MS_STATUS];
+    }
+    __syncthreads();
+  }
+
+  // pre-step snapshot buffers live in global workspace is avoided: keep the
+  // old thick positions / states in the spare CG vectors between phases
+  float* Mo = cd.metrics;
+  for (int t = t0; t < t1; ++t) {
+    const float zl = zt[t], pCa = pt[t], ls_t = lt[t];
+    const float dz = t > 0 ? zt[t] - zt[t - 1] : 0.0f;
+    // 1. rigid shift of the thin filaments
+    if (!m.precise) {
+      for (int i = NTN + m.tid; i < N; i += NT) m.s.x[i] = m.s.x[i] + dz;
+    } else {
+      m.zref = (double)zl;
+    }
+    const float cur_ls = ls_s;
+    float d_kin;
+    if (m.dyn) {
+      d_kin = cur_ls;
+      const float l0 = (float)misc[MS_L0];
+      m.d_ref = ls_t * powf(l0 / zl, m.nu_c);
+    } else {
+      d_kin = ls_t;
+    }
+    // probability tables for (pCa, d_kin)
+    if (!((double)pCa == misc[MS_TAB_PCA] && (double)d_kin == misc[MS_TAB_D])) {
+      __syncthreads();
+      m.build_tables(pCa, d_kin, true, false);
+      __syncthreads();
+      if (m.tid == 0) { misc[MS_TAB_PCA] = pCa; misc[MS_TAB_D] = d_kin; }
+      __threadfence_block();
+      __syncthreads();
+    }
+    // old_state snapshot for the metrics (metrics_fn.py reads the pre-step
+    // geometry): parked in the resident workspace arrays, which are only
+    // rewritten with the live state at the end of the launch.
+    for (int i = m.tid; i < NTN; i += NT) xg[i] = m.s.x[i];
+    for (int i = m.tid; i < X; i += NT) {
+      xbs_g[i] = m.s.xb_state[i];
+      xbn_g[i] = m.s.xb_near[i];
+      xba_g[i] = m.s.xb_ax[i];
+    }
+    for (int g = m.tid; g < S; g += NT) tm_g[g] = m.s.tm[g];
+    __syncthreads();
+    // 2-4. kinetics
+    __shared__ uint32_t sub_thin[2], sub_thick[2];
+    if (m.tid == 0) {
+      uint32_t kn[2];
+      step_keys(m.part, key_s[0], key_s[1], sub_thin, sub_thick, kn);
+      key_s[0] = kn[0];
+      key_s[1] = kn[1];
+    }
+    m.nearest(d_kin);
+    __syncthreads();
+    const size_t inj_t = ((size_t)b * A.T + t) * (size_t)S;
+    const size_t inj_x = ((size_t)b * A.T + t) * (size_t)X;
+    m.thin_step(sub_thin, inj_t);
+    m.thick_step(sub_thick, inj_x);
+    // 5. mechanics
+    double resid;
+    int iters;
+    float d = m.dyn ? cur_ls : ls_t;
+    float jdd_inv = 0.f;
+    if (m.dyn) {
+      // exact radial diagonal at the pre-solve point (solver.py:633-638)
+      float frad;
+      m.residual(zl, d, &frad);
+      float part = 0.f;
+      for (int i = m.tid; i < X; i += NT) {
+        float f, fx, fd, frd, fr;
+        m.xb_force(i, d, f, fx, fd, frd, fr);
+        part += frd;
+      }
+      if (m.tid < T.n_thick) part += m.s.tvec[3 * T.n_thick + m.tid];
+      const float ssum = m.bsum(part);
+      const float Jdd = -m.Kl - ssum;
+      jdd_inv = -1.0f / Jdd;
+    }
+    m.solve(zl, d, resid, iters, jdd_inv);
+    const float new_ls = m.dyn ? d : ls_t;
+    if (m.tid == 0) ls_s = new_ls;
+    // absorbing table for the metrics at (pCa, new_ls)
+    if (!((double)pCa == misc[MS_ABS_PCA] && (double)new_ls == misc[MS_ABS_D])) {
+      __syncthreads();
+      m.build_tables(pCa, new_ls, false, true);
+      __syncthreads();
+      if (m.tid == 0) { misc[MS_ABS_PCA] = pCa; misc[MS_ABS_D] = new_ls; }
+      __threadfence_block();
+    }
+    __syncthreads();
+    // 6. force + metrics
+    float force = 0.f;
+    if (m.tid == 0) {
+      for (int th = 0; th < T.n_thick; ++th) {
+        const int n0 = th * T.n_crowns;
+        const float u = m.precise ? m.s.x[n0] : m.s.x[n0] - T.crown_off[n0];
+        force += u * m.s.P[THICK_K];
+      }
+      m.s.red[32 * 24 - 1] = force;
+    }
+    __syncthreads();
+    force = m.s.red[32 * 24 - 1];
+    __syncthreads();
+    metrics(m, t, zl, pCa, new_ls, force, resid, iters, xg, xbs_g, nullptr, xbn_g, xba_g, tm_g, Mo);
+    if (resid > (double)A.resid_warn) m.status |= 2;
+    // optional traces
+    if (A.x_trace) {
+      float* xt = A.x_trace + ((size_t)b * A.T + t) * A.max_dof;
+      for (int i = m.tid; i < N; i += NT) {
+        float v = m.s.x[i];
+        if (m.precise) {
+          v = i < NTN ? (float)((double)T.crown_off[i] + (double)v)
+                      : (float)((m.zref - (double)T.bind_off[i - NTN]) + (double)v);
+        }
+        xt[i] = v;
+      }
+    }
+    if (A.st_trace) {
+      int8_t* st = A.st_trace + ((size_t)b * A.T + t) * (A.max_xbs + A.max_sites);
+      int* bt = A.bd_trace + ((size_t)b * A.T + t) * (A.max_xbs + A.max_sites);
+      for (int i = m.tid; i < X; i += NT) { st[i] = m.s.xb_state[i]; bt[i] = m.s.xb_bound[i]; }
+      for (int g = m.tid; g < S; g += NT) { st[A.max_xbs + g] = m.s.tm[g]; bt[A.max_xbs + g] = m.s.thin_bound[g]; }
+    }
+    __syncthreads();
+  }
+  // ---- write back resident state ----
+  for (int i = m.tid; i < N; i += NT) xg[i] = m.s.x[i];
+  for (int i = m.tid; i < X; i += NT) {
+    xbs_g[i] = m.s.xb_state[i];
+    xbb_g[i] = m.s.xb_bound[i];
+    xbn_g[i] = m.s.xb_near[i];
+    xba_g[i] = m.s.xb_ax[i];
+  }
+  for (int g = m.tid; g < S; g += NT) {
+    tm_g[g] = m.s.tm[g];
+    tb_g[g] = m.s.thin_bound[g];
+  }
+  for (int i = m.tid; i < 27 * 16; i += NT) cum_tm_g[i] = m.s.cum_tm[i];
+  const int st_all = __syncthreads_or(m.status);
+  if (m.tid == 0) {
+    uint32_t* kk = reinterpret_cast<uint32_t*>(misc + MS_KEY);
+    kk[0] = key_s[0];
+    kk[1] = key_s[1];
+    misc[MS_CUR_LS] = ls_s;
+    misc[MS_ZREF] = m.zref;
+    misc[MS_STATUS] = (double)(m.status | st_all);
+    if (cd.status) *cd.status = m.status | st_all;
+    if (cd.key_out) { cd.key_out[0] = key_s[0]; cd.key_out[1] = key_s[1]; }
+  }
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) step_kernel(StepArgs A, int cond_base) {
+  run_condition<NT>(A, cond_base + blockIdx.x);
+}
+
+}  // namespace mf

@@ -1,0 +1,311 @@
+"""ctypes binding of ``libmultifil_b200.so`` and the device-side batch runner.
+
+PyTorch provides device memory and streams; the timestep itself runs in the
+hand-written sm_100a kernels behind the C ABI declared in
+``include/multifil_b200.h``.  There is no CPU fallback: when the shared library
+or a CUDA device is missing every entry point raises :class:`EngineError`.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+from dataclasses import dataclass
+from typing import Dict, Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.environ.get('MULTIFIL_B200_LIB', os.path.join(_HERE, 'libmultifil_b200.so'))
+
+MF_FLAG_DYNAMIC_LS = 1
+MF_FLAG_PRECISE = 2
+MF_FLAG_ORIGINAL_PRNG = 4
+MF_FLAG_PLAIN = 8
+MF_FLAG_NO_GRAPH = 16
+
+MF_STATUS_NONFINITE = 1
+MF_STATUS_NOT_CONVERGED = 2
+
+MF_ERR_BUSY = -6
+MF_ERR_NOMEM = -3
+
+N_METRICS = 52
+N_PARAMS = 44
+
+
+class EngineError(RuntimeError):
+    """The CUDA engine is unavailable or a call through the C ABI failed."""
+
+
+class mf_topo_desc(ctypes.Structure):
+    _fields_ = [
+        ('n_thick', ctypes.c_int32), ('n_crowns', ctypes.c_int32), ('n_thin', ctypes.c_int32),
+        ('n_sites', ctypes.c_int32), ('n_xb_per_crown', ctypes.c_int32),
+        ('max_sites_per_face', ctypes.c_int32), ('n_xb_bins', ctypes.c_int32),
+        ('xb_to_thin_id', ctypes.c_void_p), ('xb_to_thin_face', ctypes.c_void_p),
+        ('xb_valid', ctypes.c_void_p), ('face_to_sites', ctypes.c_void_p),
+        ('n_sites_per_face', ctypes.c_void_p), ('tm_prev_neighbor', ctypes.c_void_p),
+        ('tm_next_neighbor', ctypes.c_void_p), ('crown_offsets', ctypes.c_void_p),
+        ('crown_rests', ctypes.c_void_p), ('binding_offsets', ctypes.c_void_p),
+        ('binding_rests', ctypes.c_void_p), ('thin_rest_cumsum', ctypes.c_void_p),
+        ('xb_bin_edges', ctypes.c_void_p), ('xb_bin_centers', ctypes.c_void_p),
+    ]
+
+
+class mf_batch(ctypes.Structure):
+    _fields_ = [
+        ('B', ctypes.c_int32), ('T_max', ctypes.c_int32), ('topo_id', ctypes.c_void_p),
+        ('params', ctypes.c_void_p), ('z', ctypes.c_void_p), ('pCa', ctypes.c_void_p),
+        ('ls', ctypes.c_void_p), ('n_steps', ctypes.c_void_p), ('keys', ctypes.c_void_p),
+        ('K_lat', ctypes.c_void_p), ('nu', ctypes.c_void_p), ('dt', ctypes.c_void_p),
+        ('n_newton', ctypes.c_int32), ('n_cg', ctypes.c_int32), ('flags', ctypes.c_int32),
+        ('chunk_steps', ctypes.c_int32), ('residual_warn', ctypes.c_float),
+        ('metrics_out', ctypes.c_void_p), ('status_out', ctypes.c_void_p),
+        ('keys_out', ctypes.c_void_p), ('u_thin', ctypes.c_void_p), ('u_xb', ctypes.c_void_p),
+        ('x_trace', ctypes.c_void_p), ('state_trace', ctypes.c_void_p),
+        ('bound_trace', ctypes.c_void_p),
+    ]
+
+
+class mf_request(ctypes.Structure):
+    _fields_ = [
+        ('topo_id', ctypes.c_int32), ('n_steps', ctypes.c_int32), ('dt', ctypes.c_float),
+        ('key', ctypes.c_uint32 * 2), ('params', ctypes.c_float * N_PARAMS),
+        ('pCa', ctypes.c_float), ('z_line', ctypes.c_float), ('lattice_spacing', ctypes.c_float),
+    ]
+
+
+# exported symbol -> (restype, argtypes)
+_SIGNATURES = {
+    'mf_abi_version': (ctypes.c_int, []),
+    'mf_create': (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    'mf_destroy': (ctypes.c_int, [ctypes.c_void_p]),
+    'mf_last_error': (ctypes.c_char_p, [ctypes.c_void_p]),
+    'mf_upload_topology': (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(mf_topo_desc),
+                                          ctypes.POINTER(ctypes.c_int32)]),
+    'mf_tune_threads': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]),
+    'mf_run_batch': (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(mf_batch), ctypes.c_void_p]),
+    'mf_workspace_bytes': (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(mf_batch),
+                                          ctypes.POINTER(ctypes.c_uint64)]),
+    'mf_prng_split': (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32,
+                                     ctypes.c_void_p]),
+    'mf_prng_uniform': (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32,
+                                       ctypes.c_void_p]),
+    'mf_server_start': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int32, ctypes.c_int32]),
+    'mf_server_submit': (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(mf_request),
+                                        ctypes.POINTER(ctypes.c_uint64)]),
+    'mf_server_step': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                                      ctypes.POINTER(ctypes.c_int32)]),
+    'mf_server_poll': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                      ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double),
+                                      ctypes.POINTER(ctypes.c_double)]),
+    'mf_server_cancel': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    'mf_server_stop': (ctypes.c_int, [ctypes.c_void_p]),
+}
+
+_lib = None
+_lib_lock = threading.Lock()
+
+
+def load_library(path: str = LIB_PATH):
+    """Load the shared library (no GPU needed) and bind every exported symbol."""
+    global _lib
+    with _lib_lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(path):
+            raise EngineError(f"CUDA engine library not found at {path}; run __graft_entry__.build()")
+        lib = ctypes.CDLL(path)
+        for name, (res, args) in _SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def prng_split(key, n: int, partitionable: bool = True) -> np.ndarray:
+    """``jax.random.split(key, n)`` computed by the library's host Threefry."""
+    lib = load_library()
+    out = np.zeros((n, 2), dtype=np.uint32)
+    rc = lib.mf_prng_split(int(key[0]), int(key[1]), n, 1 if partitionable else 0, out.ctypes.data)
+    if rc:
+        raise EngineError(f"mf_prng_split failed ({rc})")
+    return out
+
+
+def prng_key(seed: int) -> np.ndarray:
+    """``jax.random.PRNGKey(seed)`` for 32-bit seeds: ``[0, seed]``."""
+    s = int(seed)
+    return np.array([(s >> 32) & 0xFFFFFFFF if s >= 0 else 0, s & 0xFFFFFFFF], dtype=np.uint32)
+
+
+def _torch():
+    import torch
+    return torch
+
+
+@dataclass
+class _UploadedTopo:
+    topo_id: int
+    n_dof: int
+    total_xbs: int
+    n_sites_total: int
+
+
+def topo_desc_arrays(topo) -> Dict[str, np.ndarray]:
+    """Host arrays of a SarcTopology in the layout ``mf_topo_desc`` expects."""
+    from .topology import thin_rest_cumsum
+    c = np.ascontiguousarray
+    return dict(
+        xb_to_thin_id=c(topo.xb_to_thin_id, dtype=np.int32),
+        xb_to_thin_face=c(topo.xb_to_thin_face, dtype=np.int32),
+        xb_valid=c(topo.xb_valid, dtype=np.uint8),
+        face_to_sites=c(topo.face_to_sites, dtype=np.int32),
+        n_sites_per_face=c(topo.n_sites_per_face, dtype=np.int32),
+        tm_prev_neighbor=c(topo.tm_prev_neighbor, dtype=np.int32),
+        tm_next_neighbor=c(topo.tm_next_neighbor, dtype=np.int32),
+        crown_offsets=c(topo.crown_offsets, dtype=np.float32),
+        crown_rests=c(topo.crown_rests, dtype=np.float32),
+        binding_offsets=c(topo.binding_offsets, dtype=np.float32),
+        binding_rests=c(topo.binding_rests, dtype=np.float32),
+        thin_rest_cumsum=c(thin_rest_cumsum(topo), dtype=np.float32),
+        xb_bin_edges=c(topo.xb_bin_edges, dtype=np.float32),
+        xb_bin_centers=c(topo.xb_bin_centers, dtype=np.float32),
+    )
+
+
+class Engine:
+    """One device context of the CUDA engine (``mf_create`` ... ``mf_destroy``)."""
+
+    def __init__(self, device: int = 0):
+        torch = _torch()
+        if not torch.cuda.is_available():
+            raise EngineError("multifil_jax_b200 needs a CUDA device; none is available")
+        self.lib = load_library()
+        self.device = device
+        torch.cuda.set_device(device)
+        torch.cuda.init()
+        h = ctypes.c_void_p()
+        rc = self.lib.mf_create(device, ctypes.byref(h))
+        if rc:
+            raise EngineError(f"mf_create failed ({rc})")
+        self.h = h
+        self._topos: Dict[tuple, _UploadedTopo] = {}
+
+    def close(self):
+        if getattr(self, 'h', None):
+            self.lib.mf_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            msg = self.lib.mf_last_error(self.h)
+            raise EngineError(f"{what} failed ({rc}): {msg.decode() if msg else ''}")
+
+    def upload(self, topo) -> _UploadedTopo:
+        key = topo.size_key()
+        if key in self._topos:
+            return self._topos[key]
+        arrs = topo_desc_arrays(topo)
+        d = mf_topo_desc(topo.n_thick, topo.n_crowns, topo.n_thin, topo.n_sites, topo.n_xb_per_crown,
+                         topo.max_sites_per_face, topo.n_xb_bins,
+                         *[arrs[f].ctypes.data for f in (
+                             'xb_to_thin_id', 'xb_to_thin_face', 'xb_valid', 'face_to_sites',
+                             'n_sites_per_face', 'tm_prev_neighbor', 'tm_next_neighbor', 'crown_offsets',
+                             'crown_rests', 'binding_offsets', 'binding_rests', 'thin_rest_cumsum',
+                             'xb_bin_edges', 'xb_bin_centers')])
+        tid = ctypes.c_int32()
+        self._check(self.lib.mf_upload_topology(self.h, ctypes.byref(d), ctypes.byref(tid)), 'mf_upload_topology')
+        up = _UploadedTopo(tid.value, topo.n_dof, topo.total_xbs, topo.n_sites_total)
+        self._topos[key] = up
+        return up
+
+    def tune_threads(self, topo, threads: int):
+        up = self.upload(topo)
+        self._check(self.lib.mf_tune_threads(self.h, up.topo_id, int(threads)), 'mf_tune_threads')
+
+    # ------------------------------------------------------------------
+    def run_batch(self, topos, params, z, pCa, ls, n_steps, keys, K_lat=None, nu=None, dt=None,
+                  n_newton=4, n_cg=6, flags=0, chunk_steps=0, residual_warn=1.5, stream=None,
+                  u_thin=None, u_xb=None, want_x_trace=False, want_state_trace=False, keys_out=None):
+        """Run B conditions through the fused kernel; every array is a torch CUDA tensor.
+
+        ``topos`` is a list of B SarcTopology objects (or one shared).  Returns
+        a dict with ``metrics`` [B, 52, T], ``status`` [B] and optional traces.
+        """
+        torch = _torch()
+        dev = torch.device('cuda', self.device)
+        B, T = z.shape
+        if not isinstance(topos, (list, tuple)):
+            topos = [topos] * B
+        ups = [self.upload(t) for t in topos]
+        tid = np.array([u.topo_id for u in ups], dtype=np.int32)
+        max_dof = max(u.n_dof for u in ups)
+        max_x = max(u.total_xbs for u in ups)
+        max_s = max(u.n_sites_total for u in ups)
+
+        def f32(a):
+            assert a.is_cuda and a.dtype == torch.float32 and a.is_contiguous()
+            return a
+
+        metrics = torch.empty((B, N_METRICS, T), dtype=torch.float32, device=dev)
+        status = torch.zeros(B, dtype=torch.int32, device=dev)
+        out = dict(metrics=metrics, status=status)
+        xt = st = bt = None
+        if want_x_trace:
+            xt = torch.zeros((B, T, max_dof), dtype=torch.float32, device=dev)
+            out['x_trace'] = xt
+        if want_state_trace:
+            st = torch.zeros((B, T, max_x + max_s), dtype=torch.int8, device=dev)
+            bt = torch.zeros((B, T, max_x + max_s), dtype=torch.int32, device=dev)
+            out['state_trace'] = st
+            out['bound_trace'] = bt
+        bat = mf_batch()
+        bat.B, bat.T_max = B, T
+        bat.topo_id = tid.ctypes.data
+        bat.params = f32(params).data_ptr()
+        bat.z = f32(z).data_ptr()
+        bat.pCa = f32(pCa).data_ptr()
+        bat.ls = f32(ls).data_ptr()
+        assert n_steps.dtype == torch.int32
+        bat.n_steps = n_steps.data_ptr()
+        bat.keys = keys.data_ptr()
+        bat.K_lat = f32(K_lat).data_ptr() if K_lat is not None else None
+        bat.nu = f32(nu).data_ptr() if nu is not None else None
+        bat.dt = f32(dt).data_ptr() if dt is not None else None
+        bat.n_newton, bat.n_cg, bat.flags = int(n_newton), int(n_cg), int(flags)
+        bat.chunk_steps = int(chunk_steps)
+        bat.residual_warn = float(residual_warn)
+        bat.metrics_out = metrics.data_ptr()
+        bat.status_out = status.data_ptr()
+        bat.keys_out = keys_out.data_ptr() if keys_out is not None else None
+        bat.u_thin = f32(u_thin).data_ptr() if u_thin is not None else None
+        bat.u_xb = f32(u_xb).data_ptr() if u_xb is not None else None
+        bat.x_trace = xt.data_ptr() if xt is not None else None
+        bat.state_trace = st.data_ptr() if st is not None else None
+        bat.bound_trace = bt.data_ptr() if bt is not None else None
+        s = stream if stream is not None else torch.cuda.current_stream(dev)
+        self._check(self.lib.mf_run_batch(self.h, ctypes.byref(bat), ctypes.c_void_p(s.cuda_stream)),
+                    'mf_run_batch')
+        return out
+
+
+_engines: Dict[int, Engine] = {}
+
+
+def get_engine(device: Optional[int] = None) -> Engine:
+    torch = _torch()
+    if not torch.cuda.is_available():
+        raise EngineError("multifil_jax_b200 needs a CUDA device; none is available")
+    d = torch.cuda.current_device() if device is None else device
+    if d not in _engines:
+        _engines[d] = Engine(d)
+    return _engines[d]
