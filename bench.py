@@ -1,0 +1,456 @@
+"""Benchmark: condition-timesteps/s on the 256-condition pCa sweep (2x2 skeletal, 500 ms).
+
+One bench step = the whole sweep (256 conditions x 500 timesteps) through the
+fused kernel in one launch.  Prints ONE JSON line on rank 0.
+
+  value    device throughput with inputs resident in HBM (CUDA events, L2
+           flushed between steps, max over ranks)
+  e2e      the same sweep through the public run() with host inputs, host
+           metrics out (H2D + kernel + D2H inside the timed region)
+  plain    one condition per launch, one launch per timestep (baseline form)
+  serving  continuous batching of a Poisson request stream, p50/p99 latency
+
+``--impl reference`` times the CPU restatement of the reference algorithm (the
+reference's JAX CPU path cannot be installed here) on all host cores.
+Multi-GPU: replicas only -- every rank runs its own copy of the sweep.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+B_SWEEP, T_SWEEP = 256, 500
+METRIC = 'condition-timesteps/s'
+
+
+def _dist():
+    rank = int(os.environ.get('RANK', 0))
+    world = int(os.environ.get('WORLD_SIZE', 1))
+    local = int(os.environ.get('LOCAL_RANK', 0))
+    return rank, world, local
+
+
+def _init_pg(world, local, backend):
+    import torch.distributed as dist
+    from datetime import timedelta
+    if world > 1 and not dist.is_initialized():
+        os.environ.setdefault('MASTER_ADDR', '127.0.0.1')
+        dist.init_process_group(backend=backend, timeout=timedelta(seconds=120))
+    return dist
+
+
+def _max_over_ranks(x, world, device=None):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms in the background."""
+    Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+         'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+         'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(REPO, '_build', f'clocks_{os.getpid()}.csv')
+
+    def __enter__(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        try:
+            self.f = open(self.path, 'w')
+            self.proc = subprocess.Popen(['nvidia-smi', f'--id={self.gpu}', f'--query-gpu={self.Q}',
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [l.split(',') for l in open(self.path).read().strip().splitlines() if l.strip()]
+        except Exception:
+            rows = []
+        if not rows:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['unsampled']}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace('.', '').isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace('.', '').isdigit()]
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        reasons = sorted({names[i] for r in rows for i in range(4)
+                          if len(r) > 5 + i and r[5 + i].strip() == 'Active'})
+        return {'sm_mhz': float(np.median(sm)) if sm else None, 'sm_max_mhz': max(mx) if mx else None,
+                'reasons': reasons, 'samples': len(rows)}
+
+
+def sweep_inputs():
+    from multifil_jax_b200 import SarcTopology, get_skeletal_params
+    from multifil_jax_b200.simulation import plan_batch
+    s, d = get_skeletal_params()
+    topo = SarcTopology.create(2, 2, s, d)
+    pcas = list(np.linspace(4.0, 7.0, B_SWEEP))
+    plan = plan_batch(topo, duration_ms=T_SWEEP, pCa=pcas, z_line=900.0, dynamic_params=d, static_params=s,
+                      rng_seed=0)
+    return topo, s, d, pcas, plan
+
+
+# ---------------------------------------------------------------------------
+# algorithmic work of one condition-timestep (Roofline)
+# ---------------------------------------------------------------------------
+def flops_per_condition_step(topo, iters, n_bound, tables_rebuilt=0.0):
+    """FP32 flops the fused step performs, counted from the kernel's arithmetic.
+
+    Per step: nearest-site search 3 flops x 30 candidates per head; sampling
+    ~6 compares per head/site; residual: 12 per node + 40 per bound head
+    (sqrt, atan2 counted as 1 flop each, SFU separately); per CG iteration:
+    JVP 8 per node + 6 per bound head, Thomas scans 2 x 2 flops per scan node
+    (2n nodes per filament) + 1 per node, dots/axpys 10 per node; CG iterations
+    per Newton iteration = 6, plus one residual per Newton iteration and the
+    initial one; metrics 12 per node.
+    """
+    N, X, S = topo.n_dof, topo.total_xbs, topo.n_sites_total
+    scan_nodes = topo.n_thick * 2 * topo.n_crowns + topo.n_thin * 2 * topo.n_sites
+    kin = X * 30 * 3 + (X + S) * 6
+    resid = N * 12 + n_bound * 40
+    cg = N * 8 + n_bound * 6 + 2 * 2 * scan_nodes + N + N * 10
+    newton = resid + 6 * cg
+    metrics = N * 12 + X * 4
+    per_step = kin + resid + iters * newton + metrics
+    return per_step
+
+
+def fp32_peak_tflops(sm_mhz, n_sm=148):
+    return n_sm * 128 * 2 * sm_mhz * 1e6 / 1e12
+
+
+# ---------------------------------------------------------------------------
+def bench_gpu(args):
+    import torch
+    rank, world, local = _dist()
+    torch.cuda.set_device(local)
+    dev = torch.device('cuda', local)
+    _init_pg(world, local, 'nccl')
+    from multifil_jax_b200 import run
+    from multifil_jax_b200.engine import get_engine, MF_FLAG_PLAIN, MF_FLAG_PRECISE
+    eng = get_engine(local)
+    topo, s, d, pcas, plan = sweep_inputs()
+    flags = MF_FLAG_PRECISE if args.precision == 'mixed' else 0
+    B, T = plan.total, plan.n_steps
+
+    def dv(a, dt=torch.float32):
+        return torch.as_tensor(np.ascontiguousarray(a), device=dev).to(dt).contiguous()
+    P, Z, PC, L = dv(plan.params), dv(plan.z), dv(plan.pCa), dv(plan.ls)
+    NS = torch.full((B,), T, dtype=torch.int32, device=dev)
+    K = dv(plan.keys.astype(np.int64), torch.int64).to(torch.int32)
+    Kl, NU, DT = dv(plan.K_lat), dv(plan.nu), torch.ones(B, dtype=torch.float32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    stream = torch.cuda.current_stream(dev)
+
+    def one_step():
+        return eng.run_batch(topo, P, Z, PC, L, NS, K, K_lat=Kl, nu=NU, dt=DT, flags=flags,
+                             n_newton=s.n_newton_steps, n_cg=s.n_cg_steps, stream=stream)
+    for _ in range(args.warmup):
+        out = one_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.fill_(k & 0xFF)
+            ev[k][0].record(stream)
+            out = one_step()
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = [a.elapsed_time(b) for a, b in ev]
+    t_dev = sum(ms) / 1e3
+    t_dev = _max_over_ranks(t_dev, world, dev)
+    value = B * T * args.steps * world / t_dev
+    met = out['metrics'].cpu().numpy()
+    iters_mean = float(met[:, 51, :].mean())
+    nbound_mean = float(met[:, 5, :].mean())
+    clocks = clk.summary()
+
+    # e2e: the public API with host buffers (plan, H2D, kernel, D2H inside)
+    e2e_times = []
+    for k in range(max(1, args.steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = run(topo, duration_ms=T_SWEEP, pCa=pcas, z_line=900.0, dynamic_params=d, static_params=s,
+                rng_seed=0, precision=args.precision)
+        t1 = time.perf_counter()
+        e2e_times.append(t1 - t0)
+    t_e2e = _max_over_ranks(float(np.sum(e2e_times)), world, dev)
+    e2e_value = B * T * len(e2e_times) * world / t_e2e
+    h2d = plan.params.nbytes + plan.z.nbytes + plan.pCa.nbytes + plan.ls.nbytes + plan.keys.nbytes + \
+        plan.K_lat.nbytes + plan.nu.nbytes + 2 * 4 * B
+    d2h = B * 52 * T * 4
+
+    # plain: one condition per launch, one launch per timestep, on a subset
+    nplain = args.plain_conditions
+    res_plain = None
+    if nplain > 0:
+        sl = slice(0, nplain)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        eng.run_batch(topo, P[sl].contiguous(), Z[sl].contiguous(), PC[sl].contiguous(), L[sl].contiguous(),
+                      NS[sl].contiguous(), K[sl].contiguous(), K_lat=Kl[sl].contiguous(), nu=NU[sl].contiguous(),
+                      dt=DT[sl].contiguous(), flags=flags | MF_FLAG_PLAIN, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_plain = e0.elapsed_time(e1) / 1e3
+        res_plain = nplain * T / t_plain
+
+    # the other precision mode, device-timed the same way (for the record)
+    other = 'float32' if args.precision == 'mixed' else 'mixed'
+    oflags = MF_FLAG_PRECISE if other == 'mixed' else 0
+    eng.run_batch(topo, P, Z, PC, L, NS, K, K_lat=Kl, nu=NU, dt=DT, flags=oflags, stream=stream)
+    oe = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.fill_(k & 0xFF)
+        oe[k][0].record(stream)
+        eng.run_batch(topo, P, Z, PC, L, NS, K, K_lat=Kl, nu=NU, dt=DT, flags=oflags, stream=stream)
+        oe[k][1].record(stream)
+    torch.cuda.synchronize()
+    other_value = B * T * args.steps / (sum(a.elapsed_time(b) for a, b in oe) / 1e3)
+
+    flops = flops_per_condition_step(topo, iters_mean, nbound_mean)
+    sm_mhz = clocks.get('sm_mhz') or 1965.0
+    fp32_peak = fp32_peak_tflops(sm_mhz)
+    achieved_tf = flops * (B * T) / (t_dev / args.steps / world * 1.0) / 1e12 if world == 1 else \
+        flops * (B * T) / (t_dev / args.steps) / 1e12
+    peaks = json.load(open(os.path.join(REPO, 'MEASURED_PEAKS.json'))) if os.path.exists(
+        os.path.join(REPO, 'MEASURED_PEAKS.json')) else {'hbm_gbs': 6650.0}
+    hbm_bytes_step = B * T * (52 * 4 + 3 * 4)  # metrics written + drivers read (algorithmic)
+    launch_s = t_dev / args.steps / world if world == 1 else t_dev / args.steps
+    hbm_gbs = hbm_bytes_step / launch_s / 1e9
+    line = {
+        'metric': METRIC, 'value': value, 'unit': METRIC, 'n_gpus': world, 'steps': args.steps,
+        'warmup': args.warmup, 'ms_per_step': t_dev / args.steps * 1e3, 'higher_is_better': True,
+        'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32' if args.precision == 'float32' else 'f32+f64',
+        'data': 'synthetic (pCa sweep inputs, random keys from PRNGKey(0))',
+        'config': {'workload': '256-condition pCa sweep, 2x2 skeletal lattice, pCa=linspace(4,7,256), '
+                               'z_line=900 nm, 500 ms at dt=1 ms, keys split(PRNGKey(0),256)',
+                   'conditions': B, 'timesteps': T, 'precision': args.precision, 'parallelism': f'replicas{world}',
+                   'l2': 'flushed between timed steps (256 MB write)', 'launches_per_step': 1,
+                   'plain_conditions': nplain, 'plain_condition_timesteps_per_s': res_plain,
+                   'batched_over_plain': (value / world / res_plain) if res_plain else None,
+                   'mean_newton_iters': iters_mean, 'mean_bound_heads': nbound_mean,
+                   f'{other}_value': other_value,
+                   'precision_modes': 'mixed = node displacements + float64 residual test + renormalised '
+                                      'float64 expm squaring (<=1e-5 force error vs the FP64 oracle); '
+                                      'float32 = the reference\'s single-precision arithmetic'},
+        'e2e': {'value': e2e_value, 'unit': METRIC, 'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': int(d2h)},
+        'gpu_launches': args.steps,
+        'roofline': {'bound': 'hbm', 'achieved': hbm_gbs, 'peak': peaks['hbm_gbs'], 'unit': 'GB/s',
+                     'frac': hbm_gbs / peaks['hbm_gbs'], 'traffic': args.traffic,
+                     'note': 'state stays in shared memory; algorithmic HBM bytes = 220 B per condition-step'},
+        'roofline_fp32': {'bound': 'fp32 cuda-core issue', 'achieved': achieved_tf, 'peak': fp32_peak,
+                          'unit': 'TFLOP/s', 'frac': achieved_tf / fp32_peak,
+                          'flops_per_condition_step': flops,
+                          'peak_basis': f'148 SMs x 128 lanes x 2 x median SM clock {sm_mhz:.0f} MHz'},
+        'clocks': clocks,
+    }
+    if args.serve_requests > 0 and rank == 0:
+        line['serving'] = bench_serving(args, local)
+    if rank == 0 and not args.no_cpu_baseline:
+        line['cpu_baseline'] = cpu_baseline(args)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def bench_serving(args, device):
+    """Poisson arrivals of mixed requests through the continuous-batching server."""
+    from multifil_jax_b200 import SarcTopology, get_skeletal_params, get_cardiac_params
+    from multifil_jax_b200.serve import SimulationServer
+    from multifil_jax_b200.engine import prng_split, prng_key
+    rng = np.random.default_rng(1)
+    n = args.serve_requests
+    topos = {}
+    reqs = []
+    for i in range(n):
+        r, c = (int(v) for v in rng.integers(1, args.serve_max_lattice + 1, 2))
+        preset = 'skeletal' if rng.random() < 0.5 else 'cardiac'
+        key = (r, c, preset)
+        if key not in topos:
+            sp = get_skeletal_params() if preset == 'skeletal' else get_cardiac_params()
+            topos[key] = (SarcTopology.create(r, c, *sp), sp[1])
+        dur = float(rng.uniform(args.serve_min_ms, args.serve_max_ms))
+        reqs.append((key, float(rng.uniform(4, 7)), float(rng.uniform(850, 1000)), dur,
+                     prng_split(prng_key(1000 + i), 1)[0]))
+    total_steps = sum(int(r[3]) for r in reqs)
+    srv = SimulationServer(mem_budget=args.serve_budget_gb << 30, chunk_steps=args.serve_chunk, device=device)
+    # arrival rate: a fraction of the measured batched capacity for this mix
+    lam = args.serve_rate
+    t_arr = np.cumsum(rng.exponential(1.0 / lam, n))
+    ids = {}
+    t0 = time.perf_counter()
+    i = 0
+    while i < n or srv.step(0) != (0, 0):
+        now = time.perf_counter() - t0
+        while i < n and t_arr[i] <= now:
+            k, pCa, z, dur, key = reqs[i]
+            ids[srv.submit(topos[k][0], topos[k][1], pCa, z, dur, key)] = i
+            i += 1
+        a, q = srv.step(1)
+        if a == 0 and q == 0 and i < n:
+            time.sleep(max(0.0, min(0.002, t_arr[i] - (time.perf_counter() - t0))))
+        if i >= n and a == 0 and q == 0:
+            break
+    t_end = time.perf_counter() - t0
+    lat = []
+    for rid in list(ids):
+        r = srv.poll(rid)
+        if r is not None:
+            lat.append(r.latency_s)
+    srv.close()
+    lat = np.array(lat)
+    return {'requests': n, 'completed': int(lat.size), 'arrival_rate_per_s': lam,
+            'p50_latency_s': float(np.percentile(lat, 50)) if lat.size else None,
+            'p99_latency_s': float(np.percentile(lat, 99)) if lat.size else None,
+            'condition_timesteps_per_s': total_steps / t_end, 'wall_s': t_end,
+            'mix': f'lattice 1..{args.serve_max_lattice} square/rect, duration U[{args.serve_min_ms},{args.serve_max_ms}] ms, '
+                   f'skeletal/cardiac 50/50, chunk {args.serve_chunk} steps'}
+
+
+def _oracle_sample(args_tuple):
+    nr, nc, T, pCa, seed = args_tuple
+    import numpy as np
+    from multifil_jax_b200 import SarcTopology, get_skeletal_params
+    from oracle import step as OS, prng
+    s, d = get_skeletal_params()
+    topo = SarcTopology.create(nr, nc, s, d)
+    key = prng.split(prng.PRNGKey(0), 256)[seed]
+    t0 = time.perf_counter()
+    OS.run_condition(topo, d.param_row(), np.full(T, 900.0), np.full(T, pCa), np.full(T, 14.0), key)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(args, cores=1, n_cond=2, T=20):
+    """The oracle (NumPy restatement of the reference timestep) on host cores."""
+    os.environ.setdefault('OMP_NUM_THREADS', '1')
+    jobs = [(2, 2, T, float(p), i) for i, p in enumerate(np.linspace(4.0, 7.0, n_cond))]
+    t0 = time.perf_counter()
+    if cores > 1:
+        import multiprocessing as mp
+        with mp.get_context('spawn').Pool(cores) as pool:
+            pool.map(_oracle_sample, jobs)
+    else:
+        for j in jobs:
+            _oracle_sample(j)
+    dt = time.perf_counter() - t0
+    return {'value': n_cond * T / dt, 'unit': METRIC, 'cores': cores, 'kind': 'port',
+            'sample': f'{n_cond} conditions x {T} timesteps of the 2x2 pCa sweep (oracle, NumPy float32)'}
+
+
+def bench_reference(args):
+    """--impl reference: the reference algorithm on the host CPU (JAX is not installable here)."""
+    rank, world, local = _dist()
+    if rank != 0:
+        return
+    cores = len(os.sched_getaffinity(0))
+    vals = []
+    for _ in range(args.warmup):
+        cpu_baseline(args, cores=cores, n_cond=cores, T=5)
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(args, cores=cores, n_cond=cores, T=10)['value'])
+    v = float(np.mean(vals))
+    print(json.dumps({
+        'impl': 'reference', 'metric': METRIC, 'value': v, 'unit': METRIC, 'n_gpus': world,
+        'steps': args.steps, 'warmup': args.warmup, 'higher_is_better': True, 'scaling': 'weak',
+        'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+        'config': {'workload': '256-condition pCa sweep, 2x2 skeletal lattice, 500 ms (sampled)',
+                   'note': 'reference JAX path not installable (no jax wheel offline); its NumPy restatement '
+                           '(oracle) runs instead, one condition per host core'},
+        'cpu_baseline': {'value': v, 'unit': METRIC, 'cores': cores, 'kind': 'port',
+                         'sample': f'{cores} conditions x 10 timesteps per step, 2x2 lattice'},
+        'e2e': {'value': v, 'unit': METRIC, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }), flush=True)
+
+
+def profile_case(args):
+    """One warm-up and one measured launch of the fused kernel (profiling target)."""
+    import torch
+    from multifil_jax_b200 import SarcTopology, get_skeletal_params
+    from multifil_jax_b200.simulation import plan_batch
+    from multifil_jax_b200.engine import get_engine, MF_FLAG_PRECISE
+    parts = [int(v) for v in args.profile_case.split(',')]
+    B, T = parts[0], parts[1]
+    n = parts[2] if len(parts) > 2 else 2
+    s, d = get_skeletal_params()
+    topo = SarcTopology.create(n, n, s, d)
+    plan = plan_batch(topo, duration_ms=T, pCa=list(np.linspace(4.0, 7.0, B)), dynamic_params=d, static_params=s)
+    dev = torch.device('cuda', 0)
+    dv = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev).to(torch.float32).contiguous()
+    eng = get_engine(0)
+    keys = torch.as_tensor(plan.keys.astype(np.int64), device=dev).to(torch.int32)
+    NS = torch.full((B,), T, dtype=torch.int32, device=dev)
+    flags = MF_FLAG_PRECISE if args.precision == 'mixed' else 0
+    for _ in range(2):
+        out = eng.run_batch(topo, dv(plan.params), dv(plan.z), dv(plan.pCa), dv(plan.ls), NS, keys, flags=flags)
+    torch.cuda.synchronize()
+    print(json.dumps({'profile_case': [B, T, n], 'force_last_mean': float(out['metrics'][:, 0, -1].mean())}))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=5)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--precision', default='mixed', choices=['float32', 'mixed'])
+    ap.add_argument('--plain-conditions', type=int, default=8)
+    ap.add_argument('--serve-requests', type=int, default=300)
+    ap.add_argument('--serve-rate', type=float, default=200.0)
+    ap.add_argument('--serve-max-lattice', type=int, default=6)
+    ap.add_argument('--serve-min-ms', type=float, default=100.0)
+    ap.add_argument('--serve-max-ms', type=float, default=400.0)
+    ap.add_argument('--serve-chunk', type=int, default=25)
+    ap.add_argument('--serve-budget-gb', type=int, default=8)
+    ap.add_argument('--traffic', type=float, default=None)
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--profile-case', default=None,
+                    help='B,T[,lattice]: run the fused kernel once on B conditions x T steps (for ncu)')
+    args = ap.parse_args()
+    if args.profile_case:
+        profile_case(args)
+    elif args.impl == 'reference':
+        bench_reference(args)
+    else:
+        bench_gpu(args)
+
+
+if __name__ == '__main__':
+    main()

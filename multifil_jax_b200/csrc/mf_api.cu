@@ -45,6 +45,8 @@ struct mf_ctx {
   int smem_optin = 0;
   int num_sms = 0;
   Server* server = nullptr;
+  cudaStream_t cap_stream = nullptr;  // private stream for CUDA-graph capture
+  cudaEvent_t cap_event = nullptr;
 };
 
 static int fail(mf_ctx* c, int code, const char* fmt, ...) {
@@ -70,22 +72,39 @@ static int fail(mf_ctx* c, int code, const char* fmt, ...) {
 // ---------------------------------------------------------------------------
 // kernel dispatch by CTA size
 // ---------------------------------------------------------------------------
+// Raise the dynamic shared-memory limit of a kernel instance (not capturable,
+// so it is done before any graph capture).
 template <int NT>
-static cudaError_t launch_nt(const StepArgs& a, int grid, int base, size_t smem, cudaStream_t st) {
-  static bool attr_set = false;
+static cudaError_t prepare_nt(size_t smem) {
   static size_t attr_bytes = 0;
-  if (!attr_set || smem > attr_bytes) {
+  if (smem > attr_bytes) {
     cudaError_t e = cudaFuncSetAttribute(step_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
-    attr_set = true;
     attr_bytes = smem;
   }
+  return cudaSuccess;
+}
+
+static cudaError_t prepare(int nt, size_t smem) {
+  switch (nt) {
+    case 128: return prepare_nt<128>(smem);
+    case 256: return prepare_nt<256>(smem);
+    case 512: return prepare_nt<512>(smem);
+    default: return prepare_nt<1024>(smem);
+  }
+}
+
+template <int NT>
+static cudaError_t launch_nt(const StepArgs& a, int grid, int base, size_t smem, cudaStream_t st) {
   step_kernel<NT><<<grid, NT, smem, st>>>(a, base);
-  return cudaGetLastError();
+  return cudaPeekAtLastError();
 }
 
 static cudaError_t launch(int nt, const StepArgs& a, int grid, int base, size_t smem, cudaStream_t st) {
+  cudaError_t e = prepare(nt, smem);
+  if (e != cudaSuccess) return e;
+  cudaGetLastError();  // clear a stale non-sticky error of an earlier, already reported call
   switch (nt) {
     case 128: return launch_nt<128>(a, grid, base, smem, st);
     case 256: return launch_nt<256>(a, grid, base, smem, st);
@@ -132,6 +151,8 @@ int mf_destroy(mf_ctx* ctx) {
   }
   if (ctx->ws) cudaFree(ctx->ws);
   if (ctx->d_cond) cudaFree(ctx->d_cond);
+  if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
+  if (ctx->cap_event) cudaEventDestroy(ctx->cap_event);
   delete ctx;
   return MF_OK;
 }
@@ -313,7 +334,7 @@ static StepArgs make_args(const mf_batch* bt, const CondDesc* dc, int flags, int
   a.n_cg = bt->n_cg;
   a.flags = flags;
   a.resid_warn = bt->residual_warn;
-  a.sq64_from = (flags & FLAG_PRECISE) ? 8 : 1 << 20;
+  a.sq64_from = (flags & FLAG_PRECISE) ? 1 : 1 << 20;
   a.u_thin = bt->u_thin;
   a.u_xb = bt->u_xb;
   a.x_trace = bt->x_trace;
@@ -460,15 +481,28 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
   CK(cudaMemcpyAsync(ctx->d_cond, tab.data(), sizeof(CondDesc) * tab.size(), cudaMemcpyHostToDevice, st));
   const bool use_graph = !(bt->flags & MF_FLAG_NO_GRAPH) && n_chunks > 1;
   cudaGraph_t graph = nullptr;
-  if (use_graph) CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  cudaStream_t launch_st = st;
+  if (use_graph) {
+    // capture on a private non-blocking stream (the caller's may be the legacy
+    // default stream, which cannot be captured); the graph replays on st
+    if (!ctx->cap_stream) {
+      CK(cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&ctx->cap_event, cudaEventDisableTiming));
+    }
+    launch_st = ctx->cap_stream;
+    for (const Group& g : groups) CK(prepare(g.threads, g.smem));
+    CK(cudaEventRecord(ctx->cap_event, st));
+    CK(cudaStreamWaitEvent(launch_st, ctx->cap_event, 0));
+    CK(cudaStreamBeginCapture(launch_st, cudaStreamCaptureModeThreadLocal));
+  }
   for (int c = 0; c < n_chunks; ++c) {
     for (const Group& g : groups) {
       StepArgs a = make_args(bt, ctx->d_cond + (size_t)c * B, base_flags | (g.vg ? 64 : 0), max_dof,
                              max_x, max_s);
-      cudaError_t e = launch(g.threads, a, g.end - g.begin, g.begin, g.smem, st);
+      cudaError_t e = launch(g.threads, a, g.end - g.begin, g.begin, g.smem, launch_st);
       if (e != cudaSuccess) {
         if (use_graph) {
-          cudaStreamEndCapture(st, &graph);
+          cudaStreamEndCapture(launch_st, &graph);
           if (graph) cudaGraphDestroy(graph);
         }
         return fail(ctx, MF_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
@@ -476,7 +510,7 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
     }
   }
   if (use_graph) {
-    CK(cudaStreamEndCapture(st, &graph));
+    CK(cudaStreamEndCapture(launch_st, &graph));
     cudaGraphExec_t exec = nullptr;
     cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
     cudaGraphDestroy(graph);

@@ -16,7 +16,8 @@ __host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, bool vec_
   add(sizeof(double) * 64);                // redd
   add(sizeof(float) * 32 * 24);            // red
   if (!vec_global) add(sizeof(float) * 5 * N);  // x r dx pv zz
-  add(sizeof(float) * 3 * X);              // fxb fdx xb_ax
+  if (!vec_global) add(sizeof(float) * 4 * X);  // fxb fdx fdd frdd
+  add(sizeof(float) * X);                  // xb_ax
   add(sizeof(float) * S);                  // site / win1
   add(sizeof(int) * S);                    // win2
   add(sizeof(int16_t) * 2 * X);            // xb_bound xb_near
@@ -28,6 +29,9 @@ __host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, bool vec_
   add(sizeof(float) * nw * scan);          // scan
   add(sizeof(float) * kNParams);           // P
   add(sizeof(float) * 4 * t.n_thick);      // tvec
+  add(sizeof(int16_t) * X);                // blist
+  add(sizeof(int) * 4);                    // nbound
+  add(sizeof(int) * 32);                   // wsum
   return o;
 }
 
@@ -42,8 +46,9 @@ __device__ void carve(Sim<NT>& m, char* base, bool vec_global) {
   m.s.red = (float*)take(sizeof(float) * 32 * 24);
   float* v5 = vec_global ? reinterpret_cast<float*>(m.ws + m.L.vec) : (float*)take(sizeof(float) * 5 * N);
   m.s.x = v5; m.s.r = v5 + N; m.s.dx = v5 + 2 * N; m.s.pv = v5 + 3 * N; m.s.zz = v5 + 4 * N;
-  float* v3 = (float*)take(sizeof(float) * 3 * X);
-  m.s.fxb = v3; m.s.fdx = v3 + X; m.s.xb_ax = v3 + 2 * X;
+  float* f4 = vec_global ? reinterpret_cast<float*>(m.ws + m.L.vec) + 5 * N : (float*)take(sizeof(float) * 4 * X);
+  m.s.fxb = f4; m.s.fdx = f4 + X; m.s.fdd = f4 + 2 * X; m.s.frdd = f4 + 3 * X;
+  m.s.xb_ax = (float*)take(sizeof(float) * X);
   m.s.site = (float*)take(sizeof(float) * S);
   m.s.win2 = (int*)take(sizeof(int) * S);
   int16_t* i2 = (int16_t*)take(sizeof(int16_t) * 2 * X);
@@ -57,6 +62,9 @@ __device__ void carve(Sim<NT>& m, char* base, bool vec_global) {
   m.s.scan = (float*)take(sizeof(float) * NT / 32 * scan);
   m.s.P = (float*)take(sizeof(float) * kNParams);
   m.s.tvec = (float*)take(sizeof(float) * 4 * t.n_thick);
+  m.s.blist = (int16_t*)take(sizeof(int16_t) * X);
+  m.s.nbound = (int*)take(sizeof(int) * 4);
+  m.s.wsum = (int*)take(sizeof(int) * 32);
 }
 
 // ---------------------------------------------------------------------------
@@ -236,8 +244,30 @@ __device__ void metrics(Sim<NT>& m, int t, float zl, float pCa, float new_ls, fl
 // ---------------------------------------------------------------------------
 // one CTA = one condition, steps [t_begin, t_end)
 // ---------------------------------------------------------------------------
+#ifdef MF_PHASE_TIMING
+// Diagnostic build only: thread 0 accumulates clock64() per phase and writes
+// the totals over the x_trace test-hook buffer at the end of the launch.
+#define MF_PH(k)                                  \
+  do {                                            \
+    __syncthreads();                              \
+    if (m.tid == 0) {                             \
+      const long long now_ = clock64();           \
+      ph_acc[ph_cur] += (double)(now_ - ph_t0);   \
+      ph_t0 = now_;                               \
+      ph_cur = (k);                               \
+    }                                             \
+  } while (0)
+#else
+#define MF_PH(k) do { } while (0)
+#endif
+
 template <int NT>
 __device__ void run_condition(const StepArgs& A, int ci) {
+#ifdef MF_PHASE_TIMING
+  double ph_acc[12] = {0};
+  long long ph_t0 = clock64();
+  int ph_cur = 0;
+#endif
   extern __shared__ __align__(16) char smem_raw[];
   const CondDesc cd = A.cond[ci];
   const TopoDev& T = *cd.topo;
@@ -310,7 +340,8 @@ __device__ void run_condition(const StepArgs& A, int ci) {
     float d0 = m.s.P[LATTICE_SPACING];
     const bool dyn_save = m.dyn;
     m.dyn = false;
-    m.solve(m.s.P[Z_LINE], d0, resid, it, 0.f);
+    m.build_bound_list();
+    m.solve(m.s.P[Z_LINE], d0, resid, it, false);
     m.dyn = dyn_save;
     if (m.tid == 0) {
       key_s[0] = cd.key[0];
@@ -370,6 +401,7 @@ __device__ void run_condition(const StepArgs& A, int ci) {
     } else {
       d_kin = ls_t;
     }
+    MF_PH(1);
     // probability tables for (pCa, d_kin)
     if (!((double)pCa == misc[MS_TAB_PCA] && (double)d_kin == misc[MS_TAB_D])) {
       __syncthreads();
@@ -379,6 +411,7 @@ __device__ void run_condition(const StepArgs& A, int ci) {
       __threadfence_block();
       __syncthreads();
     }
+    MF_PH(2);
     // old_state snapshot for the metrics (metrics_fn.py reads the pre-step
     // geometry): parked in the resident workspace arrays, which are only
     // rewritten with the live state at the end of the launch.
@@ -398,33 +431,24 @@ __device__ void run_condition(const StepArgs& A, int ci) {
       key_s[0] = kn[0];
       key_s[1] = kn[1];
     }
+    MF_PH(3);
     m.nearest(d_kin);
     __syncthreads();
+    MF_PH(4);
     const size_t inj_t = ((size_t)b * A.T + t) * (size_t)S;
     const size_t inj_x = ((size_t)b * A.T + t) * (size_t)X;
     m.thin_step(sub_thin, inj_t);
+    MF_PH(5);
     m.thick_step(sub_thick, inj_x);
+    MF_PH(6);
     // 5. mechanics
     double resid;
     int iters;
     float d = m.dyn ? cur_ls : ls_t;
-    float jdd_inv = 0.f;
-    if (m.dyn) {
-      // exact radial diagonal at the pre-solve point (solver.py:633-638)
-      float frad;
-      m.residual(zl, d, &frad);
-      float part = 0.f;
-      for (int i = m.tid; i < X; i += NT) {
-        float f, fx, fd, frd, fr;
-        m.xb_force(i, d, f, fx, fd, frd, fr);
-        part += frd;
-      }
-      if (m.tid < T.n_thick) part += m.s.tvec[3 * T.n_thick + m.tid];
-      const float ssum = m.bsum(part);
-      const float Jdd = -m.Kl - ssum;
-      jdd_inv = -1.0f / Jdd;
-    }
-    m.solve(zl, d, resid, iters, jdd_inv);
+    m.build_bound_list();
+    MF_PH(7);
+    m.solve(zl, d, resid, iters, m.dyn);
+    MF_PH(8);
     const float new_ls = m.dyn ? d : ls_t;
     if (m.tid == 0) ls_s = new_ls;
     // absorbing table for the metrics at (pCa, new_ls)
@@ -436,6 +460,7 @@ __device__ void run_condition(const StepArgs& A, int ci) {
       __threadfence_block();
     }
     __syncthreads();
+    MF_PH(9);
     // 6. force + metrics
     float force = 0.f;
     if (m.tid == 0) {
@@ -451,6 +476,7 @@ __device__ void run_condition(const StepArgs& A, int ci) {
     __syncthreads();
     metrics(m, t, zl, pCa, new_ls, force, resid, iters, xg, xbs_g, nullptr, xbn_g, xba_g, tm_g, Mo);
     if (resid > (double)A.resid_warn) m.status |= 2;
+    MF_PH(10);
     // optional traces
     if (A.x_trace) {
       float* xt = A.x_trace + ((size_t)b * A.T + t) * A.max_dof;
@@ -471,6 +497,13 @@ __device__ void run_condition(const StepArgs& A, int ci) {
     }
     __syncthreads();
   }
+  MF_PH(11);
+#ifdef MF_PHASE_TIMING
+  if (m.tid == 0 && A.x_trace) {
+    float* o = A.x_trace + (size_t)b * A.T * A.max_dof;
+    for (int k = 0; k < 12; ++k) o[k] = (float)ph_acc[k];
+  }
+#endif
   // ---- write back resident state ----
   for (int i = m.tid; i < N; i += NT) xg[i] = m.s.x[i];
   for (int i = m.tid; i < X; i += NT) {
@@ -497,8 +530,11 @@ __device__ void run_condition(const StepArgs& A, int ci) {
   }
 }
 
+// Register cap of 128 per thread (64 at 1024 threads) so that several
+// conditions share an SM; the table builder's 6x6 temporaries spill instead.
 template <int NT>
-__global__ void __launch_bounds__(NT) step_kernel(StepArgs A, int cond_base) {
+__global__ void __launch_bounds__(NT, (65536 / (NT * 128)) > 0 ? 65536 / (NT * 128) : 1)
+    step_kernel(StepArgs A, int cond_base) {
   run_condition<NT>(A, cond_base + blockIdx.x);
 }
 

@@ -106,6 +106,11 @@ struct Smem {
   float* red;     // reduction scratch [64]
   double* redd;   // [64]
   float* tvec;    // [4*n_thick] titin partials
+  float* fdd;     // [X] df/dd per head (dynamic spacing)
+  float* frdd;    // [X] d(radial)/dd per head (dynamic spacing)
+  int16_t* blist; // [X] heads carrying force this step, increasing index
+  int* nbound;    // [1] length of blist
+  int* wsum;      // [32] per-warp counts of the compaction scan
 };
 
 // Thomas coefficient block layout inside coef (floats).
@@ -143,6 +148,7 @@ struct Sim {
   float d_ref;
   int status;
   int Tstride;
+  int redbuf = 0;
 
   __device__ Sim(const TopoDev& t, const StepArgs& a) : T(t), A(a) {}
 
@@ -273,11 +279,27 @@ struct Sim {
     }
   }
 
-  // out = M^{-1} in for every filament (warp per filament).
-  __device__ void precondition(const float* in, float* out) {
+  // Node ownership: warp w owns filaments w, w + NW, ...; lane l handles
+  // nodes l, l + 32, ... of each.  Every elementwise vector update and the
+  // Thomas solves stay inside a warp, so only the crossbridge coupling and
+  // the dot products need block barriers.
+  template <class Fn>
+  __device__ __forceinline__ void own_nodes(Fn&& fn) const {
+    const int nf = T.n_thick + T.n_thin;
+    for (int f = warp; f < nf; f += NW) {
+      const bool thick = f < T.n_thick;
+      const int n = thick ? T.n_crowns : T.n_sites;
+      const int base = thick ? f * T.n_crowns : T.n_thick_nodes + (f - T.n_thick) * T.n_sites;
+      for (int j = lane; j < n; j += 32) fn(base + j, f, j, thick);
+    }
+  }
+
+  // out = M^{-1} in on this warp's own filaments (no block barrier needed).
+  __device__ void precondition_own(const float* in, float* out) {
     const int nf = T.n_thick + T.n_thin;
     float* buf = s.scan + warp * (T.plan_thin.total > T.plan_thick.total ? T.plan_thin.total
                                                                           : T.plan_thick.total);
+    __syncwarp();
     for (int f = warp; f < nf; f += NW) {
       const bool thick = f < T.n_thick;
       const int n = thick ? T.n_crowns : T.n_sites;
@@ -300,6 +322,26 @@ struct Sim {
       scan_b(pl, Ab, buf);
       for (int i = lane; i < n; i += 32) out[base + i] = buf[n - 1 - i];
       __syncwarp();
+    }
+  }
+
+  // One-barrier block reduction of K floats (sum) with an optional max in
+  // slot 0; double-buffered so consecutive reductions need no extra barrier.
+  template <int K>
+  __device__ __forceinline__ void reduce(float (&v)[K], bool max0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = (max0 && k == 0) ? warp_max(v[k]) : warp_sum(v[k]);
+    float* rb = s.red + 512 + redbuf * 96;  // clear of bsum_* (red[0, 512)) and red[767]
+    redbuf ^= 1;
+    if (lane == 0)
+#pragma unroll
+      for (int k = 0; k < K; ++k) rb[k * NW + warp] = v[k];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      float t = rb[k * NW];
+      for (int w = 1; w < NW; ++w) t = (max0 && k == 0) ? fmaxf(t, rb[k * NW + w]) : t + rb[k * NW + w];
+      v[k] = t;
     }
   }
 
@@ -399,21 +441,89 @@ struct Sim {
     rad = 6.0f * Ft * (d / Ls);
   }
 
-  // Residual F(x) into s.r; also caches df/dx per head (s.fdx) and titin
-  // partials (s.tvec) for the JVPs of the next Newton iteration.  Returns
-  // max|F| (float64 in precise mode) and the radial residual in *frad.
-  __device__ double residual(float zl, float d, float* frad) {
-    const int X = T.total_xbs, S = T.n_sites_total, N = T.n_dof;
-    float rad_part = 0.f;
-    for (int i = tid; i < S; i += NT) s.site[i] = 0.f;
+  // Compact list of the heads that carry force this step (states 1-3 with a
+  // site), in increasing head index (block prefix scan, deterministic), plus
+  // the number of heads on every site.  Clears the per-head and per-site
+  // accumulators.  Sites holding 3+ heads are summed in head order by their
+  // node owner (sums of two are order-free; the reference adds in index
+  // order, transitions/forces.py segment_sum).
+  __device__ void build_bound_list() {
+    const int X = T.total_xbs, S = T.n_sites_total;
+    int* cnt = s.win2;
     __syncthreads();
-    for (int i = tid; i < X; i += NT) {
+    for (int g = tid; g < S; g += NT) {
+      s.site[g] = 0.f;
+      cnt[g] = 0;
+    }
+    __syncthreads();
+    int base = 0;
+    for (int c = 0; c < X; c += NT) {
+      const int i = c + tid;
+      bool f = false;
+      if (i < X) {
+        s.fxb[i] = 0.f;
+        const int st = s.xb_state[i];
+        f = st >= 1 && st <= 3 && s.xb_bound[i] >= 0;
+        if (f) atomicAdd(&cnt[thin_of(i) * T.n_sites + s.xb_bound[i]], 1);
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, f);
+      if (lane == 0) s.wsum[warp] = __popc(m);
+      __syncthreads();
+      int off = base, tot = 0;
+      for (int w = 0; w < NW; ++w) {
+        const int v = s.wsum[w];
+        off += w < warp ? v : 0;
+        tot += v;
+      }
+      if (f) s.blist[off + __popc(m & ((1u << lane) - 1u))] = (int16_t)i;
+      base += tot;
+      __syncthreads();
+    }
+    if (tid == 0) *s.nbound = base;
+    __syncthreads();
+  }
+
+  // crossbridge sum of a site with 3+ bound heads: -sum of fxb in head order
+  __device__ float ordered_site_sum(int g) const {
+    const int nb = *s.nbound;
+    float acc = 0.f;
+    int prev = -1;
+    while (true) {
+      int nxt = 0x7fffffff;
+      for (int k = 0; k < nb; ++k) {
+        const int i = s.blist[k];
+        if (i > prev && i < nxt && thin_of(i) * T.n_sites + s.xb_bound[i] == g) nxt = i;
+      }
+      if (nxt == 0x7fffffff) break;
+      acc = acc + (-s.fxb[nxt]);
+      prev = nxt;
+    }
+    return acc;
+  }
+
+  // Residual F(x) into s.r (own nodes); caches df/dx per bound head and the
+  // titin partials for the JVPs of the next Newton iteration.  Returns max|F|
+  // over the augmented vector; *frad = radial residual, *jdd = dF_rad/dd.
+  // In precise mode the node forces are accumulated in float64.
+  __device__ float residual(float zl, float d, float* frad, float* jdd, int bad_in, int* bad_out) {
+    const int nb = *s.nbound;
+    float rad_part = 0.f, jdd_part = 0.f;
+    const int any_bad = __syncthreads_or(bad_in);
+    if (bad_out) *bad_out = any_bad;
+    for (int k = tid; k < nb; k += NT) {
+      const int i = s.blist[k];
       float f, fx, fd, frd, fr;
       xb_force(i, d, f, fx, fd, frd, fr);
       s.fxb[i] = f;
       s.fdx[i] = fx;
-      if (dyn) rad_part += fr;
-      if (f != 0.f) atomicAdd(&s.site[thin_of(i) * T.n_sites + (s.xb_bound[i] < 0 ? 0 : s.xb_bound[i])], -f);
+      if (dyn) {
+        s.fdd[i] = fd;
+        s.frdd[i] = frd;
+        rad_part += fr;
+        jdd_part += frd;
+      }
+      const int gs = thin_of(i) * T.n_sites + s.xb_bound[i];
+      if (s.win2[gs] < 3) atomicAdd(&s.site[gs], -f);
     }
     if (tid < T.n_thick) {
       float ax, a_x, a_d, r_d, rad;
@@ -422,97 +532,82 @@ struct Sim {
       s.tvec[T.n_thick + tid] = a_x;
       s.tvec[2 * T.n_thick + tid] = a_d;
       s.tvec[3 * T.n_thick + tid] = r_d;
-      if (dyn) rad_part += rad;
+      if (dyn) {
+        rad_part += rad;
+        jdd_part += r_d;
+      }
     }
     __syncthreads();
     const float kth = s.P[THICK_K], ktn = s.P[THIN_K];
-    double fmax = 0.0;
-    for (int i = tid; i < N; i += NT) {
+    float fmax = 0.f;
+    own_nodes([&](int i, int f, int j, bool thick) {
       double F;
-      if (i < T.n_thick_nodes) {
-        const int t = i / T.n_crowns, c = i % T.n_crowns;
-        const int base = t * T.n_crowns;
-        float sp_c, sp_n;
+      if (thick) {
+        const int c = j;
         float xsum = s.fxb[i * T.nxb];
-        for (int j = 1; j < T.nxb; ++j) xsum += s.fxb[i * T.nxb + j];
+        for (int q = 1; q < T.nxb; ++q) xsum += s.fxb[i * T.nxb + q];
         if (!precise) {
           const float xm = c > 0 ? s.x[i - 1] : 0.f;
-          sp_c = ((s.x[i] - xm) - T.crown_rest[i]) * kth;
-          sp_n = (c + 1 < T.n_crowns) ? ((s.x[i + 1] - s.x[i]) - T.crown_rest[i + 1]) * kth : s.tvec[t];
+          const float sp_c = ((s.x[i] - xm) - T.crown_rest[i]) * kth;
+          const float sp_n = (c + 1 < T.n_crowns) ? ((s.x[i + 1] - s.x[i]) - T.crown_rest[i + 1]) * kth : s.tvec[f];
           F = (double)((sp_n - sp_c) + xsum);
         } else {
           const double um = c > 0 ? (double)s.x[i - 1] : 0.0;
           const double e_c = ((double)s.x[i] - um) + (double)T.thick_c[i];
-          const double e_n = (c + 1 < T.n_crowns) ? ((double)s.x[i + 1] - (double)s.x[i]) + (double)T.thick_c[i + 1]
-                                                  : 0.0;
-          const double spn = (c + 1 < T.n_crowns) ? e_n * (double)kth : (double)s.tvec[t];
+          const double spn = (c + 1 < T.n_crowns)
+                                 ? (((double)s.x[i + 1] - (double)s.x[i]) + (double)T.thick_c[i + 1]) * (double)kth
+                                 : (double)s.tvec[f];
           F = (spn - e_c * (double)kth) + (double)xsum;
-          (void)base;
         }
       } else {
         const int g = i - T.n_thick_nodes;
-        const int j = g % T.n_sites;
+        const float acc = s.win2[g] < 3 ? s.site[g] : ordered_site_sum(g);
+        s.site[g] = 0.f;
         if (!precise) {
           const float xn = (j + 1 < T.n_sites) ? s.x[i + 1] : zl;
           const float sp_j = ((xn - s.x[i]) - T.bind_rest[g]) * ktn;
           const float sp_m = j > 0 ? ((s.x[i] - s.x[i - 1]) - T.bind_rest[g - 1]) * ktn : 0.f;
-          F = (double)((sp_j - sp_m) + s.site[g]);
+          F = (double)((sp_j - sp_m) + acc);
         } else {
           const double un = (j + 1 < T.n_sites) ? (double)s.x[i + 1] : 0.0;
           double e_j = (un - (double)s.x[i]) + (double)T.thin_c[g];
           if (j + 1 == T.n_sites) e_j += (double)zl - zref;  // anchor vs reference z
           const double e_m = j > 0 ? ((double)s.x[i] - (double)s.x[i - 1]) + (double)T.thin_c[g - 1] : 0.0;
-          F = (e_j - e_m) * (double)ktn + (double)s.site[g];
+          F = (e_j - e_m) * (double)ktn + (double)acc;
         }
       }
       s.r[i] = (float)F;
-      fmax = fmax > fabs(F) ? fmax : fabs(F);
-    }
+      fmax = fmaxf(fmax, (float)fabs(F));
+    });
+    float v[3] = {fmax, rad_part, jdd_part};
+    reduce<3>(v, true);
+    float m = v[0];
     if (dyn) {
-      const float rs = bsum(rad_part);
-      const float Fr = -Kl * (d - d_ref) + (-rs);
+      const float Fr = -Kl * (d - d_ref) + (-v[1]);
       *frad = Fr;
-      fmax = fmax > fabs((double)Fr) ? fmax : fabs((double)Fr);
-    }
-    // block max of fmax (as float bits for the reference path, double in precise)
-    double m = (double)bmax((float)fmax);
-    if (precise) {
-      // exact double max through the double scratch
-      double v = fmax;
-      for (int o = 16; o > 0; o >>= 1) v = fmax_d(v, __shfl_xor_sync(0xffffffffu, v, o));
-      __syncthreads();
-      if (lane == 0) s.redd[warp] = v;
-      __syncthreads();
-      m = s.redd[0];
-      for (int w = 1; w < NW; ++w) m = fmax_d(m, s.redd[w]);
+      m = fmaxf(m, fabsf(Fr));
+      if (jdd) *jdd = -Kl - v[2];
     }
     return m;
   }
-  static __device__ __forceinline__ double fmax_d(double a, double b) { return a > b ? a : b; }
 
-  // out = -(J [v, vd]); returns dot(v_full, out_full) and sets *out_d.
-  __device__ float neg_jvp(const float* v, float vd, float* out, float* out_d, float d) {
-    const int X = T.total_xbs, S = T.n_sites_total, N = T.n_dof;
+  // out = -(J [v, vd]) on own nodes; returns the augmented dot(v, out), *out_d
+  // the radial component.
+  __device__ float neg_jvp(const float* v, float vd, float* out, float* out_d) {
+    const int nb = *s.nbound;
     float rad_part = 0.f;
-    for (int i = tid; i < S; i += NT) s.site[i] = 0.f;
-    __syncthreads();
-    for (int i = tid; i < X; i += NT) {
-      float w = 0.f;
-      const int bnd = s.xb_bound[i];
-      const int st = s.xb_state[i];
-      if (st >= 1 && st <= 3 && bnd >= 0) {
-        const int gs = thin_of(i) * T.n_sites + bnd;
-        const float dxd = v[T.n_thick_nodes + gs] - v[crown_node(i)];
-        w = s.fdx[i] * dxd;
-        if (dyn) {
-          float f, fx, fd, frd, fr;
-          xb_force(i, d, f, fx, fd, frd, fr);
-          w = w + fd * vd;
-          rad_part += -(fd * dxd) - frd * vd;
-        }
-        if (w != 0.f) atomicAdd(&s.site[gs], -w);
+    __syncthreads();  // v complete
+    for (int k = tid; k < nb; k += NT) {
+      const int i = s.blist[k];
+      const int gs = thin_of(i) * T.n_sites + s.xb_bound[i];
+      const float dxd = v[T.n_thick_nodes + gs] - v[crown_node(i)];
+      float w = s.fdx[i] * dxd;
+      if (dyn) {
+        w = w + s.fdd[i] * vd;
+        rad_part += -(s.fdd[i] * dxd) - s.frdd[i] * vd;
       }
       s.fxb[i] = w;
+      if (s.win2[gs] < 3) atomicAdd(&s.site[gs], -w);
     }
     if (dyn && tid < T.n_thick) {
       const int last = tid * T.n_crowns + T.n_crowns - 1;
@@ -521,110 +616,102 @@ struct Sim {
     __syncthreads();
     const float kth = s.P[THICK_K], ktn = s.P[THIN_K];
     float dot = 0.f;
-    for (int i = tid; i < N; i += NT) {
+    own_nodes([&](int i, int f, int j, bool thick) {
       float J;
-      if (i < T.n_thick_nodes) {
-        const int t = i / T.n_crowns, c = i % T.n_crowns;
-        const float vm = c > 0 ? v[i - 1] : 0.f;
+      if (thick) {
+        const float vm = j > 0 ? v[i - 1] : 0.f;
         const float sc = (v[i] - vm) * kth;
         float sn;
-        if (c + 1 < T.n_crowns) sn = (v[i + 1] - v[i]) * kth;
+        if (j + 1 < T.n_crowns) sn = (v[i + 1] - v[i]) * kth;
         else {
-          sn = s.tvec[T.n_thick + t] * v[i];
-          if (dyn) sn = sn + s.tvec[2 * T.n_thick + t] * vd;
+          sn = s.tvec[T.n_thick + f] * v[i];
+          if (dyn) sn = sn + s.tvec[2 * T.n_thick + f] * vd;
         }
         float xs = s.fxb[i * T.nxb];
-        for (int j = 1; j < T.nxb; ++j) xs += s.fxb[i * T.nxb + j];
+        for (int q = 1; q < T.nxb; ++q) xs += s.fxb[i * T.nxb + q];
         J = (sn - sc) + xs;
       } else {
         const int g = i - T.n_thick_nodes;
-        const int j = g % T.n_sites;
         const float vn = (j + 1 < T.n_sites) ? v[i + 1] : 0.f;
         const float sj = (vn - v[i]) * ktn;
         const float sm = j > 0 ? (v[i] - v[i - 1]) * ktn : 0.f;
-        J = (sj - sm) + s.site[g];
+        J = (sj - sm) + (s.win2[g] < 3 ? s.site[g] : ordered_site_sum(g));
+        s.site[g] = 0.f;
       }
       const float o = -J;
       out[i] = o;
       dot = fmaf(v[i], o, dot);
-    }
+    });
+    float r2[2] = {dot, rad_part};
+    reduce<2>(r2, false);
     if (dyn) {
-      float pair[2] = {dot, rad_part};
-      bsum_k<2>(pair);
-      const float od = -((pair[1]) + (-Kl) * vd);
+      const float od = -(r2[1] + (-Kl) * vd);
       *out_d = od;
-      return pair[0] + vd * od;
+      return r2[0] + vd * od;
     }
-    return bsum(dot);
+    return r2[0];
   }
 
   // ------------------------------------------------------------------
   // Newton-CG (solver.py:329-427, 599-656)
   // ------------------------------------------------------------------
-  __device__ void solve(float zl, float& d, double& resid, int& iters, float J_dd_inv) {
-    const int N = T.n_dof;
+  __device__ void solve(float zl, float& d, double& resid, int& iters, bool dyn_jdd) {
     const float tol = fmaxf(s.P[SOLVER_TOL], fmaxf(s.P[THICK_K] * 1e-4f, 0.25f));
-    float frad = 0.f;
-    double fmx = residual(zl, d, &frad);
-    int it = 0;
-    while (fmx > (double)tol && it < A.n_newton) {
-      // CG on -J dx = F from dx = 0  (r = F, p = z = M r)
+    float frad = 0.f, jdd = 0.f;
+    float fmx = residual(zl, d, &frad, &jdd, 0, nullptr);
+    // exact radial diagonal at the pre-solve point (solver.py:633-638)
+    const float J_dd_inv = dyn_jdd ? -1.0f / jdd : 0.f;
+    int it = 0, bad = 0;
+    while (fmx > tol && it < A.n_newton) {
       float r_d = frad, z_d = 0.f, p_d = 0.f, dx_d = 0.f, Ap_d = 0.f;
-      __syncthreads();
-      precondition(s.r, s.zz);
-      __syncthreads();
-      float part = 0.f;
-      for (int i = tid; i < N; i += NT) {
+      precondition_own(s.r, s.zz);
+      float part[1] = {0.f};
+      own_nodes([&](int i, int, int, bool) {
         s.pv[i] = s.zz[i];
-        s.dx[i] = 0.f;
-        part = fmaf(s.r[i], s.zz[i], part);
-      }
+        s.dx[i] = A.n_cg == 0 ? s.zz[i] : 0.f;
+        part[0] = fmaf(s.r[i], s.zz[i], part[0]);
+      });
       if (dyn) {
         z_d = J_dd_inv * r_d;
         p_d = z_d;
+        if (A.n_cg == 0) dx_d = z_d;
       }
-      float rz = bsum(part) + (dyn ? r_d * z_d : 0.f);
-      if (A.n_cg == 0) {
-        for (int i = tid; i < N; i += NT) s.dx[i] = s.zz[i];
-        dx_d = z_d;
-      }
+      reduce<1>(part, false);
+      float rz = part[0] + (dyn ? r_d * z_d : 0.f);
       for (int k = 0; k < A.n_cg; ++k) {
-        __syncthreads();
-        const float pAp = neg_jvp(s.pv, p_d, s.zz, &Ap_d, d);
+        const float pAp = neg_jvp(s.pv, p_d, s.zz, &Ap_d);
         const float alpha = rz / (pAp + 1e-30f);
-        for (int i = tid; i < N; i += NT) {
+        own_nodes([&](int i, int, int, bool) {
           s.dx[i] = fmaf(alpha, s.pv[i], s.dx[i]);
           s.r[i] = s.r[i] - alpha * s.zz[i];
-        }
+        });
         dx_d = fmaf(alpha, p_d, dx_d);
         r_d = r_d - alpha * Ap_d;
-        __syncthreads();
-        precondition(s.r, s.zz);
-        __syncthreads();
-        float rzp = 0.f;
-        for (int i = tid; i < N; i += NT) rzp = fmaf(s.r[i], s.zz[i], rzp);
+        precondition_own(s.r, s.zz);
+        float rzp[1] = {0.f};
+        own_nodes([&](int i, int, int, bool) { rzp[0] = fmaf(s.r[i], s.zz[i], rzp[0]); });
         if (dyn) z_d = J_dd_inv * r_d;
-        const float rz_new = bsum(rzp) + (dyn ? r_d * z_d : 0.f);
+        reduce<1>(rzp, false);
+        const float rz_new = rzp[0] + (dyn ? r_d * z_d : 0.f);
         const float beta = rz_new / (rz + 1e-30f);
-        for (int i = tid; i < N; i += NT) s.pv[i] = fmaf(beta, s.pv[i], s.zz[i]);
+        own_nodes([&](int i, int, int, bool) { s.pv[i] = fmaf(beta, s.pv[i], s.zz[i]); });
         p_d = fmaf(beta, p_d, z_d);
         rz = rz_new;
       }
-      __syncthreads();
       // x += dx with non-finite entries zeroed
-      int bad = 0;
-      for (int i = tid; i < N; i += NT) {
+      int bad_local = 0;
+      own_nodes([&](int i, int, int, bool) {
         float v = s.dx[i];
-        if (!isfinite(v)) { v = 0.f; bad = 1; }
+        if (!isfinite(v)) { v = 0.f; bad_local = 1; }
         s.x[i] = s.x[i] + v;
-      }
+      });
       if (dyn) {
         float v = dx_d;
         if (!isfinite(v)) v = 0.f;
         d = fmaxf(d + v, 1.0f);
       }
-      if (__syncthreads_or(bad)) status |= MF_NONFINITE_BIT;
-      fmx = residual(zl, d, &frad);
+      fmx = residual(zl, d, &frad, nullptr, bad_local, &bad);
+      if (bad) status |= MF_NONFINITE_BIT;
       ++it;
     }
     resid = fmx;

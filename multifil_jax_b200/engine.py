@@ -309,3 +309,46 @@ def get_engine(device: Optional[int] = None) -> Engine:
     if d not in _engines:
         _engines[d] = Engine(d)
     return _engines[d]
+
+
+def _flags_for(plan, precision: str) -> int:
+    f = 0
+    if plan.dynamic_ls:
+        f |= MF_FLAG_DYNAMIC_LS
+    if precision == 'mixed':
+        f |= MF_FLAG_PRECISE
+    return f
+
+
+def execute_plan(topology, plan, static_params, precision: str = 'float32', device: Optional[int] = None,
+                 minibatch_size="auto", chunk_steps: int = 0, stream=None) -> np.ndarray:
+    """Run every condition of a BatchPlan on the GPU; returns host metrics [B, 52, T]."""
+    torch = _torch()
+    eng = get_engine(device)
+    dev = torch.device('cuda', eng.device)
+    B, T = plan.total, plan.n_steps
+    out = np.zeros((B, N_METRICS, T), dtype=np.float32)
+    if B == 0 or T == 0:
+        return out
+    if minibatch_size in (None, "auto"):
+        chunk = B
+    else:
+        chunk = max(1, int(minibatch_size))
+    flags = _flags_for(plan, precision)
+    with torch.cuda.device(dev):
+        for s in range(0, B, chunk):
+            e = min(B, s + chunk)
+            n = e - s
+
+            def dv(a, dt=torch.float32):
+                return torch.as_tensor(np.ascontiguousarray(a[s:e]), device=dev).to(dt).contiguous()
+            keys = torch.as_tensor(plan.keys[s:e].astype(np.int64), device=dev).to(torch.int32).contiguous()
+            res = eng.run_batch([topology] * n, dv(plan.params), dv(plan.z), dv(plan.pCa), dv(plan.ls),
+                                torch.full((n,), T, dtype=torch.int32, device=dev), keys,
+                                K_lat=dv(plan.K_lat), nu=dv(plan.nu),
+                                dt=torch.full((n,), plan.dt, dtype=torch.float32, device=dev),
+                                n_newton=static_params.n_newton_steps, n_cg=static_params.n_cg_steps,
+                                flags=flags, chunk_steps=chunk_steps,
+                                residual_warn=static_params.solver_residual_tol, stream=stream)
+            out[s:e] = res['metrics'].cpu().numpy()
+    return out

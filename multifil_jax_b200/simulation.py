@@ -1,0 +1,461 @@
+"""``run()`` and ``SimulationResult``: the reference's public entry point on the CUDA engine.
+
+Mirrors ``multifil_jax/simulation.py:754-1165`` (sweep expansion, per-field
+parameter tables, key split, Poisson lattice-spacing pre-computation, result
+data cube, residual warning) and ``:96-420`` (``SimulationResult`` with
+``sel``/``mean``/``std``/``stack``/indexing).  The per-condition time loop --
+the reference's ``jit(vmap(scan(timestep)))`` -- runs in the fused sm_100a
+kernel through :mod:`multifil_jax_b200.engine`; there is no CPU path.
+
+Sweep axes are Cartesian-producted in the reference's fixed order (z_line,
+pCa, lattice_spacing, K_lat, nu, dynamic_params fields / candidates) and
+results come back shaped ``(sweep_1, ..., replicates, time)``.
+"""
+from __future__ import annotations
+
+import warnings
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Tuple, Union
+
+import numpy as np
+
+from .params import DYNAMIC_FIELDS, DynamicParams, StaticParams, N_PARAMS
+from .topology import SarcTopology
+
+METRIC_KEYS = (
+    'axial_force', 'solver_residual', 'z_line', 'pCa', 'lattice_spacing',
+    'n_bound', 'n_xb_drx', 'n_xb_loose', 'n_xb_tight_1', 'n_xb_tight_2', 'n_xb_free_2', 'n_xb_srx',
+    'frac_xb_bound', 'frac_xb_drx', 'frac_xb_loose', 'frac_xb_tight_1', 'frac_xb_tight_2',
+    'frac_xb_free_2', 'frac_xb_srx',
+    'n_tm_state_0', 'n_tm_state_1', 'n_tm_state_2', 'n_tm_state_3',
+    'frac_tm_state_0', 'frac_tm_state_1', 'frac_tm_state_2', 'frac_tm_state_3',
+    'actin_permissiveness', 'frac_tm_state_2_overlap', 'frac_tm_state_3_overlap',
+    'frac_tm_available_overlap', 'n_overlap_sites',
+    'atp_consumed', 'newly_bound',
+    'thick_displace_mean', 'thick_displace_max', 'thick_displace_min', 'thick_displace_std',
+    'thin_displace_mean', 'thin_displace_max', 'thin_displace_min', 'thin_displace_std',
+    'thick_energy_first_avg', 'thick_energy_first_delta_avg', 'titin_energy_avg', 'titin_energy_delta_avg',
+    'work_thick', 'work_thick_mean', 'atp_expected_p', 'xb_tear_expected', 'work_per_atp', 'newton_iters')
+
+BATCH_BUCKETS = (1, 2, 4, 8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096, 8192, 16384)
+
+PRECISIONS = ('float32', 'mixed')
+
+
+class MetricsDict(dict):
+    """dict with attribute access (reference ``core/state.py:118-130``)."""
+
+    def __getattr__(self, key):
+        try:
+            return self[key]
+        except KeyError:
+            raise AttributeError(key)
+
+
+def get_bucket_size(actual_size: int) -> int:
+    """Next power-of-two bucket (reference ``simulation.py:434-450``).
+
+    The CUDA engine needs no shape buckets; this is kept because the
+    reference's returned ``rng_key`` is the last key of the padded batch.
+    """
+    for b in BATCH_BUCKETS:
+        if b >= actual_size:
+            return b
+    return actual_size
+
+
+class SimulationResult:
+    """Result container of :func:`run` (reference ``simulation.py:96-420``).
+
+    ``metrics`` maps each of the 52 metric names to a numpy array shaped
+    ``grid_shape + (replicates, n_steps)`` (``newton_iters`` int32, the rest
+    float32).
+    """
+
+    __slots__ = ('metrics', 'rng_key', 'z_line', 'pCa', 'lattice_spacing', 'final_state', 'metadata',
+                 'dt', 'name', '_grid_shape', '_axis_names', 'coords', 'topology_config')
+
+    def __init__(self, metrics, rng_key, z_line, pCa, lattice_spacing, final_state=None, metadata=None,
+                 dt=1.0, name="", grid_shape=None, axis_names=None, coords=None, topology_config=None):
+        self.metrics = metrics if isinstance(metrics, MetricsDict) else MetricsDict(metrics)
+        self.rng_key = rng_key
+        self.z_line = z_line
+        self.pCa = pCa
+        self.lattice_spacing = lattice_spacing
+        self.final_state = final_state
+        self.metadata = metadata if metadata is not None else {}
+        self.dt = float(dt)
+        self.name = str(name)
+        self._grid_shape = grid_shape
+        self._axis_names = axis_names if axis_names is not None else []
+        self.coords = coords if coords is not None else {}
+        self.topology_config = topology_config if topology_config is not None else {}
+
+    @property
+    def n_steps(self) -> int:
+        return self.metrics['axial_force'].shape[-1]
+
+    @property
+    def replicate_axis(self) -> Optional[int]:
+        return self._axis_names.index('replicates') if 'replicates' in self._axis_names else None
+
+    @property
+    def time(self) -> np.ndarray:
+        return np.arange(self.n_steps) * self.dt
+
+    @property
+    def axial_force(self) -> np.ndarray:
+        return self.metrics['axial_force']
+
+    @property
+    def mean_force(self) -> float:
+        return float(np.mean(self.metrics['axial_force']))
+
+    @property
+    def steady_state_force(self) -> float:
+        n_avg = max(1, self.n_steps // 5)
+        return float(np.mean(self.metrics['axial_force'][..., -n_avg:]))
+
+    def _reduce_replicates(self, fn, suffix: str) -> 'SimulationResult':
+        if self.replicate_axis is None:
+            raise ValueError("No replicate axis to reduce.")
+        m = MetricsDict({k: fn(v, axis=-2) for k, v in self.metrics.items()})
+        coords = {k: v for k, v in self.coords.items() if k != 'replicates'}
+        names = [n for n in self._axis_names if n != 'replicates']
+        f = m['axial_force']
+        return SimulationResult(
+            metrics=m, rng_key=self.rng_key, z_line=np.mean(self.z_line, axis=-2),
+            pCa=np.mean(self.pCa, axis=-2), lattice_spacing=np.mean(self.lattice_spacing, axis=-2),
+            final_state=None, metadata=self.metadata, dt=self.dt, name=self.name + suffix,
+            grid_shape=f.shape[:-1] if f.ndim > 1 else None, axis_names=names, coords=coords)
+
+    def mean(self) -> 'SimulationResult':
+        return self._reduce_replicates(np.mean, "_mean")
+
+    def std(self) -> 'SimulationResult':
+        return self._reduce_replicates(np.std, "_std")
+
+    def __getitem__(self, key) -> 'SimulationResult':
+        m = MetricsDict({k: v[key] for k, v in self.metrics.items()})
+        f = m['axial_force']
+        keys = key if isinstance(key, tuple) else (key,)
+        names = list(self._axis_names)
+        coords = dict(self.coords)
+        pos = 0
+        opaque = False
+        for k in keys:
+            if pos >= len(self._axis_names):
+                break
+            nm = self._axis_names[pos]
+            if isinstance(k, (int, np.integer)):
+                if nm in names:
+                    names.remove(nm)
+                coords.pop(nm, None)
+            elif isinstance(k, slice):
+                if nm in coords:
+                    try:
+                        coords[nm] = list(coords[nm])[k]
+                    except Exception:
+                        opaque = True
+            else:
+                opaque = True
+            pos += 1
+        if opaque:
+            names = list(self._axis_names)
+            coords = dict(self.coords)
+        return SimulationResult(
+            metrics=m, rng_key=self.rng_key, z_line=self.z_line[key], pCa=self.pCa[key],
+            lattice_spacing=self.lattice_spacing[key], final_state=None, metadata=self.metadata,
+            dt=self.dt, name=self.name, grid_shape=f.shape[:-1] if f.ndim > 1 else None,
+            axis_names=names, coords=coords)
+
+    def summary(self) -> str:
+        lines = [
+            f"SimulationResult: {self.name}",
+            f"  Shape: {self.axial_force.shape}",
+            f"  Duration: {self.n_steps * self.dt:.1f} ms ({self.n_steps} steps @ dt={self.dt}ms)",
+            f"  Mean force: {self.mean_force:.2f} pN",
+            f"  Steady-state force: {self.steady_state_force:.2f} pN",
+            f"  Metrics: {list(self.metrics.keys()) if self.metrics else 'none'}",
+            f"  Max solver residual: {float(np.max(self.metrics['solver_residual'])):.4f} pN",
+        ]
+        if self._axis_names:
+            lines.append(f"  Grid axes: {self._axis_names}")
+        if self.coords:
+            lines.append(f"  Coords: {list(self.coords.keys())}")
+        return '\n'.join(lines)
+
+    def sel(self, **kwargs) -> 'SimulationResult':
+        idx = [slice(None)] * self.axial_force.ndim
+        names = list(self._axis_names)
+        coords = dict(self.coords)
+        for name, value in kwargs.items():
+            if name not in self.coords:
+                raise ValueError(f"Unknown axis '{name}'. Available: {list(self.coords.keys())}")
+            cl = self.coords[name]
+            if value not in cl:
+                raise ValueError(f"Value {value} not in {name} coords: {cl}")
+            idx[self._axis_names.index(name)] = cl.index(value)
+        out = self[tuple(idx)]
+        for name in kwargs:
+            if name in names:
+                names.remove(name)
+            coords.pop(name, None)
+        out._axis_names = names
+        out.coords = coords
+        return out
+
+    @classmethod
+    def stack(cls, results: List['SimulationResult'], axis_name: str = 'structural',
+              axis_values: Optional[List] = None) -> 'SimulationResult':
+        if not results:
+            raise ValueError("Cannot stack empty list of results")
+        keys = list(results[0].metrics.keys())
+        m = MetricsDict({k: np.stack([r.metrics[k] for r in results]) for k in keys})
+        coords = dict(results[0].coords)
+        coords[axis_name] = axis_values if axis_values is not None else list(range(len(results)))
+        return cls(metrics=m, rng_key=results[-1].rng_key,
+                   z_line=np.stack([r.z_line for r in results]), pCa=np.stack([r.pCa for r in results]),
+                   lattice_spacing=np.stack([r.lattice_spacing for r in results]), final_state=None,
+                   metadata=results[0].metadata, dt=results[0].dt, name=results[0].name + "_stacked",
+                   grid_shape=m['axial_force'].shape[:-1], axis_names=[axis_name] + results[0]._axis_names,
+                   coords=coords)
+
+    def __repr__(self) -> str:
+        f = self.metrics.get('axial_force')
+        return f"SimulationResult(name='{self.name}', shape={getattr(f, 'shape', '?')}, dt={self.dt})"
+
+
+# ---------------------------------------------------------------------------
+# sweep expansion (host glue; simulation.py:848-1048)
+# ---------------------------------------------------------------------------
+
+@dataclass
+class BatchPlan:
+    """Every per-condition input of one run(), flattened to B = grid x replicates rows."""
+    n_steps: int
+    dt: float
+    params: np.ndarray        # [B, 44] float32
+    z: np.ndarray             # [B, T] float32
+    pCa: np.ndarray
+    ls: np.ndarray
+    keys: np.ndarray          # [B, 2] uint32
+    K_lat: np.ndarray         # [B] float32, already x n_thick when dynamic
+    nu: np.ndarray            # [B] float32
+    dynamic_ls: bool
+    grid_shape: Tuple[int, ...]
+    replicates: int
+    axis_names: List[str]
+    coords: Dict[str, list]
+    rng_key: np.ndarray
+    topology_config: Dict = field(default_factory=dict)
+
+    @property
+    def total(self) -> int:
+        return self.params.shape[0]
+
+
+def _split_keys(seed: int, n: int) -> np.ndarray:
+    from .engine import prng_key, prng_split
+    if n == 0:
+        return np.zeros((0, 2), np.uint32)
+    return prng_split(prng_key(seed), n)
+
+
+def plan_batch(topology: SarcTopology, duration_ms: float = 1000.0, dt: float = 1.0,
+               pCa=4.5, z_line=900.0, lattice_spacing=14.0, K_lat=None, nu=0.0, dynamic_params=None,
+               static_params: Optional[StaticParams] = None, replicates: int = 1, rng_seed: int = 0,
+               subpopulation=None) -> BatchPlan:
+    """Expand run()'s arguments into per-condition arrays (no device work)."""
+    if subpopulation is not None:
+        raise NotImplementedError("subpopulations are not supported by multifil_jax_b200")
+    if replicates < 1:
+        raise ValueError("replicates must be >= 1")
+    n_steps = int(duration_ms / dt)
+    if dynamic_params is None or isinstance(dynamic_params, (dict, list)):
+        base = DynamicParams()
+    elif isinstance(dynamic_params, DynamicParams):
+        base = dynamic_params
+    else:
+        raise ValueError(f"dynamic_params must be DynamicParams, dict, or list, got {type(dynamic_params)}")
+    is_dyn = K_lat is not None
+
+    def as_trace(v):
+        a = np.asarray(v, dtype=float)
+        return np.full(n_steps, float(a)) if a.ndim == 0 else a
+
+    axes: List[Tuple[str, list]] = []
+    wf_tables: Dict[str, np.ndarray] = {}
+    wf_sweeps = set()
+    ptables: Dict[str, np.ndarray] = {}
+    paxis: Dict[str, str] = {}
+    for name, value in (('z_line', z_line), ('pCa', pCa), ('lattice_spacing', lattice_spacing)):
+        if isinstance(value, list):
+            if not value:
+                raise ValueError(f"{name} sweep list is empty")
+            rows = [as_trace(v) for v in value]
+            if any(r.shape != (n_steps,) for r in rows):
+                raise ValueError(f"{name} trace length != n_steps {n_steps}")
+            wf_tables[name] = np.stack(rows).astype(np.float32)
+            trace_sweep = any(not isinstance(v, (int, float)) and np.asarray(v).ndim == 1
+                              and len(np.asarray(v)) == n_steps for v in value)
+            coords = ([np.asarray(wf_tables[name][i]) for i in range(len(value))] if trace_sweep
+                      else list(value))
+            axes.append((name, coords))
+            wf_sweeps.add(name)
+        else:
+            arr = np.asarray(value)
+            if arr.ndim > 0 and arr.shape[0] != n_steps:
+                raise ValueError(f"{name} array length {arr.shape[0]} != n_steps {n_steps}")
+            wf_tables[name] = as_trace(value).astype(np.float32)[None, :]
+    if isinstance(K_lat, list):
+        axes.append(('K_lat', list(K_lat)))
+    if isinstance(nu, list):
+        axes.append(('nu', list(nu)))
+    if isinstance(dynamic_params, list):
+        if not dynamic_params:
+            raise ValueError("dynamic_params candidate list is empty")
+        axes.append(('candidates', list(range(len(dynamic_params)))))
+        for name in DYNAMIC_FIELDS:
+            ptables[name] = np.stack([np.asarray(getattr(dp, name), np.float32) for dp in dynamic_params])
+            paxis[name] = 'candidates'
+    elif isinstance(dynamic_params, dict):
+        for pname, pval in dynamic_params.items():
+            if pname not in DYNAMIC_FIELDS:
+                raise ValueError(f"Unknown dynamic_params field '{pname}'. Valid: {list(DYNAMIC_FIELDS)}")
+            if isinstance(pval, list):
+                axes.append((pname, list(pval)))
+                ptables[pname] = np.asarray(pval, np.float32)
+                paxis[pname] = pname
+    elif isinstance(dynamic_params, DynamicParams):
+        for name in DYNAMIC_FIELDS:
+            arr = np.asarray(getattr(dynamic_params, name))
+            if arr.ndim > 0 and arr.shape[0] > 1:
+                axes.append((name, list(arr.tolist())))
+                ptables[name] = arr.astype(np.float32)
+                paxis[name] = name
+
+    if axes:
+        grids = np.meshgrid(*[np.arange(len(c)) for _, c in axes], indexing='ij')
+        batch = grids[0].size
+        flat = {name: np.repeat(g.reshape(-1), replicates) for (name, _), g in zip(axes, grids)}
+    else:
+        batch = 1
+        flat = {}
+    total = batch * replicates
+    grid_shape = tuple(len(c) for _, c in axes)
+    axis_names = [n for n, _ in axes] + ['replicates', 'time']
+    coords = {n: c for n, c in axes}
+    coords['replicates'] = list(range(replicates))
+    coords['time'] = (np.arange(n_steps) * dt).tolist()
+
+    def wave(name):
+        tab = wf_tables[name]
+        if name in wf_sweeps:
+            return tab[flat[name]]
+        return np.broadcast_to(tab[0], (total, n_steps))
+    z_b = np.ascontiguousarray(wave('z_line'), dtype=np.float32)
+    p_b = np.ascontiguousarray(wave('pCa'), dtype=np.float32)
+    l_b = np.ascontiguousarray(wave('lattice_spacing'), dtype=np.float32)
+    if isinstance(K_lat, list):
+        K_b = np.asarray(K_lat, np.float32)[flat['K_lat']]
+    elif is_dyn:
+        K_b = np.full(total, float(K_lat), np.float32)
+    else:
+        K_b = np.zeros(total, np.float32)
+    if isinstance(nu, list):
+        nu_b = np.asarray(nu, np.float32)[flat['nu']]
+    else:
+        nu_b = np.full(total, float(nu), np.float32)
+    if is_dyn:
+        K_b = (K_b * np.float32(topology.n_thick)).astype(np.float32)
+    ls_is_trace = not isinstance(lattice_spacing, list) and np.asarray(lattice_spacing).ndim > 0
+    nonzero_nu = any(v != 0.0 for v in nu) if isinstance(nu, list) else float(nu) != 0.0
+    if not is_dyn and not ls_is_trace and nonzero_nu and n_steps > 0:
+        d0 = l_b[:, 0:1]
+        l_b = (d0 * (z_b[:, 0:1] / z_b) ** nu_b[:, None]).astype(np.float32)
+
+    def param(name):
+        if name in paxis:
+            return ptables[name][flat[paxis[name]]]
+        if isinstance(dynamic_params, dict) and name in dynamic_params:
+            return np.full(total, float(dynamic_params[name]), np.float32)
+        return np.full(total, float(np.asarray(getattr(base, name)).reshape(-1)[0]), np.float32)
+    params = np.stack([param(n) for n in DYNAMIC_FIELDS], axis=1).astype(np.float32)
+    assert params.shape == (total, N_PARAMS)
+    keys = _split_keys(rng_seed, total)
+    padded = get_bucket_size(total)
+    if padded > total:
+        last_key = _split_keys(rng_seed + 1, padded - total)[-1]
+    else:
+        last_key = keys[-1]
+    tcfg = {'n_thick': topology.n_thick, 'n_crowns': topology.n_crowns, 'n_thin': topology.n_thin,
+            'n_sites': topology.n_sites, 'n_titin': topology.n_titin, 'total_xbs': topology.total_xbs,
+            'n_faces_per_thin': topology.n_faces_per_thin}
+    if is_dyn:
+        tcfg['K_lat'] = K_lat
+        tcfg['K_lat_eff'] = (float(K_lat * topology.n_thick) if not isinstance(K_lat, list)
+                             else [float(k * topology.n_thick) for k in K_lat])
+        tcfg['nu'] = nu
+    return BatchPlan(n_steps=n_steps, dt=float(dt), params=params, z=z_b, pCa=p_b, ls=l_b, keys=keys,
+                     K_lat=K_b, nu=nu_b, dynamic_ls=is_dyn, grid_shape=grid_shape, replicates=replicates,
+                     axis_names=axis_names, coords=coords, rng_key=last_key, topology_config=tcfg)
+
+
+def assemble_result(plan: BatchPlan, metrics: np.ndarray, static_params: StaticParams, rng_seed: int,
+                    verbose: bool = False) -> SimulationResult:
+    """[B, 52, T] metrics -> data-cube SimulationResult with the residual warning."""
+    shape = plan.grid_shape + (plan.replicates, plan.n_steps)
+    md = MetricsDict()
+    for k, name in enumerate(METRIC_KEYS):
+        v = metrics[:, k, :].reshape(shape)
+        md[name] = v.astype(np.int32) if name == 'newton_iters' else v.astype(np.float32)
+    max_res = float(np.max(md['solver_residual'])) if md['solver_residual'].size else 0.0
+    tol = static_params.solver_residual_tol
+    if max_res > tol:
+        warnings.warn(f"Solver max residual {max_res:.2f} pN exceeds threshold {tol} pN "
+                      f"(set via StaticParams.solver_residual_tol)")
+    if verbose:
+        print(f"Result shape: {md['axial_force'].shape}")
+        print(f"Max solver residual: {max_res:.4f} pN")
+    return SimulationResult(
+        metrics=md, rng_key=plan.rng_key, z_line=plan.z.reshape(shape), pCa=plan.pCa.reshape(shape),
+        lattice_spacing=plan.ls.reshape(shape), final_state=None, metadata={'master_seed': rng_seed},
+        dt=plan.dt, name="run", grid_shape=plan.grid_shape, axis_names=plan.axis_names,
+        coords=plan.coords, topology_config=plan.topology_config)
+
+
+def run(topology: SarcTopology, duration_ms: float = 1000.0, dt: float = 1.0,
+        pCa: Union[float, List[float], np.ndarray] = 4.5,
+        z_line: Union[float, List[float], np.ndarray] = 900.0,
+        lattice_spacing: Union[float, List[float], np.ndarray] = 14.0,
+        K_lat: Union[float, List[float], None] = None, nu: Union[float, List[float]] = 0.0,
+        dynamic_params=None, static_params: Optional[StaticParams] = None, replicates: int = 1,
+        rng_seed: int = 0, unroll: int = 1, minibatch_size: Optional[int] = "auto", verbose: bool = False,
+        subpopulation=None, *, precision: str = 'float32', device: Optional[int] = None,
+        chunk_steps: int = 0) -> SimulationResult:
+    """Run a muscle simulation sweep on the GPU (reference ``simulation.py:754-1165``).
+
+    Same arguments, errors and result as the reference; ``unroll`` is accepted
+    and has no effect (the fused kernel has no scan to unroll).  Keyword-only
+    extensions: ``precision`` ``'float32'`` reproduces the reference's
+    single-precision arithmetic, ``'mixed'`` stores node displacements and
+    keeps the Newton residual test and large-norm expm squarings in float64;
+    ``device`` picks the CUDA device; ``chunk_steps`` > 0 splits the time loop
+    into launches of that many steps replayed from a CUDA graph.
+    """
+    if precision not in PRECISIONS:
+        raise ValueError(f"precision must be one of {PRECISIONS}")
+    sp = static_params if static_params is not None else StaticParams()
+    plan = plan_batch(topology, duration_ms, dt, pCa, z_line, lattice_spacing, K_lat, nu, dynamic_params,
+                      sp, replicates, rng_seed, subpopulation)
+    if verbose:
+        print(f"Grid shape: {plan.grid_shape}, axes: {plan.axis_names}, total: {plan.total}")
+    from .engine import execute_plan
+    metrics = execute_plan(topology, plan, sp, precision=precision, device=device,
+                           minibatch_size=minibatch_size, chunk_steps=chunk_steps)
+    return assemble_result(plan, metrics, sp, rng_seed, verbose)
+
+
+__all__ = ['run', 'SimulationResult', 'MetricsDict', 'METRIC_KEYS', 'BATCH_BUCKETS', 'get_bucket_size',
+           'plan_batch', 'assemble_result', 'BatchPlan']

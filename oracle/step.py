@@ -271,7 +271,7 @@ def thin_rest_cumsum(topo, dt):
 
 def run_condition(topo, prow, z_tr, pCa_tr, ls_tr, key, dt_ms=1.0, n_newton=4, n_cg=6, dt=np.float32,
                   K_lat=None, nu=0.0, uniforms=None, record_states=False, partitionable=None,
-                  hoist_tables=True):
+                  hoist_tables=True, udtype=np.float32):
     """The per-condition body of ``_run_sim_kernel`` (simulation.py:633-729).
 
     Returns ``(metrics [52, T], info)``; ``info['uniforms']`` holds the draws
@@ -314,7 +314,7 @@ def run_condition(topo, prow, z_tr, pCa_tr, ls_tr, key, dt_ms=1.0, n_newton=4, n
         if uniforms is not None:
             u_thin, u_xb = uniforms[t]
         else:
-            u_thin, u_xb, key = prng.step_uniforms(key, topo.n_sites_total, topo.total_xbs, np.float32,
+            u_thin, u_xb, key = prng.step_uniforms(key, topo.n_sites_total, topo.total_xbs, udtype,
                                                     partitionable)
         used.append((u_thin, u_xb))
         if K_lat is None:

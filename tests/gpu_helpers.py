@@ -1,0 +1,56 @@
+"""Drive the CUDA engine the way the parity tests need (injected uniforms, traces)."""
+import numpy as np
+
+from oracle import step as OS, prng
+
+
+def tt(a, dtype=None):
+    import torch
+    t = torch.as_tensor(np.ascontiguousarray(a))
+    if dtype is not None:
+        t = t.to(dtype)
+    return t.cuda().contiguous()
+
+
+def keys_tensor(keys):
+    import torch
+    return tt(np.asarray(keys, np.uint32).astype(np.int64)).to(torch.int32).contiguous()
+
+
+def run_engine(eng, topos, params, z, pCa, ls, keys, n_steps=None, K_lat=None, nu=None, dt=None, flags=0,
+               u_thin=None, u_xb=None, traces=False, chunk_steps=0):
+    import torch
+    B, T = np.asarray(z).shape
+    ns = np.full(B, T, np.int32) if n_steps is None else np.asarray(n_steps, np.int32)
+    res = eng.run_batch(topos, tt(params, torch.float32), tt(z, torch.float32), tt(pCa, torch.float32),
+                        tt(ls, torch.float32), tt(ns), keys_tensor(keys),
+                        K_lat=tt(np.zeros(B) if K_lat is None else K_lat, torch.float32),
+                        nu=tt(np.zeros(B) if nu is None else nu, torch.float32),
+                        dt=tt(np.ones(B) if dt is None else dt, torch.float32), flags=flags,
+                        u_thin=None if u_thin is None else tt(u_thin, torch.float32),
+                        u_xb=None if u_xb is None else tt(u_xb, torch.float32),
+                        want_x_trace=traces, want_state_trace=traces, chunk_steps=chunk_steps)
+    torch.cuda.synchronize()
+    return {k: v.cpu().numpy() for k, v in res.items()}
+
+
+def oracle_with_states(topo, row, z, pCa, ls, key, dtype=np.float32, K_lat=None, nu=0.0, uniforms=None):
+    return OS.run_condition(topo, row, z, pCa, ls, key, dt=dtype, K_lat=K_lat, nu=nu, uniforms=uniforms,
+                            record_states=True)
+
+
+def state_divergence(res, b, info, topo, T):
+    """First step where the engine's integer state arrays differ from the oracle's."""
+    X, S = topo.total_xbs, topo.n_sites_total
+    st, bt = res['state_trace'][b], res['bound_trace'][b]
+    for t in range(T):
+        o = info['states'][t]
+        if not (np.array_equal(st[t, :X], o.xb_state) and np.array_equal(st[t, X:X + S], o.tm.reshape(-1))
+                and np.array_equal(bt[t, :X], o.xb_bound)
+                and np.array_equal(bt[t, X:X + S], o.thin_bound.reshape(-1))):
+            return t
+    return None
+
+
+def oracle_positions(info, topo):
+    return np.stack([np.concatenate([s.thick_x.reshape(-1), s.thin_x.reshape(-1)]) for s in info['states']])

@@ -1,0 +1,174 @@
+"""CUDA engine vs the oracle and vs the reference's own outputs (needs a B200)."""
+import numpy as np
+import pytest
+
+from multifil_jax_b200 import SarcTopology, get_skeletal_params, get_cardiac_params, run
+from multifil_jax_b200.engine import MF_FLAG_DYNAMIC_LS, MF_FLAG_PRECISE, MF_FLAG_PLAIN, MF_FLAG_ORIGINAL_PRNG
+from multifil_jax_b200.simulation import plan_batch, METRIC_KEYS
+from oracle import prng, step as OS
+from tests.gpu_helpers import run_engine, oracle_with_states, state_divergence, oracle_positions
+from tests.oracle_helpers import first_divergence, compare_metrics
+
+pytestmark = pytest.mark.gpu
+KEYS = list(METRIC_KEYS)
+
+
+@pytest.mark.parametrize('nr,nc,T,pCa,z', [(1, 1, 30, 4.5, 900.0), (2, 2, 40, 4.5, 900.0),
+                                           (2, 2, 25, 6.0, 950.0), (3, 3, 12, 5.0, 1000.0)])
+def test_kernel_matches_oracle_per_step(engine, nr, nc, T, pCa, z):
+    """Injected identical uniforms: integer states bit-identical, positions/forces within 1e-5."""
+    s, d = get_skeletal_params()
+    topo = SarcTopology.create(nr, nc, s, d)
+    key = prng.split(prng.PRNGKey(11), 1)[0]
+    zt, pt, lt = np.full(T, z), np.full(T, pCa), np.full(T, 14.0)
+    m_o, info = oracle_with_states(topo, d.param_row(), zt, pt, lt, key)
+    ut = np.stack([u[0] for u in info['uniforms']])[None]
+    ux = np.stack([u[1] for u in info['uniforms']])[None]
+    res = run_engine(engine, topo, d.param_row()[None], zt[None], pt[None], lt[None], key[None],
+                     u_thin=ut, u_xb=ux, traces=True)
+    div = state_divergence(res, 0, info, topo, T)
+    mdiv = first_divergence(res['metrics'], m_o[None], KEYS)
+    win = min(v for v in (div, mdiv, T) if v is not None)
+    assert win >= min(T, 10), (div, mdiv)
+    xo = oracle_positions(info, topo)[:win]
+    xg = res['x_trace'][0, :win, :topo.n_dof]
+    # relative to the coordinate scale: a node near the M-line inherits the
+    # float32 spacing of positions ~1000 nm away through the coupled solve
+    assert np.max(np.abs(xg - xo) / np.maximum(np.abs(xo), 10.0)) < 1e-5
+    f_o, f_g = m_o[0, :win], res['metrics'][0, 0, :win]
+    assert np.max(np.abs(f_g - f_o) / np.maximum(np.abs(f_o), 1.0)) < 1e-5
+    bad = compare_metrics(res['metrics'], m_o[None], KEYS, rtol=1e-4, upto=win)
+    assert not bad, bad
+
+
+def test_device_threefry_matches_jax_layout(engine):
+    """No injection: the kernel's own Threefry stream reproduces the oracle's draws."""
+    s, d = get_skeletal_params()
+    topo = SarcTopology.create(2, 2, s, d)
+    T = 30
+    for part, flags in ((None, 0), (False, MF_FLAG_ORIGINAL_PRNG)):
+        key = prng.split(prng.PRNGKey(3), 1, partitionable=part)[0]
+        m_o, info = OS.run_condition(topo, d.param_row(), np.full(T, 900.0), np.full(T, 4.5), np.full(T, 14.0),
+                                     key, record_states=True, partitionable=part)
+        res = run_engine(engine, topo, d.param_row()[None], np.full((1, T), 900.0), np.full((1, T), 4.5),
+                         np.full((1, T), 14.0), key[None], traces=True, flags=flags)
+        div = state_divergence(res, 0, info, topo, T)
+        assert div is None or div >= 20, div
+
+
+def _golden_case(name):
+    import os, sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), 'golden'))
+    from make_golden import RUNS, _trace
+    nr, nc, preset, kw = RUNS[name]
+    s, d = get_cardiac_params() if preset == 'cardiac' else get_skeletal_params()
+    kw = dict(kw)
+    if isinstance(kw.get('z_line'), str):
+        kw['z_line'] = _trace(kw['z_line'], int(kw['duration_ms']))
+    return SarcTopology.create(nr, nc, s, d), s, d, kw
+
+
+@pytest.mark.parametrize('name', ['skel_1x1', 'skel_2x2', 'card_2x2_z950', 'sweep_2x2', 'dynls_1x1',
+                                  'dynls_2x2', 'sine_2x2', 'poisson_1x1'])
+def test_run_api_matches_reference_fixture(golden, name):
+    """run() on the GPU against the reference's own run() output for the same inputs."""
+    topo, s, d, kw = _golden_case(name)
+    r = run(topo, dynamic_params=d, static_params=s, rng_seed=0, **kw)
+    assert np.array_equal(r.rng_key, golden[f'run_{name}__rng_key'])
+    B = int(np.prod(r.axial_force.shape[:-1]))
+    T = r.n_steps
+    mine = np.stack([r.metrics[k].reshape(B, T).astype(np.float64) for k in KEYS], axis=1)
+    ref = np.stack([golden[f'run_{name}__{k}'].reshape(B, T) for k in KEYS], axis=1)
+    div = first_divergence(mine, ref, KEYS)
+    upto = div if div is not None else T
+    assert upto >= min(T, 5), div
+    bad = compare_metrics(mine, ref, KEYS, rtol=1e-4, upto=upto)
+    assert not bad, bad
+
+
+def test_plain_chunked_and_batched_are_identical(engine):
+    s, d = get_skeletal_params()
+    topo = SarcTopology.create(2, 2, s, d)
+    B, T = 3, 24
+    keys = prng.split(prng.PRNGKey(0), B)
+    P = np.tile(d.param_row(), (B, 1))
+    Z, PC, L = np.full((B, T), 900.0), np.repeat(np.array([4.5, 5.5, 6.5])[:, None], T, 1), np.full((B, T), 14.0)
+    a = run_engine(engine, topo, P, Z, PC, L, keys)
+    b = run_engine(engine, topo, P, Z, PC, L, keys, flags=MF_FLAG_PLAIN)
+    c = run_engine(engine, topo, P, Z, PC, L, keys, chunk_steps=5)
+    assert np.array_equal(a['metrics'], b['metrics'])
+    assert np.array_equal(a['metrics'], c['metrics'])
+
+
+def test_condition_alone_equals_in_mixed_batch(engine):
+    """Uneven lattices and durations in one launch; each row equals its solo run."""
+    s, d = get_skeletal_params()
+    sizes = [(1, 1), (2, 2), (3, 2), (2, 2)]
+    topos = [SarcTopology.create(r, c, s, d) for r, c in sizes]
+    T = 20
+    n_steps = [20, 7, 13, 20]
+    keys = prng.split(prng.PRNGKey(5), 4)
+    pcas = [4.5, 5.0, 6.0, 7.0]
+    P = np.tile(d.param_row(), (4, 1))
+    Z, PC, L = np.full((4, T), 920.0), np.repeat(np.array(pcas)[:, None], T, 1), np.full((4, T), 13.5)
+    mix = run_engine(engine, topos, P, Z, PC, L, keys, n_steps=n_steps)
+    for i in range(4):
+        solo = run_engine(engine, topos[i], P[i:i + 1], Z[i:i + 1], PC[i:i + 1], L[i:i + 1], keys[i:i + 1],
+                          n_steps=[n_steps[i]])
+        assert np.array_equal(solo['metrics'][0, :, :n_steps[i]], mix['metrics'][i, :, :n_steps[i]])
+
+
+@pytest.mark.parametrize('nr,nc', [(1, 1), (2, 2)])
+def test_dynamic_lattice_spacing_matches_oracle(engine, nr, nc):
+    s, d = get_skeletal_params()
+    topo = SarcTopology.create(nr, nc, s, d)
+    T = 15
+    key = prng.split(prng.PRNGKey(2), 1)[0]
+    K = 5.0 * topo.n_thick
+    zt = 900.0 + 0.5 * np.arange(T)
+    m_o, info = oracle_with_states(topo, d.param_row(), zt, np.full(T, 4.5), np.full(T, 14.0), key, K_lat=K, nu=0.5)
+    ut = np.stack([u[0] for u in info['uniforms']])[None]
+    ux = np.stack([u[1] for u in info['uniforms']])[None]
+    res = run_engine(engine, topo, d.param_row()[None], zt[None], np.full((1, T), 4.5), np.full((1, T), 14.0),
+                     key[None], K_lat=[K], nu=[0.5], flags=MF_FLAG_DYNAMIC_LS, u_thin=ut, u_xb=ux, traces=True)
+    div = state_divergence(res, 0, info, topo, T)
+    mdiv = first_divergence(res['metrics'], m_o[None], KEYS)
+    win = min(v for v in (div, mdiv, T) if v is not None)
+    assert win >= 5
+    ls_o, ls_g = m_o[4, :win], res['metrics'][0, 4, :win]
+    assert np.max(np.abs(ls_g - ls_o) / ls_o) < 1e-5
+    bad = compare_metrics(res['metrics'], m_o[None], KEYS, rtol=1e-4, upto=win)
+    assert not bad, bad
+
+
+def test_mixed_precision_force_error_vs_fp64_oracle(engine):
+    """'mixed' precision: <= 1e-5 relative force error against the FP64 oracle (same uniforms)."""
+    s, d = get_skeletal_params()
+    topo = SarcTopology.create(2, 2, s, d)
+    T = 30
+    key = prng.split(prng.PRNGKey(0), 1)[0]
+    zt, pt, lt = np.full(T, 900.0), np.full(T, 4.5), np.full(T, 14.0)
+    m32, info32 = OS.run_condition(topo, d.param_row(), zt, pt, lt, key)
+    m64, info64 = OS.run_condition(topo, d.param_row(), zt, pt, lt, key, dt=np.float64,
+                                   uniforms=info32['uniforms'], record_states=True)
+    ut = np.stack([u[0] for u in info32['uniforms']])[None]
+    ux = np.stack([u[1] for u in info32['uniforms']])[None]
+    res = run_engine(engine, topo, d.param_row()[None], zt[None], pt[None], lt[None], key[None],
+                     flags=MF_FLAG_PRECISE, u_thin=ut, u_xb=ux, traces=True)
+    div = state_divergence(res, 0, info64, topo, T)
+    mdiv = first_divergence(res['metrics'], m64[None], KEYS)
+    win = min(v for v in (div, mdiv, T) if v is not None)
+    assert win >= 3
+    f64, fg = m64[0, :win], res['metrics'][0, 0, :win]
+    err_mixed = np.max(np.abs(fg - f64) / np.abs(f64))
+    assert err_mixed <= 1e-5, err_mixed
+
+
+def test_bad_arguments_raise(engine):
+    import torch
+    from multifil_jax_b200.engine import EngineError
+    s, d = get_skeletal_params()
+    topo = SarcTopology.create(1, 1, s, d)
+    with pytest.raises(EngineError):
+        run_engine(engine, topo, d.param_row()[None], np.full((1, 4), 900.0), np.full((1, 4), 4.5),
+                   np.full((1, 4), 14.0), prng.split(prng.PRNGKey(0), 1), n_steps=[9])

@@ -1,0 +1,136 @@
+"""run()'s host side: sweep expansion, parameter tables, result container (CPU only)."""
+import warnings
+
+import numpy as np
+import pytest
+
+from multifil_jax_b200 import (SarcTopology, DynamicParams, StaticParams, get_skeletal_params,
+                               get_cardiac_params, DYNAMIC_FIELDS)
+from multifil_jax_b200.simulation import plan_batch, assemble_result, SimulationResult, METRIC_KEYS, MetricsDict
+from oracle import prng
+
+
+@pytest.fixture(scope='module')
+def topo():
+    return SarcTopology.create(2, 2)
+
+
+def test_scalar_run_shape_and_keys(topo):
+    p = plan_batch(topo, duration_ms=10)
+    assert p.total == 1 and p.n_steps == 10 and p.grid_shape == () and p.axis_names == ['replicates', 'time']
+    assert np.array_equal(p.keys[0], prng.split(prng.PRNGKey(0), 1)[0])
+    assert p.params.shape == (1, 44) and p.params.dtype == np.float32
+    assert np.all(p.z == 900.0) and np.all(p.pCa == 4.5) and np.all(p.ls == 14.0)
+
+
+def test_fixed_axis_order_and_cartesian_product(topo):
+    # axes come out z_line, pCa, lattice_spacing, K_lat, nu, params -- not call order
+    p = plan_batch(topo, duration_ms=5, pCa=[4.0, 5.0, 6.0], z_line=[900.0, 950.0], replicates=2,
+                   dynamic_params={'xb_r01_coeff': [300.0, 310.0]})
+    assert p.axis_names == ['z_line', 'pCa', 'xb_r01_coeff', 'replicates', 'time']
+    assert p.grid_shape == (2, 3, 2) and p.total == 24
+    # replicates innermost: rows 0,1 share every sweep value
+    assert p.pCa[0, 0] == p.pCa[1, 0] and p.z[0, 0] == 900.0 and p.z[-1, 0] == 950.0
+    i = DYNAMIC_FIELDS.index('xb_r01_coeff')
+    assert p.params[0, i] == np.float32(300.0) and p.params[2, i] == np.float32(310.0)
+    assert np.array_equal(p.keys, prng.split(prng.PRNGKey(0), 24))
+
+
+def test_candidate_list_and_dict_overrides(topo):
+    _, card = get_cardiac_params()
+    _, skel = get_skeletal_params()
+    p = plan_batch(topo, duration_ms=3, dynamic_params=[skel, card])
+    assert p.axis_names[0] == 'candidates' and p.total == 2
+    j = DYNAMIC_FIELDS.index('xb_r05')
+    assert p.params[0, j] == np.float32(0.007) and p.params[1, j] == np.float32(0.2)
+    p = plan_batch(topo, duration_ms=3, dynamic_params={'thick_k': 8000.0})
+    assert p.params[0, 0] == 8000.0 and p.total == 1
+
+
+def test_traces_and_trace_sweeps(topo):
+    tr = 900 + np.arange(6.0)
+    p = plan_batch(topo, duration_ms=6, z_line=tr)
+    assert np.array_equal(p.z[0], tr.astype(np.float32))
+    p = plan_batch(topo, duration_ms=6, z_line=[tr, tr + 1])
+    assert p.grid_shape == (2,) and isinstance(p.coords['z_line'][0], np.ndarray)
+    with pytest.raises(ValueError):
+        plan_batch(topo, duration_ms=6, z_line=np.arange(5.0))
+
+
+def test_poisson_and_dynamic_lattice_spacing(topo):
+    tr = 900 + np.arange(4.0)
+    p = plan_batch(topo, duration_ms=4, z_line=tr, nu=0.5)
+    expect = (np.float32(14.0) * (np.float32(900.0) / tr.astype(np.float32)) ** np.float32(0.5)).astype(np.float32)
+    assert np.allclose(p.ls[0], expect, rtol=1e-7)
+    p = plan_batch(topo, duration_ms=4, K_lat=5.0, nu=0.5)
+    assert p.dynamic_ls and p.K_lat[0] == np.float32(5.0 * topo.n_thick)
+    assert p.topology_config['K_lat_eff'] == 5.0 * topo.n_thick
+
+
+def test_errors(topo):
+    with pytest.raises(ValueError):
+        plan_batch(topo, duration_ms=3, pCa=[])
+    with pytest.raises(ValueError):
+        plan_batch(topo, duration_ms=3, dynamic_params={'nope': 1.0})
+    with pytest.raises(ValueError):
+        plan_batch(topo, duration_ms=3, dynamic_params=[])
+    with pytest.raises(ValueError):
+        plan_batch(topo, duration_ms=3, dynamic_params=42)
+    with pytest.raises(NotImplementedError):
+        plan_batch(topo, duration_ms=3, subpopulation=object())
+
+
+def test_padding_key_is_last_of_bucket(topo):
+    # 3 conditions pad to 4: the returned key is split(PRNGKey(seed+1), 1)[-1]
+    p = plan_batch(topo, duration_ms=2, pCa=[4.0, 5.0, 6.0], rng_seed=5)
+    assert np.array_equal(p.rng_key, prng.split(prng.PRNGKey(6), 1)[-1])
+    p = plan_batch(topo, duration_ms=2, pCa=[4.0, 5.0], rng_seed=5)
+    assert np.array_equal(p.rng_key, p.keys[-1])
+
+
+def _fake_result(topo, **kw):
+    p = plan_batch(topo, **kw)
+    m = np.random.default_rng(0).random((p.total, 52, p.n_steps)).astype(np.float32)
+    m[:, METRIC_KEYS.index('solver_residual')] = 0.1
+    return p, assemble_result(p, m, StaticParams(), 0)
+
+
+def test_result_cube_sel_mean_std_stack(topo):
+    p, r = _fake_result(topo, duration_ms=5, pCa=[4.0, 5.0, 6.0], replicates=4)
+    assert r.axial_force.shape == (3, 4, 5) and r.n_steps == 5 and r.metrics['newton_iters'].dtype == np.int32
+    assert isinstance(r.metrics, MetricsDict) and r.metrics.axial_force is r.metrics['axial_force']
+    s = r.sel(pCa=5.0)
+    assert s.axial_force.shape == (4, 5) and 'pCa' not in s.coords
+    m = r.mean()
+    assert m.axial_force.shape == (3, 5) and np.allclose(m.axial_force, r.axial_force.mean(axis=-2))
+    sd = r.std()
+    assert np.allclose(sd.axial_force, r.axial_force.std(axis=-2))
+    st = SimulationResult.stack([r, r], axis_name='size', axis_values=[2, 3])
+    assert st.axial_force.shape == (2, 3, 4, 5) and st._axis_names[0] == 'size'
+    sub = r[1:]
+    assert sub.coords['pCa'] == [5.0, 6.0]
+    assert 'Mean force' in r.summary() and np.isclose(r.time[-1], 4.0)
+    with pytest.raises(ValueError):
+        r.sel(pCa=9.9)
+
+
+def test_residual_warning(topo):
+    p = plan_batch(topo, duration_ms=2)
+    m = np.zeros((1, 52, 2), np.float32)
+    m[:, 1] = 3.0
+    with warnings.catch_warnings(record=True) as w:
+        warnings.simplefilter('always')
+        assemble_result(p, m, StaticParams(), 0)
+    assert any('exceeds threshold' in str(x.message) for x in w)
+
+
+def test_params_api():
+    s, d = get_skeletal_params()
+    d2 = d.copy(xb_r01_coeff=350.0)
+    assert float(d2.xb_r01_coeff) == np.float32(350.0) and float(d.xb_r01_coeff) == np.float32(305.99)
+    with pytest.raises(ValueError):
+        d.copy(bogus=1.0)
+    assert len(DYNAMIC_FIELDS) == 44 and d.param_row().shape == (44,)
+    assert s.replace(n_cg_steps=3).n_cg_steps == 3
+    with pytest.raises(ValueError):
+        StaticParams(n_superlattice_classes=2)
