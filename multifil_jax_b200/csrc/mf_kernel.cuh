@@ -14,7 +14,7 @@ __host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, bool vec_
   size_t o = 0;
   auto add = [&](size_t bytes) { o = align_up(o + bytes, 16); };
   add(sizeof(double) * 64);                // redd
-  add(sizeof(float) * 32 * 24);            // red
+  add(sizeof(float) * 1536);               // red
   if (!vec_global) add(sizeof(float) * 5 * N);  // x r dx pv zz
   if (!vec_global) add(sizeof(float) * 4 * X);  // fxb fdx fdd frdd
   add(sizeof(float) * X);                  // xb_ax
@@ -43,7 +43,7 @@ __device__ void carve(Sim<NT>& m, char* base, bool vec_global) {
   size_t o = 0;
   auto take = [&](size_t bytes) { char* p = base + o; o = align_up(o + bytes, 16); return p; };
   m.s.redd = (double*)take(sizeof(double) * 64);
-  m.s.red = (float*)take(sizeof(float) * 32 * 24);
+  m.s.red = (float*)take(sizeof(float) * 1536);
   float* v5 = vec_global ? reinterpret_cast<float*>(m.ws + m.L.vec) : (float*)take(sizeof(float) * 5 * N);
   m.s.x = v5; m.s.r = v5 + N; m.s.dx = v5 + 2 * N; m.s.pv = v5 + 3 * N; m.s.zz = v5 + 4 * N;
   float* f4 = vec_global ? reinterpret_cast<float*>(m.ws + m.L.vec) + 5 * N : (float*)take(sizeof(float) * 4 * X);
@@ -137,17 +137,19 @@ __device__ void metrics(Sim<NT>& m, int t, float zl, float pCa, float new_ls, fl
     nmin = fminf(nmin, dsp);
     nmax = fmaxf(nmax, dsp);
   }
+  // one reduction: 4 maxima (min as -max), 16 counts, 5 sums
+  float red[25];
+  red[0] = -tmin; red[1] = tmax; red[2] = -nmin; red[3] = nmax;
+#pragma unroll
+  for (int k = 0; k < 15; ++k) red[4 + k] = (float)ci[k];
+  red[19] = (float)c3o;
+  red[20] = cf[0]; red[21] = cf[1]; red[22] = cf[2]; red[23] = cf[3]; red[24] = tear;
+  m.template bred<25>(red, 4);
+  tmin = -red[0]; tmax = red[1]; nmin = -red[2]; nmax = red[3];
   int cnt[16];
 #pragma unroll
-  for (int k = 0; k < 15; ++k) cnt[k] = ci[k];
-  cnt[15] = c3o;
-  m.template bsum_ki<16>(cnt);
-  float sums[5] = {cf[0], cf[1], cf[2], cf[3], tear};
-  m.template bsum_k<5>(sums);
-  tmin = m.bmin(tmin);
-  tmax = m.bmax(tmax);
-  nmin = m.bmin(nmin);
-  nmax = m.bmax(nmax);
+  for (int k = 0; k < 16; ++k) cnt[k] = (int)red[4 + k];
+  float sums[5] = {red[20], red[21], red[22], red[23], red[24]};
   const float tmean = sums[0] / (float)NTN, nmean = sums[1] / (float)S;
   float sq[2] = {0.f, 0.f};
   for (int i = tid; i < NTN; i += NT) {
@@ -162,7 +164,7 @@ __device__ void metrics(Sim<NT>& m, int t, float zl, float pCa, float new_ls, fl
     const float c = dsp - nmean;
     sq[1] += c * c;
   }
-  m.template bsum_k<2>(sq);
+  m.template bred<2>(sq, 0);
   if (tid == 0) {
     const float nx = (float)X, nt = (float)S;
     const float* P = m.s.P;
@@ -469,10 +471,10 @@ __device__ void run_condition(const StepArgs& A, int ci) {
         const float u = m.precise ? m.s.x[n0] : m.s.x[n0] - T.crown_off[n0];
         force += u * m.s.P[THICK_K];
       }
-      m.s.red[32 * 24 - 1] = force;
+      m.s.red[1535] = force;
     }
     __syncthreads();
-    force = m.s.red[32 * 24 - 1];
+    force = m.s.red[1535];
     __syncthreads();
     metrics(m, t, zl, pCa, new_ls, force, resid, iters, xg, xbs_g, nullptr, xbn_g, xba_g, tm_g, Mo);
     if (resid > (double)A.resid_warn) m.status |= 2;

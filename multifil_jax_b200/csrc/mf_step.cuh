@@ -191,6 +191,23 @@ struct Sim {
     for (int w = 1; w < NW; ++w) t = fminf(t, s.red[w]);
     return t;
   }
+  // K floats at once: entries k < nmax reduced with max, the rest summed
+  template <int K>
+  __device__ void bred(float (&v)[K], int nmax) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = k < nmax ? warp_max(v[k]) : warp_sum(v[k]);
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+      for (int k = 0; k < K; ++k) s.red[k * NW + warp] = v[k];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      float t = s.red[k * NW];
+      for (int w = 1; w < NW; ++w) t = k < nmax ? fmaxf(t, s.red[k * NW + w]) : t + s.red[k * NW + w];
+      v[k] = t;
+    }
+  }
   // sum of K floats at once
   template <int K>
   __device__ void bsum_k(float (&v)[K]) {
@@ -294,9 +311,91 @@ struct Sim {
     }
   }
 
+  // Thomas substitutions of one filament as warp-shuffle affine scans: lane l
+  // owns nodes [l*E, l*E+E); a local scan per lane, a 5-step Kogge-Stone
+  // composition across lanes, then the lane's own nodes.  Same result as the
+  // tree order in exact arithmetic; used in precise mode, where the
+  // reference's float32 association order is not the target.
+  template <int E>
+  __device__ __forceinline__ void thomas_shfl(const float* in, float* out, int n, const float* Af,
+                                              const float* Ab, const float* inv) {
+    float y[E], a[E];
+    const int i0 = lane * E;
+    // forward: y[i] = a_f[i] * y[i-1] + r[i], y[-1] = 0
+    float A = 1.f, Bv = 0.f;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int i = i0 + e;
+      const bool ok = i < n;
+      a[e] = ok ? Af[i] : 1.f;
+      y[e] = ok ? in[i] : 0.f;
+      Bv = fmaf(a[e], Bv, y[e]);
+      A = a[e] * A;
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const float Ap = __shfl_up_sync(0xffffffffu, A, o), Bp = __shfl_up_sync(0xffffffffu, Bv, o);
+      if (lane >= o) {
+        Bv = fmaf(A, Bp, Bv);
+        A = A * Ap;
+      }
+    }
+    float yp = __shfl_up_sync(0xffffffffu, Bv, 1);
+    if (lane == 0) yp = 0.f;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      yp = fmaf(a[e], yp, y[e]);
+      y[e] = yp;
+    }
+    // backward: x[i] = (y[i] * inv[i]) + a_b[i] * x[i+1], x[n] = 0
+    A = 1.f;
+    Bv = 0.f;
+#pragma unroll
+    for (int e = E - 1; e >= 0; --e) {
+      const int i = i0 + e;
+      const bool ok = i < n;
+      a[e] = ok ? Ab[n - 1 - i] : 1.f;
+      y[e] = ok ? y[e] * inv[i] : 0.f;
+      Bv = fmaf(a[e], Bv, y[e]);
+      A = a[e] * A;
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const float Ap = __shfl_down_sync(0xffffffffu, A, o), Bp = __shfl_down_sync(0xffffffffu, Bv, o);
+      if (lane + o < 32) {
+        Bv = fmaf(A, Bp, Bv);
+        A = A * Ap;
+      }
+    }
+    float xp = __shfl_down_sync(0xffffffffu, Bv, 1);
+    if (lane == 31) xp = 0.f;
+#pragma unroll
+    for (int e = E - 1; e >= 0; --e) {
+      xp = fmaf(a[e], xp, y[e]);
+      const int i = i0 + e;
+      if (i < n) out[i] = xp;
+    }
+  }
+
   // out = M^{-1} in on this warp's own filaments (no block barrier needed).
   __device__ void precondition_own(const float* in, float* out) {
     const int nf = T.n_thick + T.n_thin;
+    if (precise) {
+      __syncwarp();
+      for (int f = warp; f < nf; f += NW) {
+        const bool thick = f < T.n_thick;
+        const int n = thick ? T.n_crowns : T.n_sites;
+        const int base = thick ? f * T.n_crowns : T.n_thick_nodes + (f - T.n_thick) * T.n_sites;
+        const float* Af = s.coef + (thick ? cl.thick_fwd : cl.thin_fwd);
+        const float* Ab = s.coef + (thick ? cl.thick_back : cl.thin_back);
+        const float* inv = s.coef + (thick ? cl.thick_inv : cl.thin_inv);
+        if (n <= 64) thomas_shfl<2>(in + base, out + base, n, Af, Ab, inv);
+        else if (n <= 96) thomas_shfl<3>(in + base, out + base, n, Af, Ab, inv);
+        else thomas_shfl<4>(in + base, out + base, n, Af, Ab, inv);
+      }
+      __syncwarp();
+      return;
+    }
     float* buf = s.scan + warp * (T.plan_thin.total > T.plan_thick.total ? T.plan_thin.total
                                                                           : T.plan_thick.total);
     __syncwarp();
@@ -331,7 +430,7 @@ struct Sim {
   __device__ __forceinline__ void reduce(float (&v)[K], bool max0) {
 #pragma unroll
     for (int k = 0; k < K; ++k) v[k] = (max0 && k == 0) ? warp_max(v[k]) : warp_sum(v[k]);
-    float* rb = s.red + 512 + redbuf * 96;  // clear of bsum_* (red[0, 512)) and red[767]
+    float* rb = s.red + 1024 + redbuf * 96;  // clear of bred/bsum_* (red[0, 1024)) and red[1535]
     redbuf ^= 1;
     if (lane == 0)
 #pragma unroll
