@@ -126,6 +126,23 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* batch, void* stream);
 /* Device bytes the library needs for a batch (admission control). */
 int mf_workspace_bytes(mf_ctx* ctx, const mf_batch* batch, uint64_t* bytes);
 
+/* Allocation-free variant of mf_run_batch (no counterpart in the reference:
+ * it exists for callers of this library, not of the reference API).
+ * For callers that must not have the library allocate device memory on the
+ * call path -- a framework that owns all HBM through its own allocator and
+ * budget, or a loop that cannot absorb cudaMalloc's implicit device-wide
+ * synchronisation.  All per-call scratch (per-condition workspaces and the
+ * launch descriptor table) comes from one 8 MiB array compiled into the
+ * library (present on every device that loads it, until process exit); the
+ * call never allocates.  A batch whose scratch exceeds 8 MiB is rejected with
+ * MF_ERR_NOMEM and a message naming both sizes (at 2x2 about 75 conditions
+ * fit).  Batched single-launch path only: MF_FLAG_PLAIN and chunk_steps > 0
+ * are rejected.  The first call on a device resolves the array's device
+ * address, so make it before any stream capture.  Every call reuses the same
+ * array (the region a call uses is zeroed before its kernels run); calls that
+ * overlap on the GPU race on it and must be serialised by the caller. */
+int mf_run_batch_static(mf_ctx* ctx, const mf_batch* batch, void* stream);
+
 /* jax.random on the host: key = PRNGKey(seed); keys_out[2*i..] = split(key, n)[i].
  * partitionable=1: JAX >= 0.5 layout; 0: original layout. */
 int mf_prng_split(uint32_t k0, uint32_t k1, int32_t n, int32_t partitionable, uint32_t* keys_out);

@@ -523,6 +523,150 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
   return MF_OK;
 }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free batch entry point.
+//
+// mf_run_batch grows a library-owned workspace with cudaMalloc whenever a
+// batch needs more room than it has.  Some callers cannot accept that: a host
+// framework that hands every byte of HBM to its own allocator and budget, or
+// a latency-critical loop for which cudaMalloc's implicit device-wide
+// synchronisation is a stall.  mf_run_batch_static serves them by taking all
+// of its per-call device memory -- the per-condition resident workspaces and
+// the launch descriptor table -- from one fixed array compiled into this
+// library (kStaticScratchBytes per device, resident in every process that
+// loads the library, for the life of that process).  It never calls
+// cudaMalloc, cudaFree or any allocating routine.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kStaticScratchBytes = size_t(8) << 20;  // 8 MiB per device
+constexpr int kMaxDevices = 64;
+
+static __device__ __align__(256) char g_static_scratch[kStaticScratchBytes];
+
+// Device address of g_static_scratch per device, resolved once with that
+// device current (the host symbol itself is not a device address).
+char* g_static_ptr[kMaxDevices] = {nullptr};
+
+}  // namespace
+
+extern "C" {
+
+int mf_run_batch_static(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
+  if (!ctx || !bt) return fail(ctx, MF_ERR_INVALID, "null argument");
+  if (bt->B < 0 || bt->T_max < 0) return fail(ctx, MF_ERR_INVALID, "negative batch shape");
+  if (bt->B == 0) return MF_OK;
+  if (!bt->topo_id || !bt->params || !bt->z || !bt->pCa || !bt->ls || !bt->n_steps || !bt->keys ||
+      !bt->metrics_out)
+    return fail(ctx, MF_ERR_INVALID, "missing required array");
+  if (bt->flags & (MF_FLAG_PLAIN)) return fail(ctx, MF_ERR_INVALID, "mf_run_batch_static: plain path not offered");
+  if (bt->chunk_steps > 0) return fail(ctx, MF_ERR_INVALID, "mf_run_batch_static: runs all steps in one launch");
+  if ((bt->flags & MF_FLAG_DYNAMIC_LS) && (!bt->K_lat || !bt->nu))
+    return fail(ctx, MF_ERR_INVALID, "dynamic lattice spacing needs K_lat and nu");
+  if (ctx->device < 0 || ctx->device >= kMaxDevices) return fail(ctx, MF_ERR_INVALID, "device index out of range");
+  CK(cudaSetDevice(ctx->device));
+  // one-time set-up on this device (the first call must not be inside a capture)
+  if (!g_static_ptr[ctx->device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(ctx, MF_ERR_CUDA, "cudaGetSymbolAddress(static scratch): %s", cudaGetErrorString(e));
+    g_static_ptr[ctx->device] = static_cast<char*>(p);
+  }
+  char* base = g_static_ptr[ctx->device];
+  cudaStream_t st = (cudaStream_t)stream_v;
+  const int B = bt->B;
+  std::vector<int> n_steps(B);
+  std::vector<float> h_K(B, 0.f), h_nu(B, 0.f), h_dt(B, 1.0f);
+  CK(cudaMemcpy(n_steps.data(), bt->n_steps, sizeof(int) * B, cudaMemcpyDeviceToHost));
+  if (bt->K_lat) CK(cudaMemcpy(h_K.data(), bt->K_lat, sizeof(float) * B, cudaMemcpyDeviceToHost));
+  if (bt->nu) CK(cudaMemcpy(h_nu.data(), bt->nu, sizeof(float) * B, cudaMemcpyDeviceToHost));
+  if (bt->dt) CK(cudaMemcpy(h_dt.data(), bt->dt, sizeof(float) * B, cudaMemcpyDeviceToHost));
+  // size check: descriptor table + every condition's workspace must fit
+  const size_t desc_bytes = align_up(sizeof(CondDesc) * (size_t)B, 256);
+  size_t need = desc_bytes;
+  int max_dof = 0, max_x = 0, max_s = 0;
+  for (int i = 0; i < B; ++i) {
+    const int id = bt->topo_id[i];
+    if (id < 0 || id >= (int)ctx->topos.size()) return fail(ctx, MF_ERR_NOTFOUND, "unknown topology %d", id);
+    if (n_steps[i] < 0 || n_steps[i] > bt->T_max) return fail(ctx, MF_ERR_INVALID, "n_steps out of range");
+    const TopoDev& td = ctx->topos[id]->dev;
+    max_dof = std::max(max_dof, td.n_dof);
+    max_x = std::max(max_x, td.total_xbs);
+    max_s = std::max(max_s, td.n_sites_total);
+    need += slot_bytes(td);
+  }
+  if (need > kStaticScratchBytes)
+    return fail(ctx, MF_ERR_NOMEM,
+                "mf_run_batch_static: batch needs %zu B of scratch, the static array holds %zu B "
+                "(split the batch or use mf_run_batch)", need, kStaticScratchBytes);
+  // group by CTA configuration exactly as mf_run_batch does
+  std::vector<int> order(B);
+  for (int i = 0; i < B; ++i) order[i] = i;
+  auto key_of = [&](int i) {
+    const TopoHost& t = *ctx->topos[bt->topo_id[i]];
+    return std::make_pair(t.threads * 2 + (t.vec_global ? 1 : 0), -(long)n_steps[i] * t.dev.n_dof);
+  };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key_of(a) < key_of(b); });
+  CondDesc* d_desc = reinterpret_cast<CondDesc*>(base);
+  std::vector<CondDesc> hc(B);
+  size_t off = desc_bytes;
+  for (int k = 0; k < B; ++k) {
+    const int i = order[k];
+    const TopoHost& t = *ctx->topos[bt->topo_id[i]];
+    CondDesc& c = hc[k];
+    c.topo = t.d_struct;
+    c.ws = base + off;
+    c.n_steps = n_steps[i];
+    c.index = i;
+    c.T = bt->T_max;
+    c.t0 = 0;
+    c.t1 = n_steps[i];
+    c.params = bt->params + (size_t)i * MF_N_PARAMS;
+    c.z = bt->z + (size_t)i * bt->T_max;
+    c.pCa = bt->pCa + (size_t)i * bt->T_max;
+    c.ls = bt->ls + (size_t)i * bt->T_max;
+    c.key = bt->keys + 2 * (size_t)i;
+    c.metrics = bt->metrics_out + (size_t)i * MF_N_METRICS * bt->T_max;
+    c.status = bt->status_out ? bt->status_out + i : nullptr;
+    c.key_out = bt->keys_out ? bt->keys_out + 2 * (size_t)i : nullptr;
+    c.K_lat = h_K[i];
+    c.nu = h_nu[i];
+    c.dt = h_dt[i];
+    off += slot_bytes(t.dev);
+  }
+  // The array keeps whatever the previous call left.  The kernel rebuilds
+  // every workspace field at step 0, but the region this call uses is zeroed
+  // first so no stale byte can ever be read.  Calls whose work overlaps on
+  // the GPU (different streams, or no ordering between them) share this one
+  // array and race; callers must serialise them.
+  CK(cudaMemsetAsync(base, 0, off, st));
+  CK(cudaMemcpyAsync(d_desc, hc.data(), sizeof(CondDesc) * B, cudaMemcpyHostToDevice, st));
+  int flags = 0;
+  if (bt->flags & MF_FLAG_DYNAMIC_LS) flags |= FLAG_DYN;
+  if (bt->flags & MF_FLAG_PRECISE) flags |= FLAG_PRECISE;
+  if (bt->flags & MF_FLAG_ORIGINAL_PRNG) flags |= FLAG_ORIG_PRNG;
+  for (int k = 0; k < B;) {
+    const TopoHost& t0 = *ctx->topos[bt->topo_id[order[k]]];
+    int e = k;
+    size_t smem = 0;
+    while (e < B) {
+      const TopoHost& tk = *ctx->topos[bt->topo_id[order[e]]];
+      if (tk.threads != t0.threads || tk.vec_global != t0.vec_global) break;
+      smem = std::max(smem, tk.smem_local);
+      ++e;
+    }
+    StepArgs a = make_args(bt, d_desc, flags | (t0.vec_global ? 64 : 0), max_dof, max_x, max_s);
+    cudaError_t err = launch(t0.threads, a, e - k, k, smem, st);
+    if (err != cudaSuccess) return fail(ctx, MF_ERR_CUDA, "static launch: %s", cudaGetErrorString(err));
+    k = e;
+  }
+  CK(cudaStreamSynchronize(st));  // the host descriptor staging vector dies here
+  return MF_OK;
+}
+
 int mf_prng_split(uint32_t k0, uint32_t k1, int32_t n, int32_t partitionable, uint32_t* out) {
   if (n < 0 || (!out && n > 0)) return MF_ERR_INVALID;
   for (int i = 0; i < n; ++i) {

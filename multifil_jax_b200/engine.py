@@ -86,6 +86,7 @@ _SIGNATURES = {
                                           ctypes.POINTER(ctypes.c_int32)]),
     'mf_tune_threads': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]),
     'mf_run_batch': (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(mf_batch), ctypes.c_void_p]),
+    'mf_run_batch_static': (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(mf_batch), ctypes.c_void_p]),
     'mf_workspace_bytes': (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(mf_batch),
                                           ctypes.POINTER(ctypes.c_uint64)]),
     'mf_prng_split': (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32,
