@@ -88,7 +88,7 @@ struct TopoDev {
 
 // Byte layout of one condition's resident workspace (global memory).
 struct SlotLayout {
-  size_t x, xb_state, xb_bound, xb_near, xb_ax, tm, thin_bound, misc, cum_xb, pabs, cum_tm,
+  size_t x, xb_state, xb_bound, xb_near, xb_ax, xb_key, tm, thin_bound, misc, cum_xb, pabs, cum_tm,
       coef, vec, total;
 };
 
@@ -102,6 +102,7 @@ MF_HD SlotLayout slot_layout(int n_dof, int X, int S, int n_bins, int coef_float
   L.xb_bound = o; o = align_up(o + 2 * X, 16);
   L.xb_near = o; o = align_up(o + 2 * X, 16);
   L.xb_ax = o; o = align_up(o + 4 * X, 16);
+  L.xb_key = o; o = align_up(o + 2 * X, 16);
   L.tm = o; o = align_up(o + S, 16);
   L.thin_bound = o; o = align_up(o + 2 * S, 16);
   L.misc = o; o = align_up(o + 64 * sizeof(double), 16);

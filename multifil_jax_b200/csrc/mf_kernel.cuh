@@ -32,6 +32,12 @@ __host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, bool vec_
   add(sizeof(int16_t) * X);                // blist
   add(sizeof(int) * 4);                    // nbound
   add(sizeof(int) * 32);                   // wsum
+  add(sizeof(int16_t) * X);                // xb_key
+  if (!vec_global) {                       // old-state snapshot
+    add(sizeof(float) * t.n_thick_nodes);
+    add(X);
+    add(sizeof(int16_t) * X);
+  }
   return o;
 }
 
@@ -65,107 +71,96 @@ __device__ void carve(Sim<NT>& m, char* base, bool vec_global) {
   m.s.blist = (int16_t*)take(sizeof(int16_t) * X);
   m.s.nbound = (int*)take(sizeof(int) * 4);
   m.s.wsum = (int*)take(sizeof(int) * 32);
+  m.s.xb_key = (int16_t*)take(sizeof(int16_t) * X);
+  if (!vec_global) {
+    m.s.old_thick = (float*)take(sizeof(float) * t.n_thick_nodes);
+    m.s.old_xbs = (int8_t*)take(X);
+    m.s.old_key = (int16_t*)take(sizeof(int16_t) * X);
+  } else {
+    // the persisted copies are only rewritten at the end of a launch, so
+    // they double as snapshot space meanwhile
+    m.s.old_thick = reinterpret_cast<float*>(m.ws + m.L.x);
+    m.s.old_xbs = reinterpret_cast<int8_t*>(m.ws + m.L.xb_state);
+    m.s.old_key = reinterpret_cast<int16_t*>(m.ws + m.L.xb_near);
+  }
 }
 
 // ---------------------------------------------------------------------------
 // metrics epilogue (metrics_fn.py:154-417), written to metrics[b][k][t]
 // ---------------------------------------------------------------------------
 template <int NT>
-__device__ void metrics(Sim<NT>& m, int t, float zl, float pCa, float new_ls, float force,
-                        double resid, int iters, const float* old_x_thick, const int8_t* old_xb,
-                        const int8_t* old_tm_unused, const int16_t* old_near, const float* old_ax,
-                        const int8_t* old_tm, float* Mo) {
+__device__ void metrics(Sim<NT>& m, int t, float zl, float pCa, float new_ls, float force, double resid,
+                        int iters, float* Mo) {
   const TopoDev& T = m.T;
   const int X = T.total_xbs, S = T.n_sites_total, NTN = T.n_thick_nodes;
   const int tid = m.tid;
   const float* pabs = reinterpret_cast<const float*>(m.ws + m.L.pabs);
-  // integer counts: 6 xb states, bound, 4 tm, overlap n/n2/n3, atp, newly
-  int ci[15] = {0};
-  float cf[4] = {0.f, 0.f, 0.f, 0.f};  // thick disp sum, thin disp sum, dx sum, atp_p
-  float tear = 0.f;
-  float tmin = INFINITY, tmax = -INFINITY, nmin = INFINITY, nmax = -INFINITY;
+  const float* old_x = m.s.old_thick;
+  // per-thread partials: counts (exact in float), sums, extrema
+  float c_xb[7] = {0, 0, 0, 0, 0, 0, 0};  // 6 states + bound
+  float c_tm[4] = {0, 0, 0, 0};
+  float ov = 0.f, ov2 = 0.f, ov3 = 0.f, atp = 0.f, newly = 0.f, atp_p = 0.f, tear = 0.f;
   const float near_b = T.crown_min - 13.0f, far_b = T.crown_max + 13.0f;
   for (int i = tid; i < X; i += NT) {
-    const int sn = m.s.xb_state[i], so = old_xb[i];
-    ci[sn] += 1;
-    ci[6] += (sn >= 1 && sn <= 3);
-    ci[13] += (so == 3) && (sn == 4 || sn == 0);
-    ci[14] += (so == 0) && (sn == 1);
-    if (so >= 2 && so <= 3) {
-      // P_abs on the pre-step geometry (metrics_fn.py:297-338)
-      const int thin = m.thin_of(i);
-      const int near = old_near[i];
-      const int site = near < 0 ? 0 : (near > T.n_sites - 1 ? T.n_sites - 1 : near);
-      const bool perm = (old_tm[thin * T.n_sites + site] == 3) && T.xb_valid[i];
-      const int key = (perm ? T.n_bins : 0) + m.bin_of(old_ax[i]);
-      if (so == 3) cf[3] += pabs[key * 3 + 0];
+    const int sn = m.s.xb_state[i], so = m.s.old_xbs[i];
+    c_xb[sn] += 1.f;
+    c_xb[6] += (sn >= 1 && sn <= 3);
+    atp += (so == 3) && (sn == 4 || sn == 0);
+    newly += (so == 0) && (sn == 1);
+    if (so == 2 || so == 3) {
+      // expected exits from the absorbing generator at the pre-step geometry
+      // (metrics_fn.py:297-338); its table row is the one sampled last step
+      const int key = m.s.old_key[i];
+      if (so == 3) atp_p += pabs[key * 3 + 0];
       tear += pabs[key * 3 + (so == 2 ? 1 : 2)];
     }
   }
-  for (int g = tid; g < S; g += NT) {
-    const int st = m.s.tm[g];
-    ci[7 + st] += 1;
-    float xa;
-    if (!m.precise) xa = m.s.x[NTN + g];
-    else xa = (float)((m.zref - (double)T.bind_off[g]) + (double)m.s.x[NTN + g]);
-    const bool ov = xa >= near_b && xa <= far_b && xa > 0.0f;
-    ci[11] += ov;
-    ci[12] += ov && st == 2;
-    // n3 overlap stored after: reuse ci[14]? keep separate below
-  }
-  int c3o = 0;
-  for (int g = tid; g < S; g += NT) {
-    float xa;
-    if (!m.precise) xa = m.s.x[NTN + g];
-    else xa = (float)((m.zref - (double)T.bind_off[g]) + (double)m.s.x[NTN + g]);
-    const bool ov = xa >= near_b && xa <= far_b && xa > 0.0f;
-    c3o += ov && m.s.tm[g] == 3;
-  }
-  // displacements
+  // displacement statistics: one pass around a provisional shift (the first
+  // node), var = E[(x-s)^2] - (E[x]-s)^2 with s near the mean
+  const float t_shift = m.precise ? m.s.x[0] : m.s.x[0] - T.crown_off[0];
+  float n_shift;
+  if (!m.precise) n_shift = m.s.x[NTN] - T.thin_cum[0];
+  else n_shift = (float)((m.zref - (double)T.bind_off[0]) + (double)m.s.x[NTN] - (double)T.thin_cum[0]);
+  float tsum = 0.f, tsq = 0.f, nsum = 0.f, nsq = 0.f, dxs = 0.f;
+  float tmin = INFINITY, tmax = -INFINITY, nmin = INFINITY, nmax = -INFINITY;
   for (int i = tid; i < NTN; i += NT) {
     const float dsp = m.precise ? m.s.x[i] : m.s.x[i] - T.crown_off[i];
-    cf[0] += dsp;
+    const float c = dsp - t_shift;
+    tsum += c;
+    tsq = fmaf(c, c, tsq);
     tmin = fminf(tmin, dsp);
     tmax = fmaxf(tmax, dsp);
-    cf[2] += m.s.x[i] - old_x_thick[i];
+    dxs += m.s.x[i] - old_x[i];
   }
   for (int g = tid; g < S; g += NT) {
-    float dsp;
-    if (!m.precise) dsp = m.s.x[NTN + g] - T.thin_cum[g];
-    else dsp = (float)((m.zref - (double)T.bind_off[g]) + (double)m.s.x[NTN + g] - (double)T.thin_cum[g]);
-    cf[1] += dsp;
+    const int st = m.s.tm[g];
+    c_tm[st] += 1.f;
+    float xa, dsp;
+    if (!m.precise) {
+      xa = m.s.x[NTN + g];
+      dsp = xa - T.thin_cum[g];
+    } else {
+      const double xd = (m.zref - (double)T.bind_off[g]) + (double)m.s.x[NTN + g];
+      xa = (float)xd;
+      dsp = (float)(xd - (double)T.thin_cum[g]);
+    }
+    const bool o = xa >= near_b && xa <= far_b && xa > 0.0f;
+    ov += o;
+    ov2 += o && st == 2;
+    ov3 += o && st == 3;
+    const float c = dsp - n_shift;
+    nsum += c;
+    nsq = fmaf(c, c, nsq);
     nmin = fminf(nmin, dsp);
     nmax = fmaxf(nmax, dsp);
   }
-  // one reduction: 4 maxima (min as -max), 16 counts, 5 sums
-  float red[25];
-  red[0] = -tmin; red[1] = tmax; red[2] = -nmin; red[3] = nmax;
-#pragma unroll
-  for (int k = 0; k < 15; ++k) red[4 + k] = (float)ci[k];
-  red[19] = (float)c3o;
-  red[20] = cf[0]; red[21] = cf[1]; red[22] = cf[2]; red[23] = cf[3]; red[24] = tear;
-  m.template bred<25>(red, 4);
-  tmin = -red[0]; tmax = red[1]; nmin = -red[2]; nmax = red[3];
-  int cnt[16];
-#pragma unroll
-  for (int k = 0; k < 16; ++k) cnt[k] = (int)red[4 + k];
-  float sums[5] = {red[20], red[21], red[22], red[23], red[24]};
-  const float tmean = sums[0] / (float)NTN, nmean = sums[1] / (float)S;
-  float sq[2] = {0.f, 0.f};
-  for (int i = tid; i < NTN; i += NT) {
-    const float dsp = m.precise ? m.s.x[i] : m.s.x[i] - T.crown_off[i];
-    const float c = dsp - tmean;
-    sq[0] += c * c;
-  }
-  for (int g = tid; g < S; g += NT) {
-    float dsp;
-    if (!m.precise) dsp = m.s.x[NTN + g] - T.thin_cum[g];
-    else dsp = (float)((m.zref - (double)T.bind_off[g]) + (double)m.s.x[NTN + g] - (double)T.thin_cum[g]);
-    const float c = dsp - nmean;
-    sq[1] += c * c;
-  }
-  m.template bred<2>(sq, 0);
+  float r[29] = {-tmin, tmax, -nmin, nmax,
+                 c_xb[0], c_xb[1], c_xb[2], c_xb[3], c_xb[4], c_xb[5], c_xb[6],
+                 c_tm[0], c_tm[1], c_tm[2], c_tm[3], ov, ov2, ov3, atp, newly,
+                 tsum, tsq, nsum, nsq, dxs, atp_p, tear, 0.f, 0.f};
+  m.template bred<29>(r, 4);
   if (tid == 0) {
+    tmin = -r[0]; tmax = r[1]; nmin = -r[2]; nmax = r[3];
     const float nx = (float)X, nt = (float)S;
     const float* P = m.s.P;
     auto put = [&](int k, float v) { Mo[(size_t)k * m.Tstride + t] = v; };
@@ -174,37 +169,37 @@ __device__ void metrics(Sim<NT>& m, int t, float zl, float pCa, float new_ls, fl
     put(M_Z_LINE, zl);
     put(M_PCA, pCa);
     put(M_LATTICE_SPACING, new_ls);
-    const float nb = (float)cnt[6];
+    const float nb = r[10];
     put(M_N_BOUND, nb);
-    for (int k = 0; k < 6; ++k) put(M_N_XB_DRX + k, (float)cnt[k]);
+    for (int k = 0; k < 6; ++k) put(M_N_XB_DRX + k, r[4 + k]);
     put(M_FRAC_XB_BOUND, nb / nx);
-    for (int k = 0; k < 6; ++k) put(M_FRAC_XB_DRX + k, (float)cnt[k] / nx);
-    for (int k = 0; k < 4; ++k) put(M_N_TM_0 + k, (float)cnt[7 + k]);
-    for (int k = 0; k < 4; ++k) put(M_FRAC_TM_0 + k, (float)cnt[7 + k] / nt);
-    put(M_ACTIN_PERM, (float)cnt[10] / nt);
-    const float nov = (float)cnt[11];
-    const float n2 = (float)cnt[12], n3 = (float)cnt[15];
+    for (int k = 0; k < 6; ++k) put(M_FRAC_XB_DRX + k, r[4 + k] / nx);
+    for (int k = 0; k < 4; ++k) put(M_N_TM_0 + k, r[11 + k]);
+    for (int k = 0; k < 4; ++k) put(M_FRAC_TM_0 + k, r[11 + k] / nt);
+    put(M_ACTIN_PERM, r[14] / nt);
+    const float nov = r[15], n2 = r[16], n3 = r[17];
     put(M_FRAC_TM_2_OV, n2 / nov);
     put(M_FRAC_TM_3_OV, n3 / nov);
     put(M_FRAC_TM_AVAIL_OV, (n2 + n3) / nov);
     put(M_N_OVERLAP, nov);
-    put(M_ATP_CONSUMED, (float)cnt[13]);
-    put(M_NEWLY_BOUND, (float)cnt[14]);
-    put(M_THICK_D_MEAN, tmean);
+    put(M_ATP_CONSUMED, r[18]);
+    put(M_NEWLY_BOUND, r[19]);
+    const float tmean_c = r[20] / (float)NTN, nmean_c = r[22] / (float)S;
+    put(M_THICK_D_MEAN, t_shift + tmean_c);
     put(M_THICK_D_MAX, tmax);
     put(M_THICK_D_MIN, tmin);
-    put(M_THICK_D_STD, sqrtf(sq[0] / (float)NTN));
-    put(M_THIN_D_MEAN, nmean);
+    put(M_THICK_D_STD, sqrtf(fmaxf(r[21] / (float)NTN - tmean_c * tmean_c, 0.f)));
+    put(M_THIN_D_MEAN, n_shift + nmean_c);
     put(M_THIN_D_MAX, nmax);
     put(M_THIN_D_MIN, nmin);
-    put(M_THIN_D_STD, sqrtf(sq[1] / (float)S));
-    // energies over thick filaments (sequential, small)
+    put(M_THIN_D_STD, sqrtf(fmaxf(r[23] / (float)S - nmean_c * nmean_c, 0.f)));
+    // energies over thick filaments (metrics_fn.py:262-288)
     float e_new = 0.f, e_delta = 0.f, te_new = 0.f, te_delta = 0.f;
     const float k = P[THICK_K];
     for (int th = 0; th < T.n_thick; ++th) {
       const int n0 = th * T.n_crowns;
       const float u_new = m.precise ? m.s.x[n0] : m.s.x[n0] - T.crown_off[n0];
-      const float u_old = m.precise ? old_x_thick[n0] : old_x_thick[n0] - T.crown_off[n0];
+      const float u_old = m.precise ? old_x[n0] : old_x[n0] - T.crown_off[n0];
       const float en = 0.5f * k * (u_new * u_new);
       const float eo = 0.5f * k * (u_old * u_old);
       e_new += en;
@@ -213,11 +208,11 @@ __device__ void metrics(Sim<NT>& m, int t, float zl, float pCa, float new_ls, fl
       float ad_new, ad_old;
       if (!m.precise) {
         ad_new = zl - m.s.x[nl];
-        ad_old = zl - old_x_thick[nl];
+        ad_old = zl - old_x[nl];
       } else {
         const float zc = (float)((double)zl - (double)T.crown_off[nl]);
         ad_new = zc - m.s.x[nl];
-        ad_old = zc - old_x_thick[nl];
+        ad_old = zc - old_x[nl];
       }
       const float a = P[TITIN_A], bb = P[TITIN_B], r0 = P[TITIN_REST];
       const float Ln = sqrtf(ad_new * ad_new + new_ls * new_ls);
@@ -232,15 +227,14 @@ __device__ void metrics(Sim<NT>& m, int t, float zl, float pCa, float new_ls, fl
     put(M_THICK_E_DELTA, e_delta / fth);
     put(M_TITIN_E_AVG, te_new / fth);
     put(M_TITIN_E_DELTA, te_delta / fth);
-    const float work = force * (sums[2] / (float)NTN);
+    const float work = force * (r[24] / (float)NTN);
     put(M_WORK_THICK, work);
     put(M_WORK_THICK_MEAN, work / (float)NTN);
-    put(M_ATP_EXPECTED_P, sums[3]);
-    put(M_XB_TEAR, sums[4]);
-    put(M_WORK_PER_ATP, sums[3] > 0.01f ? work / sums[3] : 0.0f);
+    put(M_ATP_EXPECTED_P, r[25]);
+    put(M_XB_TEAR, r[26]);
+    put(M_WORK_PER_ATP, r[25] > 0.01f ? work / r[25] : 0.0f);
     put(M_NEWTON_ITERS, (float)iters);
   }
-  (void)old_tm_unused;
 }
 
 // ---------------------------------------------------------------------------
@@ -294,6 +288,7 @@ __device__ void run_condition(const StepArgs& A, int ci) {
   int8_t* xbs_g = reinterpret_cast<int8_t*>(m.ws + m.L.xb_state);
   int16_t* xbb_g = reinterpret_cast<int16_t*>(m.ws + m.L.xb_bound);
   int16_t* xbn_g = reinterpret_cast<int16_t*>(m.ws + m.L.xb_near);
+  int16_t* xbk_g = reinterpret_cast<int16_t*>(m.ws + m.L.xb_key);
   float* xba_g = reinterpret_cast<float*>(m.ws + m.L.xb_ax);
   int8_t* tm_g = reinterpret_cast<int8_t*>(m.ws + m.L.tm);
   int16_t* tb_g = reinterpret_cast<int16_t*>(m.ws + m.L.thin_bound);
@@ -337,6 +332,8 @@ __device__ void run_condition(const StepArgs& A, int ci) {
     __syncthreads();
     m.nearest(m.s.P[LATTICE_SPACING]);
     __syncthreads();
+    // table rows of the initial geometry (every site starts in state 0: block 0)
+    for (int i = m.tid; i < X; i += NT) m.s.xb_key[i] = (int16_t)m.bin_of(m.s.xb_ax[i]);
     double resid;
     int it;
     float d0 = m.s.P[LATTICE_SPACING];
@@ -365,6 +362,7 @@ __device__ void run_condition(const StepArgs& A, int ci) {
       m.s.xb_bound[i] = xbb_g[i];
       m.s.xb_near[i] = xbn_g[i];
       m.s.xb_ax[i] = xba_g[i];
+      m.s.xb_key[i] = xbk_g[i];
     }
     for (int g = m.tid; g < S; g += NT) {
       m.s.tm[g] = tm_g[g];
@@ -417,13 +415,11 @@ __device__ void run_condition(const StepArgs& A, int ci) {
     // old_state snapshot for the metrics (metrics_fn.py reads the pre-step
     // geometry): parked in the resident workspace arrays, which are only
     // rewritten with the live state at the end of the launch.
-    for (int i = m.tid; i < NTN; i += NT) xg[i] = m.s.x[i];
+    for (int i = m.tid; i < NTN; i += NT) m.s.old_thick[i] = m.s.x[i];
     for (int i = m.tid; i < X; i += NT) {
-      xbs_g[i] = m.s.xb_state[i];
-      xbn_g[i] = m.s.xb_near[i];
-      xba_g[i] = m.s.xb_ax[i];
+      m.s.old_xbs[i] = m.s.xb_state[i];
+      m.s.old_key[i] = m.s.xb_key[i];
     }
-    for (int g = m.tid; g < S; g += NT) tm_g[g] = m.s.tm[g];
     __syncthreads();
     // 2-4. kinetics
     __shared__ uint32_t sub_thin[2], sub_thick[2];
@@ -476,7 +472,7 @@ __device__ void run_condition(const StepArgs& A, int ci) {
     __syncthreads();
     force = m.s.red[1535];
     __syncthreads();
-    metrics(m, t, zl, pCa, new_ls, force, resid, iters, xg, xbs_g, nullptr, xbn_g, xba_g, tm_g, Mo);
+    metrics(m, t, zl, pCa, new_ls, force, resid, iters, Mo);
     if (resid > (double)A.resid_warn) m.status |= 2;
     MF_PH(10);
     // optional traces
@@ -513,6 +509,7 @@ __device__ void run_condition(const StepArgs& A, int ci) {
     xbb_g[i] = m.s.xb_bound[i];
     xbn_g[i] = m.s.xb_near[i];
     xba_g[i] = m.s.xb_ax[i];
+    xbk_g[i] = m.s.xb_key[i];
   }
   for (int g = m.tid; g < S; g += NT) {
     tm_g[g] = m.s.tm[g];

@@ -111,6 +111,12 @@ struct Smem {
   int16_t* blist; // [X] heads carrying force this step, increasing index
   int* nbound;    // [1] length of blist
   int* wsum;      // [32] per-warp counts of the compaction scan
+  // pre-step (old_state) snapshot read by the metrics epilogue: shared memory
+  // when the lattice leaves room, else the resident workspace arrays
+  float* old_thick;  // [n_thick*n_crowns]
+  int8_t* old_xbs;   // [X]
+  int16_t* old_key;  // [X] table row (permissiveness, bin) of the pre-step geometry
+  int16_t* xb_key;   // [X] table row used by the latest crossbridge sampling
 };
 
 // Thomas coefficient block layout inside coef (floats).
@@ -963,6 +969,7 @@ struct Sim {
       const int tgt = thin * T.n_sites + site;
       const bool perm = (s.tm[tgt] == 3) && T.xb_valid[i];
       const int key = (perm ? T.n_bins : 0) + bin_of(s.xb_ax[i]);
+      s.xb_key[i] = (int16_t)key;
       const int old = s.xb_state[i];
       const float* c = cum_xb + key * 36 + old * 6;
       const float u = uniform_of(sub, X, i, A.u_xb, inj_off);
