@@ -135,7 +135,7 @@ int mf_workspace_bytes(mf_ctx* ctx, const mf_batch* batch, uint64_t* bytes);
  * launch descriptor table) comes from one 8 MiB array compiled into the
  * library (present on every device that loads it, until process exit); the
  * call never allocates.  A batch whose scratch exceeds 8 MiB is rejected with
- * MF_ERR_NOMEM and a message naming both sizes (at 2x2 about 75 conditions
+ * MF_ERR_NOMEM and a message naming both sizes (at 2x2 about 70 conditions
  * fit).  Batched single-launch path only: MF_FLAG_PLAIN and chunk_steps > 0
  * are rejected.  The first call on a device resolves the array's device
  * address, so make it before any stream capture.  Every call reuses the same

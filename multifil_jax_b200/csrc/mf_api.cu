@@ -254,9 +254,9 @@ int mf_upload_topology(mf_ctx* ctx, const mf_topo_desc* d, int32_t* topo_id) {
   CK(cudaMemcpy(t->d_struct, &td, sizeof(TopoDev), cudaMemcpyHostToDevice));
   t->threads = default_threads(td);
   size_t sm = smem_bytes(td, t->threads, false);
-  t->vec_global = sm + 256 > (size_t)ctx->smem_optin;
+  t->vec_global = sm + kStaticSmem > (size_t)ctx->smem_optin;
   t->smem_local = smem_bytes(td, t->threads, t->vec_global);
-  if (t->smem_local + 256 > (size_t)ctx->smem_optin)
+  if (t->smem_local + kStaticSmem > (size_t)ctx->smem_optin)
     return fail(ctx, MF_ERR_INVALID, "lattice needs %zu B shared memory (limit %d)", t->smem_local,
                 ctx->smem_optin);
   ctx->topos.push_back(std::move(t));
@@ -272,9 +272,9 @@ int mf_tune_threads(mf_ctx* ctx, int32_t topo_id, int32_t threads) {
     return fail(ctx, MF_ERR_INVALID, "threads must be 128, 256, 512 or 1024");
   TopoHost& t = *ctx->topos[topo_id];
   size_t sm = smem_bytes(t.dev, threads, false);
-  bool vg = sm > (size_t)ctx->smem_optin;
+  bool vg = sm + kStaticSmem > (size_t)ctx->smem_optin;
   sm = smem_bytes(t.dev, threads, vg);
-  if (sm > (size_t)ctx->smem_optin) return fail(ctx, MF_ERR_INVALID, "does not fit");
+  if (sm + kStaticSmem > (size_t)ctx->smem_optin) return fail(ctx, MF_ERR_INVALID, "does not fit");
   t.threads = threads;
   t.vec_global = vg;
   t.smem_local = sm;

@@ -110,7 +110,7 @@ MF_HD SlotLayout slot_layout(int n_dof, int X, int S, int n_bins, int coef_float
   L.pabs = o; o = align_up(o + sizeof(float) * 2 * n_bins * 3, 16);
   L.cum_tm = o; o = align_up(o + sizeof(float) * 27 * 16, 16);
   L.coef = o; o = align_up(o + sizeof(float) * coef_floats, 16);
-  L.vec = o; o = align_up(o + sizeof(float) * (5 * n_dof + 4 * X), 16);  // CG vectors + head terms when not in smem
+  L.vec = o; o = align_up(o + sizeof(float) * (7 * n_dof + 4 * X), 16);  // CG vectors + head terms when not in smem
   L.total = align_up(o, 256);
   return L;
 }

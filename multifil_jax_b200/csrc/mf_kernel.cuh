@@ -5,6 +5,11 @@
 
 namespace mf {
 
+// Static shared memory of the kernel (the CTA-shared lattice, carve and
+// condition structs of run_condition, about 1 KB) plus headroom; the dynamic
+// carve below must fit in the opt-in limit next to it.
+constexpr size_t kStaticSmem = 2048;
+
 // Shared-memory bytes needed by one condition of this lattice with NT threads.
 __host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, bool vec_global) {
   const int N = t.n_dof, X = t.total_xbs, S = t.n_sites_total;
@@ -15,7 +20,7 @@ __host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, bool vec_
   auto add = [&](size_t bytes) { o = align_up(o + bytes, 16); };
   add(sizeof(double) * 64);                // redd
   add(sizeof(float) * 1536);               // red
-  if (!vec_global) add(sizeof(float) * 5 * N);  // x r dx pv zz
+  if (!vec_global) add(sizeof(float) * 7 * N);  // x r dx pv zz wv sv
   if (!vec_global) add(sizeof(float) * 4 * X);  // fxb fdx fdd frdd
   add(sizeof(float) * X);                  // xb_ax
   add(sizeof(float) * S);                  // site / win1
@@ -33,6 +38,11 @@ __host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, bool vec_
   add(sizeof(int) * 4);                    // nbound
   add(sizeof(int) * 32);                   // wsum
   add(sizeof(int16_t) * X);                // xb_key
+  add(sizeof(int16_t) * X);                // hsite
+  add(sizeof(int16_t) * 2 * S);            // site_h
+  if (!vec_global) add(sizeof(int16_t) * 6 * N);  // nb_node nb_head
+  add(sizeof(double) * t.n_thin * 3 * t.width);  // face_pos
+  add(3 * t.n_thin * 3);                   // face_mono face_kl face_kh
   if (!vec_global) {                       // old-state snapshot
     add(sizeof(float) * t.n_thick_nodes);
     add(X);
@@ -50,9 +60,10 @@ __device__ void carve(Sim<NT>& m, char* base, bool vec_global) {
   auto take = [&](size_t bytes) { char* p = base + o; o = align_up(o + bytes, 16); return p; };
   m.s.redd = (double*)take(sizeof(double) * 64);
   m.s.red = (float*)take(sizeof(float) * 1536);
-  float* v5 = vec_global ? reinterpret_cast<float*>(m.ws + m.L.vec) : (float*)take(sizeof(float) * 5 * N);
-  m.s.x = v5; m.s.r = v5 + N; m.s.dx = v5 + 2 * N; m.s.pv = v5 + 3 * N; m.s.zz = v5 + 4 * N;
-  float* f4 = vec_global ? reinterpret_cast<float*>(m.ws + m.L.vec) + 5 * N : (float*)take(sizeof(float) * 4 * X);
+  float* v7 = vec_global ? reinterpret_cast<float*>(m.ws + m.L.vec) : (float*)take(sizeof(float) * 7 * N);
+  m.s.x = v7; m.s.r = v7 + N; m.s.dx = v7 + 2 * N; m.s.pv = v7 + 3 * N; m.s.zz = v7 + 4 * N;
+  m.s.wv = v7 + 5 * N; m.s.sv = v7 + 6 * N;
+  float* f4 = vec_global ? reinterpret_cast<float*>(m.ws + m.L.vec) + 7 * N : (float*)take(sizeof(float) * 4 * X);
   m.s.fxb = f4; m.s.fdx = f4 + X; m.s.fdd = f4 + 2 * X; m.s.frdd = f4 + 3 * X;
   m.s.xb_ax = (float*)take(sizeof(float) * X);
   m.s.site = (float*)take(sizeof(float) * S);
@@ -72,6 +83,18 @@ __device__ void carve(Sim<NT>& m, char* base, bool vec_global) {
   m.s.nbound = (int*)take(sizeof(int) * 4);
   m.s.wsum = (int*)take(sizeof(int) * 32);
   m.s.xb_key = (int16_t*)take(sizeof(int16_t) * X);
+  m.s.hsite = (int16_t*)take(sizeof(int16_t) * X);
+  m.s.site_h = (int16_t*)take(sizeof(int16_t) * 2 * S);
+  m.s.face_pos = (double*)take(sizeof(double) * t.n_thin * 3 * t.width);
+  m.s.face_mono = (int8_t*)take(3 * t.n_thin * 3);
+  m.s.face_kl = m.s.face_mono + t.n_thin * 3;
+  m.s.face_kh = m.s.face_kl + t.n_thin * 3;
+  if (!vec_global) {
+    m.s.nb_node = (int16_t*)take(sizeof(int16_t) * 6 * N);
+    m.s.nb_head = m.s.nb_node + 3 * N;
+  } else {
+    m.s.nb_node = m.s.nb_head = nullptr;
+  }
   if (!vec_global) {
     m.s.old_thick = (float*)take(sizeof(float) * t.n_thick_nodes);
     m.s.old_xbs = (int8_t*)take(X);
@@ -103,7 +126,8 @@ __device__ void metrics(Sim<NT>& m, int t, float zl, float pCa, float new_ls, fl
   const float near_b = T.crown_min - 13.0f, far_b = T.crown_max + 13.0f;
   for (int i = tid; i < X; i += NT) {
     const int sn = m.s.xb_state[i], so = m.s.old_xbs[i];
-    c_xb[sn] += 1.f;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) c_xb[k] += (sn == k);  // compile-time indices keep the counts in registers
     c_xb[6] += (sn >= 1 && sn <= 3);
     atp += (so == 3) && (sn == 4 || sn == 0);
     newly += (so == 0) && (sn == 1);
@@ -134,7 +158,8 @@ __device__ void metrics(Sim<NT>& m, int t, float zl, float pCa, float new_ls, fl
   }
   for (int g = tid; g < S; g += NT) {
     const int st = m.s.tm[g];
-    c_tm[st] += 1.f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) c_tm[k] += (st == k);
     float xa, dsp;
     if (!m.precise) {
       xa = m.s.x[NTN + g];
@@ -265,22 +290,38 @@ __device__ void run_condition(const StepArgs& A, int ci) {
   int ph_cur = 0;
 #endif
   extern __shared__ __align__(16) char smem_raw[];
-  const CondDesc cd = A.cond[ci];
-  const TopoDev& T = *cd.topo;
-  Sim<NT> m(T, A);
+  __shared__ CondDesc sh_cd;
+  __shared__ TopoDev sh_T;
+  __shared__ Smem sh_s;
+  __shared__ CoefLayout sh_cl;
+  __shared__ SlotLayout sh_L;
+  if (threadIdx.x == 0) {
+    sh_cd = A.cond[ci];
+    sh_T = *sh_cd.topo;
+    sh_cl = coef_layout(sh_T);
+    sh_L = slot_layout(sh_T.n_dof, sh_T.total_xbs, sh_T.n_sites_total, sh_T.n_bins, sh_cl.total);
+  }
+  __syncthreads();
+  const CondDesc& cd = sh_cd;
+  const TopoDev& T = sh_T;
+  Sim<NT> m(T, A, sh_s, sh_cl, sh_L);
   m.tid = threadIdx.x;
   m.lane = m.tid & 31;
   m.warp = m.tid >> 5;
   m.b = cd.index;
   m.ws = cd.ws;
-  m.cl = coef_layout(T);
-  m.L = slot_layout(T.n_dof, T.total_xbs, T.n_sites_total, T.n_bins, m.cl.total);
   m.dyn = (A.flags & FLAG_DYN) != 0;
   m.precise = (A.flags & FLAG_PRECISE) != 0;
   m.part = (A.flags & FLAG_ORIG_PRNG) == 0;
   m.status = 0;
   m.Tstride = cd.T;
-  carve(m, smem_raw, (A.flags & 64) != 0);
+  if (m.tid == 0) carve(m, smem_raw, (A.flags & 64) != 0);
+  __syncthreads();
+  {
+    const int nf = T.n_thick + T.n_thin;
+    m.regcg = m.precise && A.n_cg > 0 && (A.flags & 64) == 0 && nf <= Sim<NT>::RF * (NT / 32) &&
+              T.n_crowns <= 32 * Sim<NT>::RE && T.n_sites <= 32 * Sim<NT>::RE && T.nxb <= 3;
+  }
   const int b = m.b;
   const int N = T.n_dof, X = T.total_xbs, S = T.n_sites_total, NTN = T.n_thick_nodes;
   double* misc = reinterpret_cast<double*>(m.ws + m.L.misc);
@@ -500,6 +541,7 @@ __device__ void run_condition(const StepArgs& A, int ci) {
   if (m.tid == 0 && A.x_trace) {
     float* o = A.x_trace + (size_t)b * A.T * A.max_dof;
     for (int k = 0; k < 12; ++k) o[k] = (float)ph_acc[k];
+    for (int k = 0; k < 8; ++k) o[12 + k] = (float)m.sub_acc[k];
   }
 #endif
   // ---- write back resident state ----

@@ -88,6 +88,8 @@ struct Smem {
   float* dx;      // [N] CG solution
   float* pv;      // [N] CG direction
   float* zz;      // [N] preconditioned residual / J p
+  float* wv;      // [N] A u (precise-mode CG)
+  float* sv;      // [N] A p (precise-mode CG)
   float* fxb;     // [X] per-head force or directional term
   float* fdx;     // [X] per-head df/dx at the current Newton point
   float* site;    // [S] per-site crossbridge accumulator (aliases win1 in kinetics)
@@ -109,6 +111,14 @@ struct Smem {
   float* fdd;     // [X] df/dd per head (dynamic spacing)
   float* frdd;    // [X] d(radial)/dd per head (dynamic spacing)
   int16_t* blist; // [X] heads carrying force this step, increasing index
+  int16_t* hsite; // [X] global site of a force-carrying head, else -1
+  int16_t* site_h;// [2S] first two force-carrying heads of every site
+  int16_t* nb_node; // [3N] partner nodes of every node (register CG only)
+  int16_t* nb_head; // [3N] the heads behind them
+  double* face_pos; // [n_thin*3*width] staged candidate positions (NaN = invalid)
+  int8_t* face_mono;// [n_thin*3] 0 scan, 1 increasing, 2 decreasing, 3 no candidate
+  int8_t* face_kl;  // [n_thin*3] first valid candidate
+  int8_t* face_kh;  // [n_thin*3] last valid candidate
   int* nbound;    // [1] length of blist
   int* wsum;      // [32] per-warp counts of the compaction scan
   // pre-step (old_state) snapshot read by the metrics epilogue: shared memory
@@ -139,15 +149,19 @@ __host__ __device__ inline CoefLayout coef_layout(const TopoDev& t) {
 template <int NT>
 struct Sim {
   static constexpr int NW = NT / 32;
+  // The lattice, the shared-memory carve and the layouts live in CTA-shared
+  // structs at fixed addresses: reading a field is one shared load, and none
+  // of the ~50 pointers and sizes occupies a register across the step loop.
   const TopoDev& T;
   const StepArgs& A;
-  Smem s;
-  CoefLayout cl;
-  SlotLayout L;
+  Smem& s;
+  CoefLayout& cl;
+  SlotLayout& L;
   char* ws;
   int b;        // caller row
   int tid, lane, warp;
   bool dyn, precise, part;
+  bool regcg;   // register-resident precise Newton-CG (solve_regs)
   float Kl, nu_c, dtm;
   double zref;  // precise mode thin reference z
   float dvar;   // lattice spacing unknown (dynamic) / fixed spacing
@@ -155,8 +169,27 @@ struct Sim {
   int status;
   int Tstride;
   int redbuf = 0;
+#ifdef MF_PHASE_TIMING
+  // diagnostic build only: thread 0's clock64() totals of solver sub-phases
+  long long sub_t0 = 0;
+  double sub_acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#define MF_SUB(k)                                               \
+  do {                                                          \
+    __syncthreads();                                            \
+    if (tid == 0) {                                             \
+      const long long now_ = clock64();                         \
+      if ((k) >= 0) sub_acc[(k) < 0 ? 0 : (k)] += (double)(now_ - sub_t0); \
+      sub_t0 = now_;                                            \
+    }                                                           \
+  } while (0)
+#define MF_COUNT(k) (sub_acc[k] += 1.0)
+#else
+#define MF_SUB(k) do { } while (0)
+#define MF_COUNT(k) do { } while (0)
+#endif
 
-  __device__ Sim(const TopoDev& t, const StepArgs& a) : T(t), A(a) {}
+  __device__ Sim(const TopoDev& t, const StepArgs& a, Smem& sm, CoefLayout& c, SlotLayout& l)
+      : T(t), A(a), s(sm), cl(c), L(l) {}
 
   // ------------------------------------------------------------------
   // reductions
@@ -323,18 +356,16 @@ struct Sim {
   // tree order in exact arithmetic; used in precise mode, where the
   // reference's float32 association order is not the target.
   template <int E>
-  __device__ __forceinline__ void thomas_shfl(const float* in, float* out, int n, const float* Af,
-                                              const float* Ab, const float* inv) {
-    float y[E], a[E];
+  __device__ __forceinline__ void thomas_regs(float (&y)[E], int n, const float* __restrict__ Af,
+                                              const float* __restrict__ Ab, const float* __restrict__ inv) const {
+    float a[E];
     const int i0 = lane * E;
     // forward: y[i] = a_f[i] * y[i-1] + r[i], y[-1] = 0
     float A = 1.f, Bv = 0.f;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int i = i0 + e;
-      const bool ok = i < n;
-      a[e] = ok ? Af[i] : 1.f;
-      y[e] = ok ? in[i] : 0.f;
+      a[e] = i < n ? Af[i] : 1.f;
       Bv = fmaf(a[e], Bv, y[e]);
       A = a[e] * A;
     }
@@ -378,13 +409,24 @@ struct Sim {
 #pragma unroll
     for (int e = E - 1; e >= 0; --e) {
       xp = fmaf(a[e], xp, y[e]);
-      const int i = i0 + e;
-      if (i < n) out[i] = xp;
+      y[e] = xp;
     }
+  }
+  template <int E>
+  __device__ __forceinline__ void thomas_shfl(const float* in, float* out, int n, const float* Af,
+                                              const float* Ab, const float* inv) {
+    float y[E];
+    const int i0 = lane * E;
+#pragma unroll
+    for (int e = 0; e < E; ++e) y[e] = i0 + e < n ? in[i0 + e] : 0.f;
+    thomas_regs<E>(y, n, Af, Ab, inv);
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+      if (i0 + e < n) out[i0 + e] = y[e];
   }
 
   // out = M^{-1} in on this warp's own filaments (no block barrier needed).
-  __device__ void precondition_own(const float* in, float* out) {
+  __device__ __forceinline__ void precondition_own(const float* in, float* out) {
     const int nf = T.n_thick + T.n_thin;
     if (precise) {
       __syncwarp();
@@ -509,7 +551,7 @@ struct Sim {
     const float g0 = strong ? s.P[XB_G_REST_STRONG] : s.P[XB_G_REST_WEAK];
     const float ck = strong ? s.P[XB_C_K_STRONG] : s.P[XB_C_K_WEAK];
     const float c0 = strong ? s.P[XB_C_REST_STRONG] : s.P[XB_C_REST_WEAK];
-    const int gs = thin_of(xb) * T.n_sites + bnd;
+    const int gs = s.hsite[xb];
     const float x = xb_offset(gs, crown_node(xb));
     const float r = sqrtf(x * x + d * d);
     const float rs = r > 1e-10f ? r : 1e-10f;
@@ -547,19 +589,19 @@ struct Sim {
   }
 
   // Compact list of the heads that carry force this step (states 1-3 with a
-  // site), in increasing head index (block prefix scan, deterministic), plus
-  // the number of heads on every site.  Clears the per-head and per-site
-  // accumulators.  Sites holding 3+ heads are summed in head order by their
-  // node owner (sums of two are order-free; the reference adds in index
-  // order, transitions/forces.py segment_sum).
-  __device__ void build_bound_list() {
-    const int X = T.total_xbs, S = T.n_sites_total;
-    int* cnt = s.win2;
+  // site), in increasing head index (block prefix scan, deterministic); the
+  // global site of every such head (hsite, -1 for the others); per site the
+  // number of such heads (win2) and the first two of them (site_h).  Node
+  // owners gather the crossbridge terms of their sites from these lists:
+  // sums of one or two heads are order-free, sites holding 3+ heads are
+  // summed in head order (the reference adds in index order,
+  // transitions/forces.py segment_sum).  Clears the per-head accumulator.
+  __device__ __forceinline__ void build_bound_list() {
+    const int X = T.total_xbs, S = T.n_sites_total, nsi = T.n_sites;
+    int* __restrict__ cnt = s.win2;
+    int16_t* __restrict__ site_h = s.site_h;
     __syncthreads();
-    for (int g = tid; g < S; g += NT) {
-      s.site[g] = 0.f;
-      cnt[g] = 0;
-    }
+    for (int g = tid; g < S; g += NT) cnt[g] = 0;
     __syncthreads();
     int base = 0;
     for (int c = 0; c < X; c += NT) {
@@ -568,8 +610,15 @@ struct Sim {
       if (i < X) {
         s.fxb[i] = 0.f;
         const int st = s.xb_state[i];
-        f = st >= 1 && st <= 3 && s.xb_bound[i] >= 0;
-        if (f) atomicAdd(&cnt[thin_of(i) * T.n_sites + s.xb_bound[i]], 1);
+        const int bnd = s.xb_bound[i];
+        f = st >= 1 && st <= 3 && bnd >= 0;
+        int gs = -1;
+        if (f) {
+          gs = thin_of(i) * nsi + bnd;
+          const int k = atomicAdd(&cnt[gs], 1);
+          if (k < 2) site_h[2 * gs + k] = (int16_t)i;
+        }
+        s.hsite[i] = (int16_t)gs;
       }
       const unsigned m = __ballot_sync(0xffffffffu, f);
       if (lane == 0) s.wsum[warp] = __popc(m);
@@ -588,20 +637,22 @@ struct Sim {
     __syncthreads();
   }
 
-  // crossbridge sum of a site with 3+ bound heads: -sum of fxb in head order
-  __device__ float ordered_site_sum(int g) const {
-    const int nb = *s.nbound;
+  // -sum of val(h) over the force-carrying heads of site g: in head order
+  // for 3+ heads (blist is sorted), order-free otherwise; starts from 0 like
+  // the reference's segment_sum.
+  template <class Val>
+  __device__ __forceinline__ float site_sum(int g, Val&& val) const {
+    const int c = s.win2[g];
     float acc = 0.f;
-    int prev = -1;
-    while (true) {
-      int nxt = 0x7fffffff;
-      for (int k = 0; k < nb; ++k) {
-        const int i = s.blist[k];
-        if (i > prev && i < nxt && thin_of(i) * T.n_sites + s.xb_bound[i] == g) nxt = i;
-      }
-      if (nxt == 0x7fffffff) break;
-      acc = acc + (-s.fxb[nxt]);
-      prev = nxt;
+    if (c < 3) {
+      if (c >= 1) acc = acc + (-val((int)s.site_h[2 * g]));
+      if (c >= 2) acc = acc + (-val((int)s.site_h[2 * g + 1]));
+      return acc;
+    }
+    const int nb = *s.nbound;
+    for (int k = 0; k < nb; ++k) {
+      const int h = s.blist[k];
+      if (s.hsite[h] == g) acc = acc + (-val(h));
     }
     return acc;
   }
@@ -610,8 +661,13 @@ struct Sim {
   // titin partials for the JVPs of the next Newton iteration.  Returns max|F|
   // over the augmented vector; *frad = radial residual, *jdd = dF_rad/dd.
   // In precise mode the node forces are accumulated in float64.
-  __device__ float residual(float zl, float d, float* frad, float* jdd, int bad_in, int* bad_out) {
+  __device__ __forceinline__ float residual(float zl, float d, float* frad, float* jdd, int bad_in, int* bad_out) {
     const int nb = *s.nbound;
+    const int nthk = T.n_thick, ncr = T.n_crowns, nsi = T.n_sites, ntn = T.n_thick_nodes, nxb = T.nxb;
+    const float* __restrict__ x = s.x;
+    float* __restrict__ r = s.r;
+    float* __restrict__ fxb = s.fxb;
+    float* __restrict__ tvec = s.tvec;
     float rad_part = 0.f, jdd_part = 0.f;
     const int any_bad = __syncthreads_or(bad_in);
     if (bad_out) *bad_out = any_bad;
@@ -619,7 +675,7 @@ struct Sim {
       const int i = s.blist[k];
       float f, fx, fd, frd, fr;
       xb_force(i, d, f, fx, fd, frd, fr);
-      s.fxb[i] = f;
+      fxb[i] = f;
       s.fdx[i] = fx;
       if (dyn) {
         s.fdd[i] = fd;
@@ -627,16 +683,14 @@ struct Sim {
         rad_part += fr;
         jdd_part += frd;
       }
-      const int gs = thin_of(i) * T.n_sites + s.xb_bound[i];
-      if (s.win2[gs] < 3) atomicAdd(&s.site[gs], -f);
     }
-    if (tid < T.n_thick) {
+    if (tid < nthk) {
       float ax, a_x, a_d, r_d, rad;
       titin(tid, zl, d, ax, a_x, a_d, r_d, rad);
-      s.tvec[tid] = ax;
-      s.tvec[T.n_thick + tid] = a_x;
-      s.tvec[2 * T.n_thick + tid] = a_d;
-      s.tvec[3 * T.n_thick + tid] = r_d;
+      tvec[tid] = ax;
+      tvec[nthk + tid] = a_x;
+      tvec[2 * nthk + tid] = a_d;
+      tvec[3 * nthk + tid] = r_d;
       if (dyn) {
         rad_part += rad;
         jdd_part += r_d;
@@ -644,44 +698,46 @@ struct Sim {
     }
     __syncthreads();
     const float kth = s.P[THICK_K], ktn = s.P[THIN_K];
+    const float* __restrict__ crest = T.crown_rest;
+    const float* __restrict__ brest = T.bind_rest;
+    const float* __restrict__ thc = T.thick_c;
+    const float* __restrict__ tnc = T.thin_c;
+    const double zoff = (double)zl - zref;
     float fmax = 0.f;
     own_nodes([&](int i, int f, int j, bool thick) {
       double F;
       if (thick) {
-        const int c = j;
-        float xsum = s.fxb[i * T.nxb];
-        for (int q = 1; q < T.nxb; ++q) xsum += s.fxb[i * T.nxb + q];
+        float xsum = fxb[i * nxb];
+        for (int q = 1; q < nxb; ++q) xsum += fxb[i * nxb + q];
         if (!precise) {
-          const float xm = c > 0 ? s.x[i - 1] : 0.f;
-          const float sp_c = ((s.x[i] - xm) - T.crown_rest[i]) * kth;
-          const float sp_n = (c + 1 < T.n_crowns) ? ((s.x[i + 1] - s.x[i]) - T.crown_rest[i + 1]) * kth : s.tvec[f];
+          const float xm = j > 0 ? x[i - 1] : 0.f;
+          const float sp_c = ((x[i] - xm) - crest[i]) * kth;
+          const float sp_n = (j + 1 < ncr) ? ((x[i + 1] - x[i]) - crest[i + 1]) * kth : tvec[f];
           F = (double)((sp_n - sp_c) + xsum);
         } else {
-          const double um = c > 0 ? (double)s.x[i - 1] : 0.0;
-          const double e_c = ((double)s.x[i] - um) + (double)T.thick_c[i];
-          const double spn = (c + 1 < T.n_crowns)
-                                 ? (((double)s.x[i + 1] - (double)s.x[i]) + (double)T.thick_c[i + 1]) * (double)kth
-                                 : (double)s.tvec[f];
+          const double um = j > 0 ? (double)x[i - 1] : 0.0;
+          const double e_c = ((double)x[i] - um) + (double)thc[i];
+          const double spn = (j + 1 < ncr) ? (((double)x[i + 1] - (double)x[i]) + (double)thc[i + 1]) * (double)kth
+                                           : (double)tvec[f];
           F = (spn - e_c * (double)kth) + (double)xsum;
         }
       } else {
-        const int g = i - T.n_thick_nodes;
-        const float acc = s.win2[g] < 3 ? s.site[g] : ordered_site_sum(g);
-        s.site[g] = 0.f;
+        const int g = i - ntn;
+        const float acc = site_sum(g, [&](int h) { return fxb[h]; });
         if (!precise) {
-          const float xn = (j + 1 < T.n_sites) ? s.x[i + 1] : zl;
-          const float sp_j = ((xn - s.x[i]) - T.bind_rest[g]) * ktn;
-          const float sp_m = j > 0 ? ((s.x[i] - s.x[i - 1]) - T.bind_rest[g - 1]) * ktn : 0.f;
+          const float xn = (j + 1 < nsi) ? x[i + 1] : zl;
+          const float sp_j = ((xn - x[i]) - brest[g]) * ktn;
+          const float sp_m = j > 0 ? ((x[i] - x[i - 1]) - brest[g - 1]) * ktn : 0.f;
           F = (double)((sp_j - sp_m) + acc);
         } else {
-          const double un = (j + 1 < T.n_sites) ? (double)s.x[i + 1] : 0.0;
-          double e_j = (un - (double)s.x[i]) + (double)T.thin_c[g];
-          if (j + 1 == T.n_sites) e_j += (double)zl - zref;  // anchor vs reference z
-          const double e_m = j > 0 ? ((double)s.x[i] - (double)s.x[i - 1]) + (double)T.thin_c[g - 1] : 0.0;
+          const double un = (j + 1 < nsi) ? (double)x[i + 1] : 0.0;
+          double e_j = (un - (double)x[i]) + (double)tnc[g];
+          if (j + 1 == nsi) e_j += zoff;  // anchor vs reference z
+          const double e_m = j > 0 ? ((double)x[i] - (double)x[i - 1]) + (double)tnc[g - 1] : 0.0;
           F = (e_j - e_m) * (double)ktn + (double)acc;
         }
       }
-      s.r[i] = (float)F;
+      r[i] = (float)F;
       fmax = fmaxf(fmax, (float)fabs(F));
     });
     float v[3] = {fmax, rad_part, jdd_part};
@@ -696,119 +752,151 @@ struct Sim {
     return m;
   }
 
-  // out = -(J [v, vd]) on own nodes; returns the augmented dot(v, out), *out_d
-  // the radial component.
-  __device__ float neg_jvp(const float* v, float vd, float* out, float* out_d) {
-    const int nb = *s.nbound;
-    float rad_part = 0.f;
-    __syncthreads();  // v complete
-    for (int k = tid; k < nb; k += NT) {
-      const int i = s.blist[k];
-      const int gs = thin_of(i) * T.n_sites + s.xb_bound[i];
-      const float dxd = v[T.n_thick_nodes + gs] - v[crown_node(i)];
-      float w = s.fdx[i] * dxd;
-      if (dyn) {
-        w = w + s.fdd[i] * vd;
-        rad_part += -(s.fdd[i] * dxd) - s.frdd[i] * vd;
-      }
-      s.fxb[i] = w;
-      if (s.win2[gs] < 3) atomicAdd(&s.site[gs], -w);
-    }
-    if (dyn && tid < T.n_thick) {
-      const int last = tid * T.n_crowns + T.n_crowns - 1;
-      rad_part += s.tvec[2 * T.n_thick + tid] * v[last] - s.tvec[3 * T.n_thick + tid] * vd;
-    }
-    __syncthreads();
+  // out = -(J [v, vd]) on own nodes; returns the augmented dot(v, out) and
+  // *out_d the radial component.  The crossbridge couplings are gathered by
+  // the node owners (each crown from its own heads, each site from the heads
+  // bound to it), so one barrier before and the reduction after are all the
+  // synchronisation.  The same reduction returns the block sum of
+  // extra_part in *extra when extra is given.
+  __device__ __forceinline__ float neg_jvp(const float* __restrict__ v, float vd, float* __restrict__ out, float* out_d,
+                           float extra_part = 0.f, float* extra = nullptr) {
+    const int nthk = T.n_thick, ncr = T.n_crowns, nsi = T.n_sites, ntn = T.n_thick_nodes, nxb = T.nxb;
+    const float* __restrict__ fdx = s.fdx;
+    const float* __restrict__ fdd = s.fdd;
+    const float* __restrict__ frdd = s.frdd;
+    const int16_t* __restrict__ hsite = s.hsite;
+    const float* __restrict__ tvec = s.tvec;
     const float kth = s.P[THICK_K], ktn = s.P[THIN_K];
-    float dot = 0.f;
+    float rad_part = 0.f, dot = 0.f;
+    auto head_w = [&](int h, float dxd) {
+      float w = fdx[h] * dxd;
+      if (dyn) w = w + fdd[h] * vd;
+      return w;
+    };
+    __syncthreads();  // v complete
     own_nodes([&](int i, int f, int j, bool thick) {
       float J;
+      const float vi = v[i];
       if (thick) {
         const float vm = j > 0 ? v[i - 1] : 0.f;
-        const float sc = (v[i] - vm) * kth;
+        const float sc = (vi - vm) * kth;
         float sn;
-        if (j + 1 < T.n_crowns) sn = (v[i + 1] - v[i]) * kth;
+        if (j + 1 < ncr) sn = (v[i + 1] - vi) * kth;
         else {
-          sn = s.tvec[T.n_thick + f] * v[i];
-          if (dyn) sn = sn + s.tvec[2 * T.n_thick + f] * vd;
+          sn = tvec[nthk + f] * vi;
+          if (dyn) {
+            sn = sn + tvec[2 * nthk + f] * vd;
+            rad_part += tvec[2 * nthk + f] * vi - tvec[3 * nthk + f] * vd;
+          }
         }
-        float xs = s.fxb[i * T.nxb];
-        for (int q = 1; q < T.nxb; ++q) xs += s.fxb[i * T.nxb + q];
+        float xs = 0.f;
+        for (int q = 0; q < nxb; ++q) {
+          const int h = i * nxb + q;
+          const int g = hsite[h];
+          float w = 0.f;
+          if (g >= 0) {
+            const float dxd = v[ntn + g] - vi;
+            w = head_w(h, dxd);
+            if (dyn) rad_part += -(fdd[h] * dxd) - frdd[h] * vd;
+          }
+          xs = q == 0 ? w : xs + w;
+        }
         J = (sn - sc) + xs;
       } else {
-        const int g = i - T.n_thick_nodes;
-        const float vn = (j + 1 < T.n_sites) ? v[i + 1] : 0.f;
-        const float sj = (vn - v[i]) * ktn;
-        const float sm = j > 0 ? (v[i] - v[i - 1]) * ktn : 0.f;
-        J = (sj - sm) + (s.win2[g] < 3 ? s.site[g] : ordered_site_sum(g));
-        s.site[g] = 0.f;
+        const int g = i - ntn;
+        const float vn = (j + 1 < nsi) ? v[i + 1] : 0.f;
+        const float sj = (vn - vi) * ktn;
+        const float sm = j > 0 ? (vi - v[i - 1]) * ktn : 0.f;
+        J = (sj - sm) + site_sum(g, [&](int h) { return head_w(h, vi - v[h / nxb]); });
       }
       const float o = -J;
       out[i] = o;
-      dot = fmaf(v[i], o, dot);
+      dot = fmaf(vi, o, dot);
     });
-    float r2[2] = {dot, rad_part};
-    reduce<2>(r2, false);
-    if (dyn) {
-      const float od = -(r2[1] + (-Kl) * vd);
-      *out_d = od;
-      return r2[0] + vd * od;
+    float r3[3] = {dot, rad_part, extra_part};
+    if (extra) {
+      reduce<3>(r3, false);
+      *extra = r3[2];
+    } else {
+      float r2[2] = {dot, rad_part};
+      reduce<2>(r2, false);
+      r3[0] = r2[0];
+      r3[1] = r2[1];
     }
-    return r2[0];
+    if (dyn) {
+      const float od = -(r3[1] + (-Kl) * vd);
+      *out_d = od;
+      return r3[0] + vd * od;
+    }
+    return r3[0];
   }
 
   // ------------------------------------------------------------------
   // Newton-CG (solver.py:329-427, 599-656)
   // ------------------------------------------------------------------
-  __device__ void solve(float zl, float& d, double& resid, int& iters, bool dyn_jdd) {
+  __device__ __forceinline__ void solve(float zl, float& d, double& resid, int& iters, bool dyn_jdd) {
+    if (regcg) {
+      solve_regs(zl, d, resid, iters, dyn_jdd);
+      return;
+    }
+    if (precise && A.n_cg > 0) {
+      solve_cg_gear(zl, d, resid, iters, dyn_jdd);
+      return;
+    }
     const float tol = fmaxf(s.P[SOLVER_TOL], fmaxf(s.P[THICK_K] * 1e-4f, 0.25f));
     float frad = 0.f, jdd = 0.f;
     float fmx = residual(zl, d, &frad, &jdd, 0, nullptr);
     // exact radial diagonal at the pre-solve point (solver.py:633-638)
     const float J_dd_inv = dyn_jdd ? -1.0f / jdd : 0.f;
+    const int n_cg = A.n_cg, n_newton = A.n_newton;
+    float* __restrict__ xv = s.x;
+    float* __restrict__ rv = s.r;
+    float* __restrict__ zv = s.zz;
+    float* __restrict__ pv = s.pv;
+    float* __restrict__ dxv = s.dx;
     int it = 0, bad = 0;
-    while (fmx > tol && it < A.n_newton) {
+    while (fmx > tol && it < n_newton) {
       float r_d = frad, z_d = 0.f, p_d = 0.f, dx_d = 0.f, Ap_d = 0.f;
-      precondition_own(s.r, s.zz);
+      precondition_own(rv, zv);
       float part[1] = {0.f};
       own_nodes([&](int i, int, int, bool) {
-        s.pv[i] = s.zz[i];
-        s.dx[i] = A.n_cg == 0 ? s.zz[i] : 0.f;
-        part[0] = fmaf(s.r[i], s.zz[i], part[0]);
+        pv[i] = zv[i];
+        dxv[i] = n_cg == 0 ? zv[i] : 0.f;
+        part[0] = fmaf(rv[i], zv[i], part[0]);
       });
       if (dyn) {
         z_d = J_dd_inv * r_d;
         p_d = z_d;
-        if (A.n_cg == 0) dx_d = z_d;
+        if (n_cg == 0) dx_d = z_d;
       }
       reduce<1>(part, false);
       float rz = part[0] + (dyn ? r_d * z_d : 0.f);
-      for (int k = 0; k < A.n_cg; ++k) {
-        const float pAp = neg_jvp(s.pv, p_d, s.zz, &Ap_d);
+      for (int k = 0; k < n_cg; ++k) {
+        const float pAp = neg_jvp(pv, p_d, zv, &Ap_d);
         const float alpha = rz / (pAp + 1e-30f);
         own_nodes([&](int i, int, int, bool) {
-          s.dx[i] = fmaf(alpha, s.pv[i], s.dx[i]);
-          s.r[i] = s.r[i] - alpha * s.zz[i];
+          dxv[i] = fmaf(alpha, pv[i], dxv[i]);
+          rv[i] = rv[i] - alpha * zv[i];
         });
         dx_d = fmaf(alpha, p_d, dx_d);
         r_d = r_d - alpha * Ap_d;
-        precondition_own(s.r, s.zz);
+        precondition_own(rv, zv);
         float rzp[1] = {0.f};
-        own_nodes([&](int i, int, int, bool) { rzp[0] = fmaf(s.r[i], s.zz[i], rzp[0]); });
+        own_nodes([&](int i, int, int, bool) { rzp[0] = fmaf(rv[i], zv[i], rzp[0]); });
         if (dyn) z_d = J_dd_inv * r_d;
         reduce<1>(rzp, false);
         const float rz_new = rzp[0] + (dyn ? r_d * z_d : 0.f);
         const float beta = rz_new / (rz + 1e-30f);
-        own_nodes([&](int i, int, int, bool) { s.pv[i] = fmaf(beta, s.pv[i], s.zz[i]); });
+        own_nodes([&](int i, int, int, bool) { pv[i] = fmaf(beta, pv[i], zv[i]); });
         p_d = fmaf(beta, p_d, z_d);
         rz = rz_new;
       }
       // x += dx with non-finite entries zeroed
       int bad_local = 0;
       own_nodes([&](int i, int, int, bool) {
-        float v = s.dx[i];
+        float v = dxv[i];
         if (!isfinite(v)) { v = 0.f; bad_local = 1; }
-        s.x[i] = s.x[i] + v;
+        xv[i] = xv[i] + v;
       });
       if (dyn) {
         float v = dx_d;
@@ -823,7 +911,536 @@ struct Sim {
     iters = it;
     if (!isfinite(fmx)) status |= MF_NONFINITE_BIT;
   }
+
+  // Precise-mode CG step on one filament of this warp, lane-contiguous
+  // layout (lane owns nodes [lane*E, lane*E+E)).  With update: the
+  // Chronopoulos-Gear recurrences p = u + beta p, s = w + beta s,
+  // dx += alpha p, r -= alpha s (first: p = u, s = w, dx = alpha u).  Then,
+  // unless last, u = M^{-1} r by the register Thomas solve; returns this
+  // lane's share of (r, u).  last: x += dx (non-finite entries zeroed).
+  template <int E>
+  __device__ __forceinline__ float cg_filament(int base, int n, const float* __restrict__ Af,
+                                               const float* __restrict__ Ab, const float* __restrict__ inv,
+                                               float alpha, float beta, bool update, bool first, bool last,
+                                               int& bad) {
+    float* __restrict__ r = s.r + base;
+    float* __restrict__ u = s.zz + base;
+    float* __restrict__ p = s.pv + base;
+    float* __restrict__ sv = s.sv + base;
+    float* __restrict__ dx = s.dx + base;
+    const float* __restrict__ w = s.wv + base;
+    float y[E], rr[E];
+    const int i0 = lane * E;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int i = i0 + e;
+      float ri = 0.f;
+      if (i < n) {
+        ri = r[i];
+        if (update) {
+          const float ui = u[i], wi = w[i];
+          const float pi = first ? ui : fmaf(beta, p[i], ui);
+          const float si = first ? wi : fmaf(beta, sv[i], wi);
+          const float di = first ? alpha * pi : fmaf(alpha, pi, dx[i]);
+          ri = ri - alpha * si;
+          if (last) {
+            float v = di;
+            if (!isfinite(v)) { v = 0.f; bad = 1; }
+            float* __restrict__ x = s.x + base;
+            x[i] = x[i] + v;
+          } else {
+            p[i] = pi;
+            sv[i] = si;
+            dx[i] = di;
+            r[i] = ri;
+          }
+        }
+      }
+      rr[e] = ri;
+      y[e] = ri;
+    }
+    if (last) return 0.f;
+    thomas_regs<E>(y, n, Af, Ab, inv);
+    float g = 0.f;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int i = i0 + e;
+      if (i < n) {
+        u[i] = y[e];
+        g = fmaf(rr[e], y[e], g);
+      }
+    }
+    return g;
+  }
+
+  __device__ __forceinline__ float cg_pass(float alpha, float beta, bool update, bool first, bool last, int& bad) {
+    const int nthk = T.n_thick, nf = T.n_thick + T.n_thin, ncr = T.n_crowns, nsi = T.n_sites;
+    const int ntn = T.n_thick_nodes;
+    float g = 0.f;
+    __syncwarp();
+    for (int f = warp; f < nf; f += NW) {
+      const bool thick = f < nthk;
+      const int n = thick ? ncr : nsi;
+      const int base = thick ? f * ncr : ntn + (f - nthk) * nsi;
+      const float* Af = s.coef + (thick ? cl.thick_fwd : cl.thin_fwd);
+      const float* Ab = s.coef + (thick ? cl.thick_back : cl.thin_back);
+      const float* inv = s.coef + (thick ? cl.thick_inv : cl.thin_inv);
+      if (n <= 64) g += cg_filament<2>(base, n, Af, Ab, inv, alpha, beta, update, first, last, bad);
+      else if (n <= 96) g += cg_filament<3>(base, n, Af, Ab, inv, alpha, beta, update, first, last, bad);
+      else g += cg_filament<4>(base, n, Af, Ab, inv, alpha, beta, update, first, last, bad);
+    }
+    __syncwarp();
+    return g;
+  }
+
+  // Precise mode: the same truncated preconditioned CG in the
+  // Chronopoulos-Gear arrangement (identical iterates in exact arithmetic):
+  // w = A u is formed right after u, and (r, u), (w, u) are reduced
+  // together, so an iteration costs the JVP barrier plus one reduction.
+  // alpha_k = gamma_k / (delta_k - beta_k gamma_k / alpha_{k-1}) uses
+  // (p_k, A p_k) = (u_k, A u_k) - beta_k^2 (p_{k-1}, A p_{k-1}).
+  __device__ __forceinline__ void solve_cg_gear(float zl, float& d, double& resid, int& iters, bool dyn_jdd) {
+    const float tol = fmaxf(s.P[SOLVER_TOL], fmaxf(s.P[THICK_K] * 1e-4f, 0.25f));
+    float frad = 0.f, jdd = 0.f;
+    MF_SUB(-1);
+    float fmx = residual(zl, d, &frad, &jdd, 0, nullptr);
+    MF_SUB(0);
+    const float J_dd_inv = dyn_jdd ? -1.0f / jdd : 0.f;
+    const int n_cg = A.n_cg, n_newton = A.n_newton;
+    int it = 0, bad = 0;
+    while (fmx > tol && it < n_newton) {
+      int bad_local = 0;
+      float r_d = frad, u_d = 0.f, w_d = 0.f, p_d = 0.f, s_d = 0.f, dx_d = 0.f;
+      // u = M^-1 r, w = A u, gamma = (r, u), delta = (u, w)
+      MF_SUB(-1);
+      float gpart = cg_pass(0.f, 0.f, false, false, false, bad_local);
+      MF_SUB(1);
+      if (dyn) u_d = J_dd_inv * r_d;
+      float gamma;
+      float delta = neg_jvp(s.zz, u_d, s.wv, &w_d, gpart, &gamma);
+      MF_SUB(2);
+      if (dyn) gamma += r_d * u_d;
+      float alpha = 0.f, gamma_old = 1.f;
+      for (int k = 0; k < n_cg; ++k) {
+        const bool first = k == 0, last = k + 1 == n_cg;
+        float beta = 0.f;
+        if (first) {
+          alpha = gamma / (delta + 1e-30f);
+        } else {
+          beta = gamma / (gamma_old + 1e-30f);
+          alpha = gamma / (delta - beta * gamma / alpha + 1e-30f);
+        }
+        MF_SUB(-1);
+        gpart = cg_pass(alpha, beta, true, first, last, bad_local);
+        MF_SUB(1);
+        p_d = first ? u_d : fmaf(beta, p_d, u_d);
+        s_d = first ? w_d : fmaf(beta, s_d, w_d);
+        dx_d = first ? alpha * p_d : fmaf(alpha, p_d, dx_d);
+        r_d = r_d - alpha * s_d;
+        if (last) break;
+        if (dyn) u_d = J_dd_inv * r_d;
+        gamma_old = gamma;
+        MF_SUB(-1);
+        delta = neg_jvp(s.zz, u_d, s.wv, &w_d, gpart, &gamma);
+        MF_SUB(2);
+        if (dyn) gamma += r_d * u_d;
+        if (tid == 0) MF_COUNT(3);
+      }
+      if (dyn) {
+        float v = dx_d;
+        if (!isfinite(v)) v = 0.f;
+        d = fmaxf(d + v, 1.0f);
+      }
+      MF_SUB(-1);
+      fmx = residual(zl, d, &frad, nullptr, bad_local, &bad);
+      MF_SUB(0);
+      if (tid == 0) MF_COUNT(4);
+      if (bad) status |= MF_NONFINITE_BIT;
+      ++it;
+    }
+    resid = fmx;
+    iters = it;
+    if (!isfinite(fmx)) status |= MF_NONFINITE_BIT;
+  }
   static constexpr int MF_NONFINITE_BIT = 1;
+  // ------------------------------------------------------------------
+  // Register-resident precise Newton-CG (lattices with at most RF filaments
+  // per warp and filaments of at most 32*RE nodes, crowns of <= 3 heads).
+  // Lane l of a warp owns nodes [l*RE, l*RE+RE) of each of its filaments;
+  // the CG vectors r, p, s, u, w, dx of those nodes stay in registers for
+  // the whole solve, only u (read by the node's neighbours and partners)
+  // and x (read by the head forces) are written to shared memory.  The
+  // crossbridge coupling of every node is a fixed list of <= 3 partner
+  // nodes built once per step (nb_node / nb_head), so the JVP has no
+  // dependent index chains.  Same Chronopoulos-Gear recurrences as
+  // solve_cg_gear.
+  // ------------------------------------------------------------------
+  static constexpr int RE = 3, RF = 2;
+  using RVec = float[RF][RE];
+
+  __device__ __forceinline__ bool slot(int k, int& base, int& n, int& f, bool& thick) const {
+    f = warp + k * NW;
+    thick = f < T.n_thick;
+    n = thick ? T.n_crowns : T.n_sites;
+    base = thick ? f * T.n_crowns : T.n_thick_nodes + (f - T.n_thick) * T.n_sites;
+    return f < T.n_thick + T.n_thin;
+  }
+
+  // Partner lists of every node for this step: crown i -> the sites of its
+  // heads, site g -> the crowns of the heads bound to it (nb_node = -2 on
+  // sites holding 3+ heads, summed in head order by site_sum instead).
+  __device__ __forceinline__ void build_partner_lists() {
+    const int N = T.n_dof, ntn = T.n_thick_nodes, nxb = T.nxb;
+    int16_t* __restrict__ nbn = s.nb_node;
+    int16_t* __restrict__ nbh = s.nb_head;
+    for (int i = tid; i < N; i += NT) {
+      int16_t pn[3] = {-1, -1, -1}, ph[3] = {0, 0, 0};
+      if (i < ntn) {
+        for (int q = 0; q < nxb; ++q) {
+          const int h = i * nxb + q;
+          const int g = s.hsite[h];
+          ph[q] = (int16_t)h;
+          if (g >= 0) pn[q] = (int16_t)(ntn + g);
+        }
+      } else {
+        const int g = i - ntn;
+        const int c = s.win2[g];
+        if (c >= 3) {
+          pn[0] = -2;
+        } else {
+          for (int q = 0; q < c; ++q) {
+            const int h = s.site_h[2 * g + q];
+            ph[q] = (int16_t)h;
+            pn[q] = (int16_t)(h / nxb);
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        nbn[3 * i + q] = pn[q];
+        nbh[3 * i + q] = ph[q];
+      }
+    }
+    __syncthreads();
+  }
+
+  // F(x) of the lane's nodes into r (float64 accumulation, as residual());
+  // returns max|F| over the augmented vector.
+  __device__ __forceinline__ float residual_regs(float zl, float d, float* frad, float* jdd, int bad_in, int* bad_out, RVec& r) {
+    const int nb = *s.nbound;
+    const int nthk = T.n_thick;
+    const float* __restrict__ x = s.x;
+    float* __restrict__ fxb = s.fxb;
+    float* __restrict__ tvec = s.tvec;
+    const int16_t* __restrict__ nbn = s.nb_node;
+    const int16_t* __restrict__ nbh = s.nb_head;
+    float rad_part = 0.f, jdd_part = 0.f;
+    const int any_bad = __syncthreads_or(bad_in);
+    if (bad_out) *bad_out = any_bad;
+    for (int k = tid; k < nb; k += NT) {
+      const int i = s.blist[k];
+      float f, fx, fd, frd, fr;
+      xb_force(i, d, f, fx, fd, frd, fr);
+      fxb[i] = f;
+      s.fdx[i] = fx;
+      if (dyn) {
+        s.fdd[i] = fd;
+        s.frdd[i] = frd;
+        rad_part += fr;
+        jdd_part += frd;
+      }
+    }
+    if (tid < nthk) {
+      float ax, a_x, a_d, r_d, rad;
+      titin(tid, zl, d, ax, a_x, a_d, r_d, rad);
+      tvec[tid] = ax;
+      tvec[nthk + tid] = a_x;
+      tvec[2 * nthk + tid] = a_d;
+      tvec[3 * nthk + tid] = r_d;
+      if (dyn) {
+        rad_part += rad;
+        jdd_part += r_d;
+      }
+    }
+    __syncthreads();
+    const double kth = (double)s.P[THICK_K], ktn = (double)s.P[THIN_K];
+    const float* __restrict__ thc = T.thick_c;
+    const float* __restrict__ tnc = T.thin_c;
+    const double zoff = (double)zl - zref;
+    const int ntn = T.n_thick_nodes, nxb = T.nxb;
+    float fmax = 0.f;
+#pragma unroll
+    for (int k = 0; k < RF; ++k) {
+      int base, n, f;
+      bool thick;
+      const bool ok = slot(k, base, n, f, thick);
+#pragma unroll
+      for (int e = 0; e < RE; ++e) {
+        const int j = lane * RE + e;
+        float Fv = 0.f;
+        if (ok && j < n) {
+          const int i = base + j;
+          const double xi = (double)x[i];
+          const double xm = j > 0 ? (double)x[i - 1] : 0.0;
+          const double xn = j + 1 < n ? (double)x[i + 1] : 0.0;
+          double F;
+          if (thick) {
+            float xsum = fxb[i * nxb];
+            for (int q = 1; q < nxb; ++q) xsum += fxb[i * nxb + q];
+            const double e_c = (xi - xm) + (double)thc[i];
+            const double spn = j + 1 < n ? ((xn - xi) + (double)thc[i + 1]) * kth : (double)tvec[f];
+            F = (spn - e_c * kth) + (double)xsum;
+          } else {
+            const int g = i - ntn;
+            float acc = 0.f;
+            const int p0 = nbn[3 * i];
+            if (p0 == -2) {
+              acc = site_sum(g, [&](int h) { return fxb[h]; });
+            } else {
+              if (p0 >= 0) acc = acc + (-fxb[nbh[3 * i]]);
+              if (nbn[3 * i + 1] >= 0) acc = acc + (-fxb[nbh[3 * i + 1]]);
+            }
+            double e_j = (xn - xi) + (double)tnc[g];
+            if (j + 1 == n) e_j += zoff;
+            const double e_m = j > 0 ? (xi - xm) + (double)tnc[g - 1] : 0.0;
+            F = (e_j - e_m) * ktn + (double)acc;
+          }
+          Fv = (float)F;
+          fmax = fmaxf(fmax, (float)fabs(F));
+        }
+        r[k][e] = Fv;
+      }
+    }
+    float v[3] = {fmax, rad_part, jdd_part};
+    reduce<3>(v, true);
+    float m = v[0];
+    if (dyn) {
+      const float Fr = -Kl * (d - d_ref) + (-v[1]);
+      *frad = Fr;
+      m = fmaxf(m, fabsf(Fr));
+      if (jdd) *jdd = -Kl - v[2];
+    }
+    return m;
+  }
+
+  // u = M^-1 r on the lane's nodes (register Thomas solves), u also stored
+  // to shared memory; returns the lane's share of (r, u).
+  __device__ __forceinline__ float precond_regs(const RVec& r, RVec& u) {
+    float g = 0.f;
+#pragma unroll
+    for (int k = 0; k < RF; ++k) {
+      int base, n, f;
+      bool thick;
+      if (!slot(k, base, n, f, thick)) break;
+      const float* Af = s.coef + (thick ? cl.thick_fwd : cl.thin_fwd);
+      const float* Ab = s.coef + (thick ? cl.thick_back : cl.thin_back);
+      const float* inv = s.coef + (thick ? cl.thick_inv : cl.thin_inv);
+      float y[RE];
+#pragma unroll
+      for (int e = 0; e < RE; ++e) y[e] = r[k][e];
+      thomas_regs<RE>(y, n, Af, Ab, inv);
+      float* __restrict__ us = s.zz + base;
+#pragma unroll
+      for (int e = 0; e < RE; ++e) {
+        const int j = lane * RE + e;
+        u[k][e] = j < n ? y[e] : 0.f;
+        if (j < n) {
+          us[j] = y[e];
+          g = fmaf(r[k][e], y[e], g);
+        }
+      }
+    }
+    return g;
+  }
+
+  // w = -J [u, ud] on the lane's nodes; returns (u, w) (augmented) and the
+  // block sum of extra_part in *extra, *w_d the radial component.
+  __device__ __forceinline__ float jvp_regs(const RVec& u, float ud, RVec& w, float* w_d, float extra_part, float* extra) {
+    const int nthk = T.n_thick, nxb = T.nxb;
+    const float* __restrict__ us = s.zz;
+    const float* __restrict__ fdx = s.fdx;
+    const float* __restrict__ fdd = s.fdd;
+    const float* __restrict__ frdd = s.frdd;
+    const float* __restrict__ tvec = s.tvec;
+    const int16_t* __restrict__ nbn = s.nb_node;
+    const int16_t* __restrict__ nbh = s.nb_head;
+    const float kth = s.P[THICK_K], ktn = s.P[THIN_K];
+    float rad_part = 0.f, dot = 0.f;
+    __syncthreads();  // u of every node stored
+#pragma unroll
+    for (int k = 0; k < RF; ++k) {
+      int base, n, f;
+      bool thick;
+      const bool ok = slot(k, base, n, f, thick);
+      const float left = __shfl_up_sync(0xffffffffu, u[k][RE - 1], 1);
+      const float right = __shfl_down_sync(0xffffffffu, u[k][0], 1);
+#pragma unroll
+      for (int e = 0; e < RE; ++e) {
+        const int j = lane * RE + e;
+        float o = 0.f;
+        if (ok && j < n) {
+          const int i = base + j;
+          const float vi = u[k][e];
+          const float vm = j == 0 ? 0.f : (e > 0 ? u[k][e - 1] : left);
+          const float vn = j + 1 >= n ? 0.f : (e + 1 < RE ? u[k][e + 1] : right);
+          float J;
+          if (thick) {
+            const float sc = (vi - vm) * kth;
+            float sn;
+            if (j + 1 < n) sn = (vn - vi) * kth;
+            else {
+              sn = tvec[nthk + f] * vi;
+              if (dyn) {
+                sn = sn + tvec[2 * nthk + f] * ud;
+                rad_part += tvec[2 * nthk + f] * vi - tvec[3 * nthk + f] * ud;
+              }
+            }
+            float xs = 0.f;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+              const int pn = nbn[3 * i + q];
+              float wq = 0.f;
+              if (pn >= 0) {
+                const int h = i * nxb + q;
+                const float dxd = us[pn] - vi;
+                wq = fdx[h] * dxd;
+                if (dyn) {
+                  wq = wq + fdd[h] * ud;
+                  rad_part += -(fdd[h] * dxd) - frdd[h] * ud;
+                }
+              }
+              xs = q == 0 ? wq : xs + wq;
+            }
+            J = (sn - sc) + xs;
+          } else {
+            const float sj = (vn - vi) * ktn;
+            const float sm = j > 0 ? (vi - vm) * ktn : 0.f;
+            auto head_w = [&](int h, float vc) {
+              float wh = fdx[h] * (vi - vc);
+              if (dyn) wh = wh + fdd[h] * ud;
+              return wh;
+            };
+            float acc = 0.f;
+            const int p0 = nbn[3 * i], p1 = nbn[3 * i + 1];
+            if (p0 == -2) {
+              acc = site_sum(i - T.n_thick_nodes, [&](int h) { return head_w(h, us[h / nxb]); });
+            } else {
+              if (p0 >= 0) acc = acc + (-head_w(nbh[3 * i], us[p0]));
+              if (p1 >= 0) acc = acc + (-head_w(nbh[3 * i + 1], us[p1]));
+            }
+            J = (sj - sm) + acc;
+          }
+          o = -J;
+          dot = fmaf(vi, o, dot);
+        }
+        w[k][e] = o;
+      }
+    }
+    float r3[3] = {dot, rad_part, extra_part};
+    reduce<3>(r3, false);
+    *extra = r3[2];
+    if (dyn) {
+      const float od = -(r3[1] + (-Kl) * ud);
+      *w_d = od;
+      return r3[0] + ud * od;
+    }
+    return r3[0];
+  }
+
+  __device__ __forceinline__ void solve_regs(float zl, float& d, double& resid, int& iters, bool dyn_jdd) {
+    const float tol = fmaxf(s.P[SOLVER_TOL], fmaxf(s.P[THICK_K] * 1e-4f, 0.25f));
+    MF_SUB(-1);
+    build_partner_lists();
+    MF_SUB(5);
+    RVec r, p, sv, u, w, dx;
+#pragma unroll
+    for (int k = 0; k < RF; ++k)
+#pragma unroll
+      for (int e = 0; e < RE; ++e) p[k][e] = sv[k][e] = u[k][e] = w[k][e] = dx[k][e] = 0.f;
+    float frad = 0.f, jdd = 0.f;
+    float fmx = residual_regs(zl, d, &frad, &jdd, 0, nullptr, r);
+    MF_SUB(0);
+    const float J_dd_inv = dyn_jdd ? -1.0f / jdd : 0.f;
+    const int n_cg = A.n_cg, n_newton = A.n_newton;
+    int it = 0, bad = 0;
+    while (fmx > tol && it < n_newton) {
+      float r_d = frad, u_d = 0.f, w_d = 0.f, p_d = 0.f, s_d = 0.f, dx_d = 0.f;
+      MF_SUB(-1);
+      float gpart = precond_regs(r, u);
+      MF_SUB(1);
+      if (dyn) u_d = J_dd_inv * r_d;
+      float gamma;
+      float delta = jvp_regs(u, u_d, w, &w_d, gpart, &gamma);
+      MF_SUB(2);
+      if (dyn) gamma += r_d * u_d;
+      float alpha = 0.f, gamma_old = 1.f;
+      for (int kk = 0; kk < n_cg; ++kk) {
+        const bool first = kk == 0;
+        float beta = 0.f;
+        if (first) {
+          alpha = gamma / (delta + 1e-30f);
+        } else {
+          beta = gamma / (gamma_old + 1e-30f);
+          alpha = gamma / (delta - beta * gamma / alpha + 1e-30f);
+        }
+#pragma unroll
+        for (int k = 0; k < RF; ++k)
+#pragma unroll
+          for (int e = 0; e < RE; ++e) {
+            p[k][e] = first ? u[k][e] : fmaf(beta, p[k][e], u[k][e]);
+            sv[k][e] = first ? w[k][e] : fmaf(beta, sv[k][e], w[k][e]);
+            dx[k][e] = first ? alpha * p[k][e] : fmaf(alpha, p[k][e], dx[k][e]);
+            r[k][e] = r[k][e] - alpha * sv[k][e];
+          }
+        p_d = first ? u_d : fmaf(beta, p_d, u_d);
+        s_d = first ? w_d : fmaf(beta, s_d, w_d);
+        dx_d = first ? alpha * p_d : fmaf(alpha, p_d, dx_d);
+        r_d = r_d - alpha * s_d;
+        if (kk + 1 == n_cg) break;
+        MF_SUB(-1);
+        gpart = precond_regs(r, u);
+        MF_SUB(1);
+        if (dyn) u_d = J_dd_inv * r_d;
+        gamma_old = gamma;
+        delta = jvp_regs(u, u_d, w, &w_d, gpart, &gamma);
+        MF_SUB(2);
+        if (tid == 0) MF_COUNT(3);
+        if (dyn) gamma += r_d * u_d;
+      }
+      // x += dx with non-finite entries zeroed
+      int bad_local = 0;
+#pragma unroll
+      for (int k = 0; k < RF; ++k) {
+        int base, n, f;
+        bool thick;
+        if (!slot(k, base, n, f, thick)) break;
+        float* __restrict__ xs = s.x + base;
+#pragma unroll
+        for (int e = 0; e < RE; ++e) {
+          const int j = lane * RE + e;
+          if (j < n) {
+            float v = dx[k][e];
+            if (!isfinite(v)) { v = 0.f; bad_local = 1; }
+            xs[j] = xs[j] + v;
+          }
+        }
+      }
+      if (dyn) {
+        float v = dx_d;
+        if (!isfinite(v)) v = 0.f;
+        d = fmaxf(d + v, 1.0f);
+      }
+      MF_SUB(-1);
+      fmx = residual_regs(zl, d, &frad, nullptr, bad_local, &bad, r);
+      MF_SUB(0);
+      if (tid == 0) MF_COUNT(4);
+      if (bad) status |= MF_NONFINITE_BIT;
+      ++it;
+    }
+    resid = fmx;
+    iters = it;
+    if (!isfinite(fmx)) status |= MF_NONFINITE_BIT;
+  }
 
   // ------------------------------------------------------------------
   // probability tables (built when (pCa, d) differ from the cached key)
@@ -867,39 +1484,100 @@ struct Sim {
   // ------------------------------------------------------------------
   // kinetics
   // ------------------------------------------------------------------
+  // Nearest binding site of every head (kernels/geometry.py:60-262): the
+  // first candidate of the head's face with the smallest |site - (crown + 13)|
+  // among the valid ones (k < face_n, position > 0).  The candidate
+  // positions of every face are staged once per step; on a face whose valid
+  // candidates form one run of strictly monotone positions (the normal case:
+  // sites along a filament) the argmin is found by bisection, with ties
+  // resolved towards the lower index exactly as the linear scan does;
+  // other faces use the linear scan over the staged positions.
   __device__ void nearest(float d) {
-    const int X = T.total_xbs;
-    for (int i = tid; i < X; i += NT) {
-      const int face = T.xb_face[i];
-      const int thin = face / 3;
-      const int node = crown_node(i);
-      const int nv = T.face_n[face];
-      const int16_t* cand = T.face_sites + face * T.width;
-      int bestk = 0;
-      if (!precise) {
-        const float head = s.x[node] + 13.0f;
-        float best = INFINITY;
-        for (int k = 0; k < T.width; ++k) {
-          const float pos = s.x[T.n_thick_nodes + thin * T.n_sites + cand[k]];
-          if (k < nv && pos > 0.0f) {
-            const float dist = fabsf(pos - head);
-            if (dist < best) { best = dist; bestk = k; }
+    const int X = T.total_xbs, W = T.width, nsi = T.n_sites, ntn = T.n_thick_nodes;
+    const int nfaces = T.n_thin * 3;
+    double* __restrict__ fp = s.face_pos;
+    const int16_t* __restrict__ cands = T.face_sites;
+    const uint8_t* __restrict__ fn = T.face_n;
+    for (int q = tid; q < nfaces * W; q += NT) {
+      const int face = q / W, k = q - face * W;
+      double pos = NAN;
+      if (k < fn[face]) {
+        const int g = (face / 3) * nsi + cands[q];
+        pos = precise ? site_pos_d(g) : (double)s.x[ntn + g];
+      }
+      fp[q] = pos > 0.0 ? pos : NAN;
+    }
+    __syncthreads();
+    for (int face = warp; face < nfaces; face += NW) {
+      const double pk = (W <= 32 && lane < W) ? fp[face * W + lane] : NAN;
+      const bool v = pk == pk;
+      const unsigned vm = __ballot_sync(0xffffffffu, v);
+      const double pn = __shfl_down_sync(0xffffffffu, pk, 1);
+      const bool pair = v && lane < 31 && ((vm >> (lane + 1)) & 1u);
+      const unsigned pm = __ballot_sync(0xffffffffu, pair);
+      const unsigned im = __ballot_sync(0xffffffffu, pair && pk < pn);
+      const unsigned dm = __ballot_sync(0xffffffffu, pair && pk > pn);
+      if (lane == 0) {
+        int mono = 0, kl = 0, kh = 0;
+        if (W <= 32) {
+          if (vm == 0u) {
+            mono = 3;  // no valid candidate: the scan keeps k = 0
+          } else {
+            kl = __ffs(vm) - 1;
+            kh = 31 - __clz(vm);
+            const int len = kh - kl + 1;
+            const unsigned run = len == 32 ? 0xffffffffu : ((1u << len) - 1u);
+            if ((vm >> kl) == run) mono = im == pm ? 1 : (dm == pm ? 2 : 0);
           }
         }
-      } else {
-        const double head = crown_pos_d(node) + 13.0;
+        s.face_mono[face] = (int8_t)mono;
+        s.face_kl[face] = (int8_t)kl;
+        s.face_kh[face] = (int8_t)kh;
+      }
+    }
+    __syncthreads();
+    for (int i = tid; i < X; i += NT) {
+      const int face = T.xb_face[i];
+      const int node = crown_node(i);
+      const double* __restrict__ fpf = fp + face * W;
+      const double head = precise ? crown_pos_d(node) + 13.0 : (double)(s.x[node] + 13.0f);
+      auto dist = [&](int k) -> double {
+        const double p = fpf[k];
+        return precise ? fabs(p - head) : (double)fabsf((float)p - (float)head);
+      };
+      const int mono = s.face_mono[face];
+      int bestk = 0;
+      if (mono == 1 || mono == 2) {
+        if (head == head) {
+          const int kl = s.face_kl[face], kh = s.face_kh[face];
+          int lo = kl, hi = kh + 1;
+          while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            const double p = fpf[mid];
+            const bool right = mono == 1 ? p >= head : p <= head;
+            if (right) hi = mid;
+            else lo = mid + 1;
+          }
+          if (lo > kl && (lo > kh || dist(lo - 1) <= dist(lo))) {
+            bestk = lo - 1;
+            while (bestk > kl && dist(bestk - 1) == dist(bestk)) --bestk;
+          } else {
+            bestk = lo;
+          }
+        }
+      } else if (mono == 0) {
         double best = INFINITY;
-        for (int k = 0; k < T.width; ++k) {
-          const double pos = site_pos_d(thin * T.n_sites + cand[k]);
-          if (k < nv && pos > 0.0) {
-            const double dist = fabs(pos - head);
-            if (dist < best) { best = dist; bestk = k; }
+        for (int k = 0; k < W; ++k) {
+          const double p = fpf[k];
+          if (p == p) {
+            const double dd = dist(k);
+            if (dd < best) { best = dd; bestk = k; }
           }
         }
       }
-      const int site = cand[bestk];
+      const int site = cands[face * W + bestk];
       s.xb_near[i] = (int16_t)site;
-      s.xb_ax[i] = xb_offset(thin * T.n_sites + site, node);
+      s.xb_ax[i] = xb_offset((face / 3) * nsi + site, node);
     }
     (void)d;
   }

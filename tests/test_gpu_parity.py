@@ -164,6 +164,33 @@ def test_mixed_precision_force_error_vs_fp64_oracle(engine):
     assert err_mixed <= 1e-5, err_mixed
 
 
+@pytest.mark.parametrize('nr,nc,pCa', [(2, 2, 4.5), (3, 2, 5.5)])
+def test_mixed_precision_dynamic_ls_vs_fp64_oracle(engine, nr, nc, pCa):
+    """'mixed' precision with the lattice spacing solved as an unknown: force and
+    spacing within 1e-5 relative of the FP64 oracle (same uniforms)."""
+    s, d = get_skeletal_params()
+    topo = SarcTopology.create(nr, nc, s, d)
+    T = 25
+    key = prng.split(prng.PRNGKey(4), 1)[0]
+    K = 5.0 * topo.n_thick
+    zt, pt, lt = 900.0 + 0.5 * np.arange(T), np.full(T, pCa), np.full(T, 14.0)
+    m32, info32 = OS.run_condition(topo, d.param_row(), zt, pt, lt, key, K_lat=K, nu=0.5)
+    m64, info64 = OS.run_condition(topo, d.param_row(), zt, pt, lt, key, dt=np.float64, K_lat=K, nu=0.5,
+                                   uniforms=info32['uniforms'], record_states=True)
+    ut = np.stack([u[0] for u in info32['uniforms']])[None]
+    ux = np.stack([u[1] for u in info32['uniforms']])[None]
+    res = run_engine(engine, topo, d.param_row()[None], zt[None], pt[None], lt[None], key[None], K_lat=[K],
+                     nu=[0.5], flags=MF_FLAG_PRECISE | MF_FLAG_DYNAMIC_LS, u_thin=ut, u_xb=ux, traces=True)
+    div = state_divergence(res, 0, info64, topo, T)
+    mdiv = first_divergence(res['metrics'], m64[None], KEYS)
+    win = min(v for v in (div, mdiv, T) if v is not None)
+    assert win >= 3
+    for row in (0, 4):  # axial_force, lattice_spacing
+        ref, got = m64[row, :win], res['metrics'][0, row, :win]
+        err = np.max(np.abs(got - ref) / np.abs(ref))
+        assert err <= 1e-5, (METRIC_KEYS[row], err)
+
+
 def test_bad_arguments_raise(engine):
     import torch
     from multifil_jax_b200.engine import EngineError
