@@ -146,6 +146,46 @@ __host__ __device__ inline CoefLayout coef_layout(const TopoDev& t) {
   return c;
 }
 
+// Transition tables of one condition at (pCa, d), built by the whole CTA:
+// the 27 tropomyosin row sums (shared) and, per crossbridge bin and
+// permissiveness, the cumulative rows of expm(Q dt) ("sampling", global) or
+// the three absorbing-chain entries the metrics read ("absorbing", global).
+// Out of line: it runs only when pCa or the spacing changes, and its
+// unrolled Pade arithmetic would otherwise sit in the step loop's code.
+__device__ __noinline__ void build_tables_block(const float* P, const float* centers, int nb, float pCa, float d,
+                                                float dtm, int sq64, float* cum_tm, float* cum_xb, float* pabs,
+                                                bool sampling, bool absorbing, int tid, int nt) {
+  if (sampling) {
+    for (int m = tid; m < 27; m += nt) {
+      float Q[16];
+      tm_generator(P, pCa, m, Q);
+      for (int i = 0; i < 16; ++i) Q[i] = Q[i] * dtm;
+      expm_pade6<4>(Q, sq64);
+      for (int r = 0; r < 4; ++r) cum4(Q + 4 * r, cum_tm + m * 16 + 4 * r);
+    }
+  }
+  const int nwork = (sampling ? 2 * nb : 0) + (absorbing ? 2 * nb : 0);
+  for (int w = tid; w < nwork; w += nt) {
+    const bool is_abs = !sampling || w >= 2 * nb;
+    const int key = is_abs && sampling ? w - 2 * nb : w;
+    const int bin = key % nb;
+    const float perm = key >= nb ? 1.0f : 0.0f;
+    float Q[36];
+    xb_generator(P, pCa, centers[bin], d, perm, Q);
+    if (is_abs)
+      for (int j = 0; j < 6; ++j) { Q[24 + j] = 0.f; Q[j] = 0.f; }
+    for (int i = 0; i < 36; ++i) Q[i] = Q[i] * dtm;
+    expm_pade6<6>(Q, sq64);
+    if (is_abs) {
+      pabs[key * 3 + 0] = Q[3 * 6 + 4];  // P_abs[3,4]
+      pabs[key * 3 + 1] = Q[2 * 6 + 0];  // P_abs[2,0]
+      pabs[key * 3 + 2] = Q[3 * 6 + 0];  // P_abs[3,0]
+    } else {
+      for (int r = 0; r < 6; ++r) cum6(Q + 6 * r, cum_xb + key * 36 + 6 * r);
+    }
+  }
+}
+
 template <int NT>
 struct Sim {
   static constexpr int NW = NT / 32;
@@ -1094,32 +1134,44 @@ struct Sim {
     int16_t* __restrict__ nbn = s.nb_node;
     int16_t* __restrict__ nbh = s.nb_head;
     for (int i = tid; i < N; i += NT) {
-      int16_t pn[3] = {-1, -1, -1}, ph[3] = {0, 0, 0};
+      // three scalar slots (a runtime-indexed array would live in local memory)
+      int p0 = -1, p1 = -1, p2 = -1, h0 = 0, h1 = 0, h2 = 0;
       if (i < ntn) {
-        for (int q = 0; q < nxb; ++q) {
-          const int h = i * nxb + q;
-          const int g = s.hsite[h];
-          ph[q] = (int16_t)h;
-          if (g >= 0) pn[q] = (int16_t)(ntn + g);
+        h0 = i * nxb;
+        h1 = h0 + 1;
+        h2 = h0 + 2;
+        const int g0 = s.hsite[h0];
+        if (g0 >= 0) p0 = ntn + g0;
+        if (nxb > 1) {
+          const int g1 = s.hsite[h1];
+          if (g1 >= 0) p1 = ntn + g1;
+        }
+        if (nxb > 2) {
+          const int g2 = s.hsite[h2];
+          if (g2 >= 0) p2 = ntn + g2;
         }
       } else {
         const int g = i - ntn;
         const int c = s.win2[g];
         if (c >= 3) {
-          pn[0] = -2;
+          p0 = -2;
         } else {
-          for (int q = 0; q < c; ++q) {
-            const int h = s.site_h[2 * g + q];
-            ph[q] = (int16_t)h;
-            pn[q] = (int16_t)(h / nxb);
+          if (c >= 1) {
+            h0 = s.site_h[2 * g];
+            p0 = h0 / nxb;
+          }
+          if (c >= 2) {
+            h1 = s.site_h[2 * g + 1];
+            p1 = h1 / nxb;
           }
         }
       }
-#pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        nbn[3 * i + q] = pn[q];
-        nbh[3 * i + q] = ph[q];
-      }
+      nbn[3 * i] = (int16_t)p0;
+      nbn[3 * i + 1] = (int16_t)p1;
+      nbn[3 * i + 2] = (int16_t)p2;
+      nbh[3 * i] = (int16_t)h0;
+      nbh[3 * i + 1] = (int16_t)h1;
+      nbh[3 * i + 2] = (int16_t)h2;
     }
     __syncthreads();
   }
@@ -1446,39 +1498,9 @@ struct Sim {
   // probability tables (built when (pCa, d) differ from the cached key)
   // ------------------------------------------------------------------
   __device__ void build_tables(float pCa, float d, bool sampling, bool absorbing) {
-    float* cum_xb = reinterpret_cast<float*>(ws + L.cum_xb);
-    float* pabs = reinterpret_cast<float*>(ws + L.pabs);
-    const int nb = T.n_bins;
-    const int sq64 = A.sq64_from;
-    if (sampling) {
-      for (int m = tid; m < 27; m += NT) {
-        float Q[16];
-        tm_generator(s.P, pCa, m, Q);
-        for (int i = 0; i < 16; ++i) Q[i] = Q[i] * dtm;
-        expm_pade6<4>(Q, sq64);
-        for (int r = 0; r < 4; ++r) cum4(Q + 4 * r, s.cum_tm + m * 16 + 4 * r);
-      }
-    }
-    const int nwork = (sampling ? 2 * nb : 0) + (absorbing ? 2 * nb : 0);
-    for (int w = tid; w < nwork; w += NT) {
-      const bool is_abs = !sampling || w >= 2 * nb;
-      const int key = is_abs && sampling ? w - 2 * nb : w;
-      const int bin = key % nb;
-      const float perm = key >= nb ? 1.0f : 0.0f;
-      float Q[36];
-      xb_generator(s.P, pCa, T.centers[bin], d, perm, Q);
-      if (is_abs)
-        for (int j = 0; j < 6; ++j) { Q[24 + j] = 0.f; Q[j] = 0.f; }
-      for (int i = 0; i < 36; ++i) Q[i] = Q[i] * dtm;
-      expm_pade6<6>(Q, sq64);
-      if (is_abs) {
-        pabs[key * 3 + 0] = Q[3 * 6 + 4];  // P_abs[3,4]
-        pabs[key * 3 + 1] = Q[2 * 6 + 0];  // P_abs[2,0]
-        pabs[key * 3 + 2] = Q[3 * 6 + 0];  // P_abs[3,0]
-      } else {
-        for (int r = 0; r < 6; ++r) cum6(Q + 6 * r, cum_xb + key * 36 + 6 * r);
-      }
-    }
+    build_tables_block(s.P, T.centers, T.n_bins, pCa, d, dtm, A.sq64_from, s.cum_tm,
+                       reinterpret_cast<float*>(ws + L.cum_xb), reinterpret_cast<float*>(ws + L.pabs), sampling,
+                       absorbing, tid, NT);
   }
 
   // ------------------------------------------------------------------
