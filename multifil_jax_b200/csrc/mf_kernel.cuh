@@ -183,45 +183,32 @@ __device__ void metrics(Sim<NT>& m, int t, float zl, float pCa, float new_ls, fl
                  c_xb[0], c_xb[1], c_xb[2], c_xb[3], c_xb[4], c_xb[5], c_xb[6],
                  c_tm[0], c_tm[1], c_tm[2], c_tm[3], ov, ov2, ov3, atp, newly,
                  tsum, tsq, nsum, nsq, dxs, atp_p, tear, 0.f, 0.f};
-  m.template bred<29>(r, 4);
-  if (tid == 0) {
-    tmin = -r[0]; tmax = r[1]; nmin = -r[2]; nmax = r[3];
-    const float nx = (float)X, nt = (float)S;
-    const float* P = m.s.P;
-    auto put = [&](int k, float v) { Mo[(size_t)k * m.Tstride + t] = v; };
-    put(M_AXIAL_FORCE, force);
-    put(M_SOLVER_RESIDUAL, (float)resid);
-    put(M_Z_LINE, zl);
-    put(M_PCA, pCa);
-    put(M_LATTICE_SPACING, new_ls);
-    const float nb = r[10];
-    put(M_N_BOUND, nb);
-    for (int k = 0; k < 6; ++k) put(M_N_XB_DRX + k, r[4 + k]);
-    put(M_FRAC_XB_BOUND, nb / nx);
-    for (int k = 0; k < 6; ++k) put(M_FRAC_XB_DRX + k, r[4 + k] / nx);
-    for (int k = 0; k < 4; ++k) put(M_N_TM_0 + k, r[11 + k]);
-    for (int k = 0; k < 4; ++k) put(M_FRAC_TM_0 + k, r[11 + k] / nt);
-    put(M_ACTIN_PERM, r[14] / nt);
-    const float nov = r[15], n2 = r[16], n3 = r[17];
-    put(M_FRAC_TM_2_OV, n2 / nov);
-    put(M_FRAC_TM_3_OV, n3 / nov);
-    put(M_FRAC_TM_AVAIL_OV, (n2 + n3) / nov);
-    put(M_N_OVERLAP, nov);
-    put(M_ATP_CONSUMED, r[18]);
-    put(M_NEWLY_BOUND, r[19]);
-    const float tmean_c = r[20] / (float)NTN, nmean_c = r[22] / (float)S;
-    put(M_THICK_D_MEAN, t_shift + tmean_c);
-    put(M_THICK_D_MAX, tmax);
-    put(M_THICK_D_MIN, tmin);
-    put(M_THICK_D_STD, sqrtf(fmaxf(r[21] / (float)NTN - tmean_c * tmean_c, 0.f)));
-    put(M_THIN_D_MEAN, n_shift + nmean_c);
-    put(M_THIN_D_MAX, nmax);
-    put(M_THIN_D_MIN, nmin);
-    put(M_THIN_D_STD, sqrtf(fmaxf(r[23] / (float)S - nmean_c * nmean_c, 0.f)));
-    // energies over thick filaments (metrics_fn.py:262-288)
-    float e_new = 0.f, e_delta = 0.f, te_new = 0.f, te_delta = 0.f;
+  // block reduction: warp partials to shared memory, then warp 0 finishes
+  // the 29 totals one per lane and writes the 52 metrics in parallel
+  constexpr int NW = NT / 32;
+  const int lane = m.lane, warp = m.warp;
+#pragma unroll
+  for (int k = 0; k < 29; ++k) r[k] = k < 4 ? warp_max(r[k]) : warp_sum(r[k]);
+  float* red = m.s.red;
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < 29; ++k) red[k * NW + warp] = r[k];
+  __syncthreads();
+  if (warp != 0) return;
+  float R = 0.f;
+  if (lane < 29) {
+    R = red[lane * NW];
+    for (int w = 1; w < NW; ++w) R = lane < 4 ? fmaxf(R, red[lane * NW + w]) : R + red[lane * NW + w];
+  }
+  auto tot = [&](int k) { return __shfl_sync(0xffffffffu, R, k); };
+  // energies over thick filaments (metrics_fn.py:262-288), one filament per lane
+  const float* P = m.s.P;
+  float e_new = 0.f, e_delta = 0.f, te_new = 0.f, te_delta = 0.f;
+  {
     const float k = P[THICK_K];
-    for (int th = 0; th < T.n_thick; ++th) {
+    const float a = P[TITIN_A], bb = P[TITIN_B], r0 = P[TITIN_REST];
+    for (int th = lane; th < T.n_thick; th += 32) {
       const int n0 = th * T.n_crowns;
       const float u_new = m.precise ? m.s.x[n0] : m.s.x[n0] - T.crown_off[n0];
       const float u_old = m.precise ? old_x[n0] : old_x[n0] - T.crown_off[n0];
@@ -239,7 +226,6 @@ __device__ void metrics(Sim<NT>& m, int t, float zl, float pCa, float new_ls, fl
         ad_new = zc - m.s.x[nl];
         ad_old = zc - old_x[nl];
       }
-      const float a = P[TITIN_A], bb = P[TITIN_B], r0 = P[TITIN_REST];
       const float Ln = sqrtf(ad_new * ad_new + new_ls * new_ls);
       const float Lo = sqrtf(ad_old * ad_old + new_ls * new_ls);
       const float tn = (a / bb) * (expf(bb * (Ln - r0)) - 1.0f);
@@ -247,18 +233,71 @@ __device__ void metrics(Sim<NT>& m, int t, float zl, float pCa, float new_ls, fl
       te_new += tn;
       te_delta += tn - to;
     }
+    e_new = warp_sum(e_new);
+    e_delta = warp_sum(e_delta);
+    te_new = warp_sum(te_new);
+    te_delta = warp_sum(te_delta);
+  }
+  const float tmin_ = -tot(0), tmax_ = tot(1), nmin_ = -tot(2), nmax_ = tot(3);
+  const float nb = tot(10), nov = tot(15), n2 = tot(16), n3 = tot(17);
+  const float r18 = tot(18), r19 = tot(19), r20 = tot(20), r21 = tot(21), r22 = tot(22), r23 = tot(23);
+  const float r24 = tot(24), r25 = tot(25), r26 = tot(26);
+  const float nx = (float)X, nt = (float)S;
+  // every shuffle above and here is executed by all 32 lanes; the branches
+  // below only store
+  const float own = tot(lane < 6 ? 4 + lane : (lane < 10 ? 5 + lane : 14));
+  auto put = [&](int k, float v) { Mo[(size_t)k * m.Tstride + t] = v; };
+  if (lane < 6) {
+    put(M_N_XB_DRX + lane, own);
+    put(M_FRAC_XB_DRX + lane, own / nx);
+  } else if (lane < 10) {
+    const int j = lane - 6;
+    put(M_N_TM_0 + j, own);
+    put(M_FRAC_TM_0 + j, own / nt);
+  } else if (lane == 10) {
+    put(M_AXIAL_FORCE, force);
+    put(M_SOLVER_RESIDUAL, (float)resid);
+    put(M_Z_LINE, zl);
+    put(M_PCA, pCa);
+    put(M_LATTICE_SPACING, new_ls);
+  } else if (lane == 11) {
+    put(M_N_BOUND, nb);
+    put(M_FRAC_XB_BOUND, nb / nx);
+    put(M_ACTIN_PERM, own / nt);
+  } else if (lane == 12) {
+    put(M_FRAC_TM_2_OV, n2 / nov);
+    put(M_FRAC_TM_3_OV, n3 / nov);
+    put(M_FRAC_TM_AVAIL_OV, (n2 + n3) / nov);
+    put(M_N_OVERLAP, nov);
+  } else if (lane == 13) {
+    put(M_ATP_CONSUMED, r18);
+    put(M_NEWLY_BOUND, r19);
+    put(M_ATP_EXPECTED_P, r25);
+    put(M_XB_TEAR, r26);
+    put(M_NEWTON_ITERS, (float)iters);
+  } else if (lane == 14) {
+    const float tmean_c = r20 / (float)NTN;
+    put(M_THICK_D_MEAN, t_shift + tmean_c);
+    put(M_THICK_D_MAX, tmax_);
+    put(M_THICK_D_MIN, tmin_);
+    put(M_THICK_D_STD, sqrtf(fmaxf(r21 / (float)NTN - tmean_c * tmean_c, 0.f)));
+  } else if (lane == 15) {
+    const float nmean_c = r22 / (float)S;
+    put(M_THIN_D_MEAN, n_shift + nmean_c);
+    put(M_THIN_D_MAX, nmax_);
+    put(M_THIN_D_MIN, nmin_);
+    put(M_THIN_D_STD, sqrtf(fmaxf(r23 / (float)S - nmean_c * nmean_c, 0.f)));
+  } else if (lane == 16) {
     const float fth = (float)T.n_thick;
     put(M_THICK_E_AVG, e_new / fth);
     put(M_THICK_E_DELTA, e_delta / fth);
     put(M_TITIN_E_AVG, te_new / fth);
     put(M_TITIN_E_DELTA, te_delta / fth);
-    const float work = force * (r[24] / (float)NTN);
+  } else if (lane == 17) {
+    const float work = force * (r24 / (float)NTN);
     put(M_WORK_THICK, work);
     put(M_WORK_THICK_MEAN, work / (float)NTN);
-    put(M_ATP_EXPECTED_P, r[25]);
-    put(M_XB_TEAR, r[26]);
-    put(M_WORK_PER_ATP, r[25] > 0.01f ? work / r[25] : 0.0f);
-    put(M_NEWTON_ITERS, (float)iters);
+    put(M_WORK_PER_ATP, r25 > 0.01f ? work / r25 : 0.0f);
   }
 }
 
