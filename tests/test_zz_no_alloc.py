@@ -98,7 +98,7 @@ def test_static_scratch_rejects_oversized_batch():
     eng = get_engine(0)
     topo = SarcTopology.create(2, 2)
     up = eng.upload(topo)
-    B, T = 200, 2  # ~200 x 120 kB of workspace: far beyond the 8 MiB array
+    B, T = 200, 2  # ~200 x 116 kB of workspace: far beyond the 8 MiB array
     dev = torch.device('cuda', 0)
     z = torch.full((B, T), 900.0, device=dev)
     ns = torch.full((B,), T, dtype=torch.int32, device=dev)
