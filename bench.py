@@ -118,7 +118,7 @@ def sweep_inputs():
 
 
 # ---------------------------------------------------------------------------
-# algorithmic work of one condition-timestep (Roofline)
+# algorithmic work of one condition-timestep
 # ---------------------------------------------------------------------------
 def flops_per_condition_step(topo, iters, n_bound, tables_rebuilt=0.0):
     """FP32 flops the fused step performs, counted from the kernel's arithmetic.
@@ -427,6 +427,80 @@ def profile_case(args):
     print(json.dumps({'profile_case': [B, T, n], 'force_last_mean': float(out['metrics'][:, 0, -1].mean())}))
 
 
+# ---------------------------------------------------------------------------
+# workload studies (one JSON line each; not the driver's bench line)
+# ---------------------------------------------------------------------------
+def uneven_conditions(n=512, seed=0):
+    """512 conditions: lattices nrows, ncols ~ U{1..4}, z ~ U[850, 1000] nm,
+    pCa ~ U[4, 7], duration ~ U[200, 1000] ms, lattice spacing solved as an
+    unknown with K_lat = 5, nu = 0.5, skeletal parameters, keys
+    split(PRNGKey(0), 512)[i]."""
+    from multifil_jax_b200 import SarcTopology, get_skeletal_params
+    from multifil_jax_b200.engine import prng_split, prng_key
+    rng = np.random.default_rng(seed)
+    s, d = get_skeletal_params()
+    topos, conds = {}, []
+    keys = prng_split(prng_key(0), n)
+    for i in range(n):
+        r, c = (int(v) for v in rng.integers(1, 5, 2))
+        if (r, c) not in topos:
+            topos[(r, c)] = SarcTopology.create(r, c, s, d)
+        conds.append(dict(topology=topos[(r, c)], z_line=float(rng.uniform(850, 1000)),
+                          pCa=float(rng.uniform(4, 7)), duration_ms=float(int(rng.uniform(200, 1000))),
+                          K_lat=5.0, nu=0.5, dynamic_params=d, key=keys[i]))
+    return conds, topos
+
+
+def study_uneven(args):
+    """Uneven batch in one launch: default CTA sizes vs the autotuner's."""
+    import torch
+    from multifil_jax_b200 import run_conditions
+    from multifil_jax_b200.autotune import autotune_many
+    conds, topos = uneven_conditions()
+    total = sum(int(c['duration_ms']) for c in conds)
+    out = {'study': 'uneven', 'metric': METRIC, 'conditions': len(conds), 'condition_timesteps': total,
+           'precision': args.precision, 'lattices': sorted(f'{r}x{c}' for r, c in topos)}
+
+    def timed():
+        run_conditions(conds, precision=args.precision)  # warm-up: every kernel variant loaded
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        run_conditions(conds, precision=args.precision)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0
+
+    out['default_threads'] = 'library default: 256 threads up to 1200 nodes, 512 up to 4000, else 1024'
+    t_def = timed()
+    tuned = autotune_many(list(topos.values()), precision=args.precision)
+    t_tuned = timed()
+    out['tuned_threads'] = {f'{r}x{c}': v for (r, c), v in sorted(tuned.items())}
+    out['default_value'] = total / t_def
+    out['tuned_value'] = total / t_tuned
+    out['wall_s'] = {'default': t_def, 'tuned': t_tuned}
+    out['note'] = 'wall time of run_conditions (host arrays in, host metrics out) for the whole batch'
+    print(json.dumps(out), flush=True)
+
+
+def study_serving(args):
+    """Serving at 50 / 80 / 95 % of the measured capacity of the request mix."""
+    import torch
+    res = []
+    cap_args = argparse.Namespace(**vars(args))
+    cap_args.serve_requests = args.study_capacity_requests
+    cap_args.serve_rate = 1e9  # every request arrives at t = 0: the server's capacity
+    cap = bench_serving(cap_args, 0)
+    mean_steps = cap['condition_timesteps_per_s'] * cap['wall_s'] / max(cap['requests'], 1)
+    cap_req = cap['requests'] / cap['wall_s']
+    res.append(dict(cap, load='capacity'))
+    for frac in (0.5, 0.8, 0.95):
+        a = argparse.Namespace(**vars(args))
+        a.serve_rate = frac * cap_req
+        r = bench_serving(a, 0)
+        res.append(dict(r, load=f'{int(frac * 100)}% of capacity'))
+    print(json.dumps({'study': 'serving', 'capacity_requests_per_s': cap_req, 'mean_steps_per_request': mean_steps,
+                      'runs': res}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -444,10 +518,17 @@ def main():
     ap.add_argument('--serve-budget-gb', type=int, default=8)
     ap.add_argument('--traffic', type=float, default=None)
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--study', default=None, choices=['uneven', 'serving'],
+                    help='run one workload study instead of the bench line')
+    ap.add_argument('--study-capacity-requests', type=int, default=2000)
     ap.add_argument('--profile-case', default=None,
                     help='B,T[,lattice]: run the fused kernel once on B conditions x T steps (for ncu)')
     args = ap.parse_args()
-    if args.profile_case:
+    if args.study == 'uneven':
+        study_uneven(args)
+    elif args.study == 'serving':
+        study_serving(args)
+    elif args.profile_case:
         profile_case(args)
     elif args.impl == 'reference':
         bench_reference(args)

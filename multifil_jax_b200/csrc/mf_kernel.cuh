@@ -10,6 +10,17 @@ namespace mf {
 // carve below must fit in the opt-in limit next to it.
 constexpr size_t kStaticSmem = 2048;
 
+// One region holds three phase-disjoint uses: the per-site scatter words of
+// the kinetics step (site = win1, then win2), the staged candidate positions
+// of the nearest-site search (face_pos, doubles, over both), and from the
+// bound-head list through the solve the per-site head pairs (site_h, over
+// site) next to the per-site head counts (win2).
+__host__ __device__ inline size_t site_region_bytes(const TopoDev& t) {
+  const size_t words = 8 * (size_t)t.n_sites_total;
+  const size_t faces = sizeof(double) * (size_t)t.n_thin * 3 * t.width;
+  return words > faces ? words : faces;
+}
+
 // Shared-memory bytes needed by one condition of this lattice with NT threads.
 __host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, bool vec_global) {
   const int N = t.n_dof, X = t.total_xbs, S = t.n_sites_total;
@@ -23,8 +34,7 @@ __host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, bool vec_
   if (!vec_global) add(sizeof(float) * 7 * N);  // x r dx pv zz wv sv
   if (!vec_global) add(sizeof(float) * 4 * X);  // fxb fdx fdd frdd
   add(sizeof(float) * X);                  // xb_ax
-  add(sizeof(float) * S);                  // site / win1
-  add(sizeof(int) * S);                    // win2
+  add(site_region_bytes(t));               // site / win1 | win2, overlaid by face_pos and site_h
   add(sizeof(int16_t) * 2 * X);            // xb_bound xb_near
   add(sizeof(int16_t) * S);                // thin_bound
   add(X);                                  // xb_state
@@ -39,9 +49,7 @@ __host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, bool vec_
   add(sizeof(int) * 32);                   // wsum
   add(sizeof(int16_t) * X);                // xb_key
   add(sizeof(int16_t) * X);                // hsite
-  add(sizeof(int16_t) * 2 * S);            // site_h
   if (!vec_global) add(sizeof(int16_t) * 6 * N);  // nb_node nb_head
-  add(sizeof(double) * t.n_thin * 3 * t.width);  // face_pos
   add(3 * t.n_thin * 3);                   // face_mono face_kl face_kh
   if (!vec_global) {                       // old-state snapshot
     add(sizeof(float) * t.n_thick_nodes);
@@ -66,8 +74,13 @@ __device__ void carve(Sim<NT>& m, char* base, bool vec_global) {
   float* f4 = vec_global ? reinterpret_cast<float*>(m.ws + m.L.vec) + 7 * N : (float*)take(sizeof(float) * 4 * X);
   m.s.fxb = f4; m.s.fdx = f4 + X; m.s.fdd = f4 + 2 * X; m.s.frdd = f4 + 3 * X;
   m.s.xb_ax = (float*)take(sizeof(float) * X);
-  m.s.site = (float*)take(sizeof(float) * S);
-  m.s.win2 = (int*)take(sizeof(int) * S);
+  {
+    char* reg = take(site_region_bytes(t));
+    m.s.site = (float*)reg;
+    m.s.win2 = (int*)(reg + sizeof(float) * S);
+    m.s.face_pos = (double*)reg;
+    m.s.site_h = (int16_t*)reg;  // 2S int16 = the bytes of site
+  }
   int16_t* i2 = (int16_t*)take(sizeof(int16_t) * 2 * X);
   m.s.xb_bound = i2; m.s.xb_near = i2 + X;
   m.s.thin_bound = (int16_t*)take(sizeof(int16_t) * S);
@@ -84,8 +97,6 @@ __device__ void carve(Sim<NT>& m, char* base, bool vec_global) {
   m.s.wsum = (int*)take(sizeof(int) * 32);
   m.s.xb_key = (int16_t*)take(sizeof(int16_t) * X);
   m.s.hsite = (int16_t*)take(sizeof(int16_t) * X);
-  m.s.site_h = (int16_t*)take(sizeof(int16_t) * 2 * S);
-  m.s.face_pos = (double*)take(sizeof(double) * t.n_thin * 3 * t.width);
   m.s.face_mono = (int8_t*)take(3 * t.n_thin * 3);
   m.s.face_kl = m.s.face_mono + t.n_thin * 3;
   m.s.face_kh = m.s.face_kl + t.n_thin * 3;

@@ -112,10 +112,10 @@ struct Smem {
   float* frdd;    // [X] d(radial)/dd per head (dynamic spacing)
   int16_t* blist; // [X] heads carrying force this step, increasing index
   int16_t* hsite; // [X] global site of a force-carrying head, else -1
-  int16_t* site_h;// [2S] first two force-carrying heads of every site
+  int16_t* site_h;// [2S] first two force-carrying heads of every site (over site)
   int16_t* nb_node; // [3N] partner nodes of every node (register CG only)
   int16_t* nb_head; // [3N] the heads behind them
-  double* face_pos; // [n_thin*3*width] staged candidate positions (NaN = invalid)
+  double* face_pos; // [n_thin*3*width] staged candidate positions, NaN = invalid (over site, win2)
   int8_t* face_mono;// [n_thin*3] 0 scan, 1 increasing, 2 decreasing, 3 no candidate
   int8_t* face_kl;  // [n_thin*3] first valid candidate
   int8_t* face_kh;  // [n_thin*3] last valid candidate

@@ -457,5 +457,92 @@ def run(topology: SarcTopology, duration_ms: float = 1000.0, dt: float = 1.0,
     return assemble_result(plan, metrics, sp, rng_seed, verbose)
 
 
-__all__ = ['run', 'SimulationResult', 'MetricsDict', 'METRIC_KEYS', 'BATCH_BUCKETS', 'get_bucket_size',
-           'plan_batch', 'assemble_result', 'BatchPlan']
+def run_conditions(conditions: List[dict], *, static_params: Optional[StaticParams] = None,
+                   precision: str = 'float32', device: Optional[int] = None, chunk_steps: int = 0,
+                   autotune: bool = False) -> List[MetricsDict]:
+    """Run independent conditions on different lattices and durations in one launch.
+
+    The reference needs one ``run()`` per (lattice, n_steps) pair, both being
+    JIT shapes; here every condition is one CTA of the same persistent launch,
+    grouped by CTA size.  Each condition is a dict with ``topology``,
+    ``duration_ms``, and optionally ``dt`` (1.0), ``pCa`` (4.5), ``z_line``
+    (900.0), ``lattice_spacing`` (14.0), ``K_lat`` (None: fixed spacing; else
+    the reference's per-thick-filament value, multiplied by ``n_thick`` as in
+    ``simulation.py:1002-1003``), ``nu`` (0.0), ``dynamic_params`` (the
+    skeletal defaults) and ``key`` (uint32[2]; default ``split(PRNGKey(0), B)[i]``).
+    Scalars only: one constant driver value per condition; the parameter
+    row itself keeps the DynamicParams constants, as ``run()`` does (the
+    initial equilibrium uses them, ``simulation.py:633-642``).  Either every
+    condition gives ``K_lat`` or none does.  ``autotune`` measures the CTA size
+    of every distinct lattice first (``autotune.autotune_many``).
+
+    Returns one MetricsDict per condition, each key an array of that
+    condition's ``n_steps``.
+    """
+    import torch
+    from .engine import get_engine, MF_FLAG_DYNAMIC_LS, MF_FLAG_PRECISE, prng_key, prng_split
+    from .params import get_skeletal_params
+    if precision not in PRECISIONS:
+        raise ValueError(f"precision must be one of {PRECISIONS}")
+    sp = static_params if static_params is not None else StaticParams()
+    B = len(conditions)
+    if B == 0:
+        return []
+    dyn = [c.get('K_lat') is not None for c in conditions]
+    if any(dyn) and not all(dyn):
+        raise ValueError("either every condition gives K_lat (dynamic lattice spacing) or none does")
+    default_keys = prng_split(prng_key(0), B)
+    _, d_default = get_skeletal_params()
+    steps = []
+    for c in conditions:
+        dt = float(c.get('dt', 1.0))
+        if dt <= 0:
+            raise ValueError("dt must be positive")
+        steps.append(int(float(c['duration_ms']) / dt))
+    if min(steps) < 1:
+        raise ValueError("every condition needs at least one timestep")
+    T = max(steps)
+    P = np.zeros((B, 44), np.float32)
+    Z = np.zeros((B, T), np.float32)
+    PC = np.zeros((B, T), np.float32)
+    L = np.zeros((B, T), np.float32)
+    K = np.zeros(B, np.float32)
+    NU = np.zeros(B, np.float32)
+    DT = np.zeros(B, np.float32)
+    KEYS = np.zeros((B, 2), np.uint32)
+    for i, c in enumerate(conditions):
+        dp = c.get('dynamic_params') or d_default
+        z, pca, ls = float(c.get('z_line', 900.0)), float(c.get('pCa', 4.5)), float(c.get('lattice_spacing', 14.0))
+        P[i] = dp.param_row()  # the constants, as run() passes them
+        Z[i], PC[i], L[i] = z, pca, ls
+        if dyn[i]:
+            K[i] = np.float32(float(c['K_lat']) * c['topology'].n_thick)
+        NU[i] = float(c.get('nu', 0.0))
+        DT[i] = float(c.get('dt', 1.0))
+        KEYS[i] = np.asarray(c['key'], np.uint32) if c.get('key') is not None else default_keys[i]
+    topos = [c['topology'] for c in conditions]
+    if autotune:
+        from .autotune import autotune_many
+        autotune_many(topos, precision=precision, device=device)
+    eng = get_engine(device)
+    dev = torch.device('cuda', eng.device)
+    flags = (MF_FLAG_DYNAMIC_LS if all(dyn) else 0) | (MF_FLAG_PRECISE if precision == 'mixed' else 0)
+    f = lambda a: torch.as_tensor(a, device=dev)
+    with torch.cuda.device(dev):
+        res = eng.run_batch(topos, f(P), f(Z), f(PC), f(L), f(np.asarray(steps, np.int32)),
+                            f(KEYS.astype(np.int64)).to(torch.int32), K_lat=f(K), nu=f(NU), dt=f(DT),
+                            n_newton=sp.n_newton_steps, n_cg=sp.n_cg_steps, flags=flags, chunk_steps=chunk_steps,
+                            residual_warn=sp.solver_residual_tol)
+        m = res['metrics'].cpu().numpy()
+    out = []
+    for i, n in enumerate(steps):
+        md = MetricsDict()
+        for k, name in enumerate(METRIC_KEYS):
+            v = m[i, k, :n]
+            md[name] = v.astype(np.int32) if name == 'newton_iters' else v.copy()
+        out.append(md)
+    return out
+
+
+__all__ = ['run', 'run_conditions', 'SimulationResult', 'MetricsDict', 'METRIC_KEYS', 'BATCH_BUCKETS',
+           'get_bucket_size', 'plan_batch', 'assemble_result', 'BatchPlan']

@@ -199,3 +199,28 @@ def test_bad_arguments_raise(engine):
     with pytest.raises(EngineError):
         run_engine(engine, topo, d.param_row()[None], np.full((1, 4), 900.0), np.full((1, 4), 4.5),
                    np.full((1, 4), 14.0), prng.split(prng.PRNGKey(0), 1), n_steps=[9])
+
+
+def test_run_conditions_matches_run_per_condition():
+    """Mixed lattices, durations, dt and spacing modes in one launch equal one run() each."""
+    from multifil_jax_b200 import run_conditions
+    from multifil_jax_b200.engine import prng_split, prng_key
+    s, d = get_skeletal_params()
+    _, c = get_cardiac_params()
+    t22, t11, t32 = (SarcTopology.create(r, k, s, d) for r, k in ((2, 2), (1, 1), (3, 2)))
+    conds = [dict(topology=t22, duration_ms=20, pCa=5.0, z_line=910.0, key=prng_split(prng_key(3), 1)[0]),
+             dict(topology=t11, duration_ms=6, dt=0.5, pCa=4.5, dynamic_params=c, key=prng_split(prng_key(4), 1)[0]),
+             dict(topology=t32, duration_ms=9, pCa=6.0, lattice_spacing=13.5, key=prng_split(prng_key(5), 1)[0])]
+    got = run_conditions(conds, precision='mixed')
+    for cond, seed, g in zip(conds, (3, 4, 5), got):
+        ref = run(cond['topology'], duration_ms=cond['duration_ms'], dt=cond.get('dt', 1.0), pCa=cond['pCa'],
+                  z_line=cond.get('z_line', 900.0), lattice_spacing=cond.get('lattice_spacing', 14.0),
+                  dynamic_params=cond.get('dynamic_params'), rng_seed=seed, precision='mixed')
+        for k in METRIC_KEYS:
+            assert np.array_equal(np.asarray(ref.metrics[k]).reshape(-1), g[k]), k
+    dyn = run_conditions([dict(topology=t22, duration_ms=8, K_lat=5.0, nu=0.5),
+                          dict(topology=t11, duration_ms=5, K_lat=5.0, nu=0.5)])
+    ref = run(t22, duration_ms=8, K_lat=5.0, nu=0.5, rng_seed=0)
+    assert np.array_equal(ref.metrics['lattice_spacing'].reshape(-1), dyn[0]['lattice_spacing'])
+    with pytest.raises(ValueError):
+        run_conditions([dict(topology=t22, duration_ms=5, K_lat=5.0), dict(topology=t11, duration_ms=5)])
