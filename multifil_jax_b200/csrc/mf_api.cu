@@ -14,6 +14,7 @@
 
 #include "../../include/multifil_b200.h"
 #include "mf_kernel.cuh"
+#include "mf_launch.cuh"
 
 using namespace mf;
 
@@ -70,47 +71,26 @@ static int fail(mf_ctx* c, int code, const char* fmt, ...) {
   } while (0)
 
 // ---------------------------------------------------------------------------
-// kernel dispatch by CTA size
+// kernel dispatch by CTA size and precision (instances in mf_kernels.cu)
 // ---------------------------------------------------------------------------
-// Raise the dynamic shared-memory limit of a kernel instance (not capturable,
-// so it is done before any graph capture).
-template <int NT>
-static cudaError_t prepare_nt(size_t smem) {
-  static size_t attr_bytes = 0;
-  if (smem > attr_bytes) {
-    cudaError_t e = cudaFuncSetAttribute(step_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return e;
-    attr_bytes = smem;
-  }
-  return cudaSuccess;
-}
-
-static cudaError_t prepare(int nt, size_t smem) {
-  switch (nt) {
-    case 128: return prepare_nt<128>(smem);
-    case 256: return prepare_nt<256>(smem);
-    case 512: return prepare_nt<512>(smem);
-    default: return prepare_nt<1024>(smem);
-  }
-}
-
-template <int NT>
-static cudaError_t launch_nt(const StepArgs& a, int grid, int base, size_t smem, cudaStream_t st) {
-  step_kernel<NT><<<grid, NT, smem, st>>>(a, base);
-  return cudaPeekAtLastError();
+static cudaError_t prepare(int nt, bool precise, size_t smem) {
+#define MF_PREPARE_CASE(NT, P) \
+  if (nt == NT && precise == (P != 0)) return prepare_##NT##_##P(smem);
+  MF_FOR_EACH_INSTANCE(MF_PREPARE_CASE)
+#undef MF_PREPARE_CASE
+  return cudaErrorInvalidValue;
 }
 
 static cudaError_t launch(int nt, const StepArgs& a, int grid, int base, size_t smem, cudaStream_t st) {
-  cudaError_t e = prepare(nt, smem);
+  const bool precise = (a.flags & FLAG_PRECISE) != 0;
+  cudaError_t e = prepare(nt, precise, smem);
   if (e != cudaSuccess) return e;
   cudaGetLastError();  // clear a stale non-sticky error of an earlier, already reported call
-  switch (nt) {
-    case 128: return launch_nt<128>(a, grid, base, smem, st);
-    case 256: return launch_nt<256>(a, grid, base, smem, st);
-    case 512: return launch_nt<512>(a, grid, base, smem, st);
-    default: return launch_nt<1024>(a, grid, base, smem, st);
-  }
+#define MF_LAUNCH_CASE(NT, P) \
+  if (nt == NT && precise == (P != 0)) return launch_##NT##_##P(a, grid, base, smem, st);
+  MF_FOR_EACH_INSTANCE(MF_LAUNCH_CASE)
+#undef MF_LAUNCH_CASE
+  return cudaErrorInvalidValue;
 }
 
 static int default_threads(const TopoDev& t) {
@@ -268,8 +248,8 @@ int mf_upload_topology(mf_ctx* ctx, const mf_topo_desc* d, int32_t* topo_id) {
 int mf_tune_threads(mf_ctx* ctx, int32_t topo_id, int32_t threads) {
   if (!ctx || topo_id < 0 || topo_id >= (int)ctx->topos.size())
     return fail(ctx, MF_ERR_NOTFOUND, "unknown topology");
-  if (threads != 128 && threads != 256 && threads != 512 && threads != 1024)
-    return fail(ctx, MF_ERR_INVALID, "threads must be 128, 256, 512 or 1024");
+  if (threads != 128 && threads != 256 && threads != 384 && threads != 512 && threads != 1024)
+    return fail(ctx, MF_ERR_INVALID, "threads must be 128, 256, 384, 512 or 1024");
   TopoHost& t = *ctx->topos[topo_id];
   size_t sm = smem_bytes(t.dev, threads, false);
   bool vg = sm + kStaticSmem > (size_t)ctx->smem_optin;
@@ -490,7 +470,7 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
       CK(cudaEventCreateWithFlags(&ctx->cap_event, cudaEventDisableTiming));
     }
     launch_st = ctx->cap_stream;
-    for (const Group& g : groups) CK(prepare(g.threads, g.smem));
+    for (const Group& g : groups) CK(prepare(g.threads, (base_flags & FLAG_PRECISE) != 0, g.smem));
     CK(cudaEventRecord(ctx->cap_event, st));
     CK(cudaStreamWaitEvent(launch_st, ctx->cap_event, 0));
     CK(cudaStreamBeginCapture(launch_st, cudaStreamCaptureModeThreadLocal));

@@ -174,7 +174,7 @@ __device__ __forceinline__ void cum6(const float* p, float* c) {
 }
 
 // Tropomyosin generator of configuration cfg = 9*n2 + 3*n3 + n_closed.
-__device__ void tm_generator(const float* P, float pCa, int cfg, float* Q) {
+static __device__ void tm_generator(const float* P, float pCa, int cfg, float* Q) {
   const float ca = powf(10.0f, -pCa);
   const float n2 = (float)(cfg / 9), n3 = (float)((cfg / 3) % 3), nc = (float)(cfg % 3);
   const float JC = P[TM_J_C], JM = P[TM_J_M];
@@ -196,7 +196,7 @@ __device__ void tm_generator(const float* P, float pCa, int cfg, float* Q) {
 }
 
 // Crossbridge generator at axial offset x, spacing d, permissiveness perm.
-__device__ void xb_generator(const float* P, float pCa, float x, float d, float perm, float* Q) {
+static __device__ void xb_generator(const float* P, float pCa, float x, float d, float perm, float* Q) {
   const float ca = powf(10.0f, -pCa);
   const float r = sqrtf(x * x + d * d);
   const float th = atan2f(d, x);

@@ -59,8 +59,8 @@ __host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, bool vec_
   return o;
 }
 
-template <int NT>
-__device__ void carve(Sim<NT>& m, char* base, bool vec_global) {
+template <int NT, bool PR>
+__device__ void carve(Sim<NT, PR>& m, char* base, bool vec_global) {
   const TopoDev& t = m.T;
   const int N = t.n_dof, X = t.total_xbs, S = t.n_sites_total;
   const int scan = t.plan_thin.total > t.plan_thick.total ? t.plan_thin.total : t.plan_thick.total;
@@ -122,8 +122,8 @@ __device__ void carve(Sim<NT>& m, char* base, bool vec_global) {
 // ---------------------------------------------------------------------------
 // metrics epilogue (metrics_fn.py:154-417), written to metrics[b][k][t]
 // ---------------------------------------------------------------------------
-template <int NT>
-__device__ void metrics(Sim<NT>& m, int t, float zl, float pCa, float new_ls, float force, double resid,
+template <int NT, bool PR>
+__device__ void metrics(Sim<NT, PR>& m, int t, float zl, float pCa, float new_ls, float force, double resid,
                         int iters, float* Mo) {
   const TopoDev& T = m.T;
   const int X = T.total_xbs, S = T.n_sites_total, NTN = T.n_thick_nodes;
@@ -323,7 +323,7 @@ __device__ void metrics(Sim<NT>& m, int t, float zl, float pCa, float new_ls, fl
     __syncthreads();                              \
     if (m.tid == 0) {                             \
       const long long now_ = clock64();           \
-      ph_acc[ph_cur] += (double)(now_ - ph_t0);   \
+      ph_sh[ph_cur] += (double)(now_ - ph_t0);    \
       ph_t0 = now_;                               \
       ph_cur = (k);                               \
     }                                             \
@@ -332,10 +332,13 @@ __device__ void metrics(Sim<NT>& m, int t, float zl, float pCa, float new_ls, fl
 #define MF_PH(k) do { } while (0)
 #endif
 
-template <int NT>
+template <int NT, bool PR>
 __device__ void run_condition(const StepArgs& A, int ci) {
 #ifdef MF_PHASE_TIMING
-  double ph_acc[12] = {0};
+  // totals in shared memory: a runtime-indexed local array would add a
+  // local-memory round trip to every marker
+  __shared__ double ph_sh[20];
+  if (threadIdx.x < 20) ph_sh[threadIdx.x] = 0.0;
   long long ph_t0 = clock64();
   int ph_cur = 0;
 #endif
@@ -354,14 +357,16 @@ __device__ void run_condition(const StepArgs& A, int ci) {
   __syncthreads();
   const CondDesc& cd = sh_cd;
   const TopoDev& T = sh_T;
-  Sim<NT> m(T, A, sh_s, sh_cl, sh_L);
+  Sim<NT, PR> m(T, A, sh_s, sh_cl, sh_L);
+#ifdef MF_PHASE_TIMING
+  m.sub_acc = ph_sh + 12;
+#endif
   m.tid = threadIdx.x;
   m.lane = m.tid & 31;
   m.warp = m.tid >> 5;
   m.b = cd.index;
   m.ws = cd.ws;
   m.dyn = (A.flags & FLAG_DYN) != 0;
-  m.precise = (A.flags & FLAG_PRECISE) != 0;
   m.part = (A.flags & FLAG_ORIG_PRNG) == 0;
   m.status = 0;
   m.Tstride = cd.T;
@@ -369,8 +374,8 @@ __device__ void run_condition(const StepArgs& A, int ci) {
   __syncthreads();
   {
     const int nf = T.n_thick + T.n_thin;
-    m.regcg = m.precise && A.n_cg > 0 && (A.flags & 64) == 0 && nf <= Sim<NT>::RF * (NT / 32) &&
-              T.n_crowns <= 32 * Sim<NT>::RE && T.n_sites <= 32 * Sim<NT>::RE && T.nxb <= 3;
+    m.regcg = PR && A.n_cg > 0 && (A.flags & 64) == 0 && nf <= Sim<NT, PR>::RF * (NT / 32) &&
+              T.n_crowns <= 32 * Sim<NT, PR>::RE && T.n_sites <= 32 * Sim<NT, PR>::RE && T.nxb <= 3;
   }
   const int b = m.b;
   const int N = T.n_dof, X = T.total_xbs, S = T.n_sites_total, NTN = T.n_thick_nodes;
@@ -401,6 +406,9 @@ __device__ void run_condition(const StepArgs& A, int ci) {
 
   __shared__ uint32_t key_s[2];
   __shared__ float ls_s;
+  // (pCa, d) of the sampling and absorbing tables in the workspace and the
+  // initial z: read from shared memory every step, persisted at launch end
+  __shared__ double tab_key[5];
   if (t0 == 0) {
     // ---- realize_state + initial equilibrium with the constants (A1) ----
     m.zref = (double)zt[0];
@@ -421,29 +429,8 @@ __device__ void run_condition(const StepArgs& A, int ci) {
     __threadfence_block();
     for (int i = m.tid; i < m.cl.total; i += NT) m.s.coef[i] = coef_g[i];
     __syncthreads();
-    m.nearest(m.s.P[LATTICE_SPACING]);
-    __syncthreads();
-    // table rows of the initial geometry (every site starts in state 0: block 0)
-    for (int i = m.tid; i < X; i += NT) m.s.xb_key[i] = (int16_t)m.bin_of(m.s.xb_ax[i]);
-    double resid;
-    int it;
-    float d0 = m.s.P[LATTICE_SPACING];
-    const bool dyn_save = m.dyn;
-    m.dyn = false;
-    m.build_bound_list();
-    m.solve(m.s.P[Z_LINE], d0, resid, it, false);
-    m.dyn = dyn_save;
-    if (m.tid == 0) {
-      key_s[0] = cd.key[0];
-      key_s[1] = cd.key[1];
-      ls_s = lt[0];
-      misc[MS_TAB_PCA] = NAN;
-      misc[MS_TAB_D] = NAN;
-      misc[MS_ABS_PCA] = NAN;
-      misc[MS_ABS_D] = NAN;
-      misc[MS_L0] = (double)zt[0];
-    }
-    __syncthreads();
+    // the initial equilibrium itself runs as step -1 of the loop below, so
+    // that the nearest-site search and the solver have one call site each
   } else {
     // ---- resume a condition from its resident workspace ----
     m.zref = misc[MS_ZREF];
@@ -467,6 +454,11 @@ __device__ void run_condition(const StepArgs& A, int ci) {
       key_s[1] = kk[1];
       ls_s = (float)misc[MS_CUR_LS];
       m.status = (int)misc[MS_STATUS];
+      tab_key[0] = misc[MS_TAB_PCA];
+      tab_key[1] = misc[MS_TAB_D];
+      tab_key[2] = misc[MS_ABS_PCA];
+      tab_key[3] = misc[MS_ABS_D];
+      tab_key[4] = misc[MS_L0];
     }
     __syncthreads();
   }
@@ -474,78 +466,120 @@ __device__ void run_condition(const StepArgs& A, int ci) {
   // pre-step snapshot buffers live in global workspace is avoided: keep the
   // old thick positions / states in the spare CG vectors between phases
   float* Mo = cd.metrics;
-  for (int t = t0; t < t1; ++t) {
-    const float zl = zt[t], pCa = pt[t], ls_t = lt[t];
-    const float dz = t > 0 ? zt[t] - zt[t - 1] : 0.0f;
-    // 1. rigid shift of the thin filaments
-    if (!m.precise) {
-      for (int i = NTN + m.tid; i < N; i += NT) m.s.x[i] = m.s.x[i] + dz;
+  __shared__ uint32_t sub_thin[2], sub_thick[2];
+  // drivers of step t are loaded during step t - 1 (their latency overlaps a
+  // whole step instead of opening one)
+  float nx_z = t0 < t1 ? zt[t0] : 0.0f, nx_p = t0 < t1 ? pt[t0] : 0.0f, nx_l = t0 < t1 ? lt[t0] : 0.0f;
+  float prev_z = t0 > 0 ? zt[t0 - 1] : 0.0f;
+  // t = -1: the initial equilibrium with the constants (A1): nearest sites
+  // at the constant spacing, table rows of the initial geometry, one solve
+  // at the constant z_line with the spacing held fixed.
+  for (int t = t0 == 0 ? -1 : t0; t < t1; ++t) {
+    const bool init = t < 0;
+    float zl, pCa = 0.0f, ls_t = 0.0f, cur_ls = 0.0f, d_kin;
+    if (init) {
+      zl = m.s.P[Z_LINE];
+      d_kin = m.s.P[LATTICE_SPACING];
     } else {
-      m.zref = (double)zl;
-    }
-    const float cur_ls = ls_s;
-    float d_kin;
-    if (m.dyn) {
-      d_kin = cur_ls;
-      const float l0 = (float)misc[MS_L0];
-      m.d_ref = ls_t * powf(l0 / zl, m.nu_c);
-    } else {
-      d_kin = ls_t;
-    }
-    MF_PH(1);
-    // probability tables for (pCa, d_kin)
-    if (!((double)pCa == misc[MS_TAB_PCA] && (double)d_kin == misc[MS_TAB_D])) {
+      zl = nx_z;
+      pCa = nx_p;
+      ls_t = nx_l;
+      const float dz = t > 0 ? zl - prev_z : 0.0f;
+      prev_z = zl;
+      if (t + 1 < t1) {
+        nx_z = zt[t + 1];
+        nx_p = pt[t + 1];
+        nx_l = lt[t + 1];
+      }
+      // 1. rigid shift of the thin filaments
+      if (!m.precise) {
+        for (int i = NTN + m.tid; i < N; i += NT) m.s.x[i] = m.s.x[i] + dz;
+      } else {
+        m.zref = (double)zl;
+      }
+      cur_ls = ls_s;
+      if (m.dyn) {
+        d_kin = cur_ls;
+        const float l0 = (float)tab_key[4];
+        m.d_ref = ls_t * powf(l0 / zl, m.nu_c);
+      } else {
+        d_kin = ls_t;
+      }
+      MF_PH(1);
+      // probability tables for (pCa, d_kin)
+      if (!((double)pCa == tab_key[0] && (double)d_kin == tab_key[1])) {
+        __syncthreads();
+        m.build_tables(pCa, d_kin, true, false);
+        __syncthreads();
+        if (m.tid == 0) { tab_key[0] = pCa; tab_key[1] = d_kin; }
+        __threadfence_block();
+        __syncthreads();
+      }
+      MF_PH(2);
+      // old_state snapshot for the metrics (metrics_fn.py reads the pre-step
+      // geometry)
+      for (int i = m.tid; i < NTN; i += NT) m.s.old_thick[i] = m.s.x[i];
+      for (int i = m.tid; i < X; i += NT) {
+        m.s.old_xbs[i] = m.s.xb_state[i];
+        m.s.old_key[i] = m.s.xb_key[i];
+      }
       __syncthreads();
-      m.build_tables(pCa, d_kin, true, false);
-      __syncthreads();
-      if (m.tid == 0) { misc[MS_TAB_PCA] = pCa; misc[MS_TAB_D] = d_kin; }
-      __threadfence_block();
-      __syncthreads();
+      if (m.tid == 0) {
+        uint32_t kn[2];
+        step_keys(m.part, key_s[0], key_s[1], sub_thin, sub_thick, kn);
+        key_s[0] = kn[0];
+        key_s[1] = kn[1];
+      }
+      MF_PH(3);
     }
-    MF_PH(2);
-    // old_state snapshot for the metrics (metrics_fn.py reads the pre-step
-    // geometry): parked in the resident workspace arrays, which are only
-    // rewritten with the live state at the end of the launch.
-    for (int i = m.tid; i < NTN; i += NT) m.s.old_thick[i] = m.s.x[i];
-    for (int i = m.tid; i < X; i += NT) {
-      m.s.old_xbs[i] = m.s.xb_state[i];
-      m.s.old_key[i] = m.s.xb_key[i];
-    }
-    __syncthreads();
     // 2-4. kinetics
-    __shared__ uint32_t sub_thin[2], sub_thick[2];
-    if (m.tid == 0) {
-      uint32_t kn[2];
-      step_keys(m.part, key_s[0], key_s[1], sub_thin, sub_thick, kn);
-      key_s[0] = kn[0];
-      key_s[1] = kn[1];
-    }
-    MF_PH(3);
     m.nearest(d_kin);
     __syncthreads();
     MF_PH(4);
-    const size_t inj_t = ((size_t)b * A.T + t) * (size_t)S;
-    const size_t inj_x = ((size_t)b * A.T + t) * (size_t)X;
-    m.thin_step(sub_thin, inj_t);
-    MF_PH(5);
-    m.thick_step(sub_thick, inj_x);
-    MF_PH(6);
+    if (init) {
+      // table rows of the initial geometry (every site starts in state 0: block 0)
+      for (int i = m.tid; i < X; i += NT) m.s.xb_key[i] = (int16_t)m.bin_of(m.s.xb_ax[i]);
+    } else {
+      const size_t inj_t = ((size_t)b * A.T + t) * (size_t)S;
+      const size_t inj_x = ((size_t)b * A.T + t) * (size_t)X;
+      m.thin_step(sub_thin, inj_t);
+      MF_PH(5);
+      m.thick_step(sub_thick, inj_x);
+      MF_PH(6);
+    }
     // 5. mechanics
     double resid;
     int iters;
-    float d = m.dyn ? cur_ls : ls_t;
+    const bool dyn_save = m.dyn;
+    m.dyn = dyn_save && !init;
+    float d = init ? d_kin : (m.dyn ? cur_ls : ls_t);
     m.build_bound_list();
     MF_PH(7);
     m.solve(zl, d, resid, iters, m.dyn);
     MF_PH(8);
+    m.dyn = dyn_save;
+    if (init) {
+      if (m.tid == 0) {
+        key_s[0] = cd.key[0];
+        key_s[1] = cd.key[1];
+        ls_s = lt[0];
+        tab_key[0] = NAN;
+        tab_key[1] = NAN;
+        tab_key[2] = NAN;
+        tab_key[3] = NAN;
+        tab_key[4] = (double)zt[0];
+      }
+      __syncthreads();
+      continue;
+    }
     const float new_ls = m.dyn ? d : ls_t;
     if (m.tid == 0) ls_s = new_ls;
     // absorbing table for the metrics at (pCa, new_ls)
-    if (!((double)pCa == misc[MS_ABS_PCA] && (double)new_ls == misc[MS_ABS_D])) {
+    if (!((double)pCa == tab_key[2] && (double)new_ls == tab_key[3])) {
       __syncthreads();
       m.build_tables(pCa, new_ls, false, true);
       __syncthreads();
-      if (m.tid == 0) { misc[MS_ABS_PCA] = pCa; misc[MS_ABS_D] = new_ls; }
+      if (m.tid == 0) { tab_key[2] = pCa; tab_key[3] = new_ls; }
       __threadfence_block();
     }
     __syncthreads();
@@ -590,8 +624,7 @@ __device__ void run_condition(const StepArgs& A, int ci) {
 #ifdef MF_PHASE_TIMING
   if (m.tid == 0 && A.x_trace) {
     float* o = A.x_trace + (size_t)b * A.T * A.max_dof;
-    for (int k = 0; k < 12; ++k) o[k] = (float)ph_acc[k];
-    for (int k = 0; k < 8; ++k) o[12 + k] = (float)m.sub_acc[k];
+    for (int k = 0; k < 20; ++k) o[k] = (float)ph_sh[k];
   }
 #endif
   // ---- write back resident state ----
@@ -616,17 +649,27 @@ __device__ void run_condition(const StepArgs& A, int ci) {
     misc[MS_CUR_LS] = ls_s;
     misc[MS_ZREF] = m.zref;
     misc[MS_STATUS] = (double)(m.status | st_all);
+    misc[MS_TAB_PCA] = tab_key[0];
+    misc[MS_TAB_D] = tab_key[1];
+    misc[MS_ABS_PCA] = tab_key[2];
+    misc[MS_ABS_D] = tab_key[3];
+    misc[MS_L0] = tab_key[4];
     if (cd.status) *cd.status = m.status | st_all;
     if (cd.key_out) { cd.key_out[0] = key_s[0]; cd.key_out[1] = key_s[1]; }
   }
 }
 
-// Register cap of 128 per thread (64 at 1024 threads) so that several
-// conditions share an SM; the table builder's 6x6 temporaries spill instead.
-template <int NT>
-__global__ void __launch_bounds__(NT, (65536 / (NT * 128)) > 0 ? 65536 / (NT * 128) : 1)
+// Register cap of 128 per thread (80 at 384 threads, 64 at 1024) so that
+// several conditions share an SM; the table builder's 6x6 temporaries spill
+// instead.  min_ctas: resident CTAs per SM the register budget is sized for.
+constexpr int min_ctas(int nt) { return nt == 384 ? 2 : ((65536 / (nt * 128)) > 0 ? 65536 / (nt * 128) : 1); }
+
+// PR: precise (mixed) mode, a compile-time choice so that each kernel holds
+// only its own solver.
+template <int NT, bool PR>
+__global__ void __launch_bounds__(NT, min_ctas(NT))
     step_kernel(StepArgs A, int cond_base) {
-  run_condition<NT>(A, cond_base + blockIdx.x);
+  run_condition<NT, PR>(A, cond_base + blockIdx.x);
 }
 
 }  // namespace mf

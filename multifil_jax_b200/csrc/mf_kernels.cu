@@ -1,0 +1,32 @@
+// One instance of the fused step kernel: step_kernel<MF_NT, MF_P> and its
+// launch entry points (declared in mf_launch.cuh).  Built once per instance:
+//   nvcc ... -DMF_NT=256 -DMF_P=1 -c mf_kernels.cu
+#include "mf_kernel.cuh"
+#include "mf_launch.cuh"
+
+#if !defined(MF_NT) || !defined(MF_P)
+#error "compile with -DMF_NT=<CTA size> -DMF_P=<0|1>"
+#endif
+
+#define MF_PASTE(a, b, c) a##b##_##c
+#define MF_NAME(a, b, c) MF_PASTE(a, b, c)
+
+namespace mf {
+
+cudaError_t MF_NAME(prepare_, MF_NT, MF_P)(size_t smem) {
+  static size_t attr_bytes = 0;
+  if (smem > attr_bytes) {
+    cudaError_t e = cudaFuncSetAttribute(step_kernel<MF_NT, (MF_P != 0)>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr_bytes = smem;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t MF_NAME(launch_, MF_NT, MF_P)(const StepArgs& a, int grid, int base, size_t smem, cudaStream_t st) {
+  step_kernel<MF_NT, (MF_P != 0)><<<grid, MF_NT, smem, st>>>(a, base);
+  return cudaPeekAtLastError();
+}
+
+}  // namespace mf

@@ -152,7 +152,7 @@ __host__ __device__ inline CoefLayout coef_layout(const TopoDev& t) {
 // the three absorbing-chain entries the metrics read ("absorbing", global).
 // Out of line: it runs only when pCa or the spacing changes, and its
 // unrolled Pade arithmetic would otherwise sit in the step loop's code.
-__device__ __noinline__ void build_tables_block(const float* P, const float* centers, int nb, float pCa, float d,
+static __device__ __noinline__ void build_tables_block(const float* P, const float* centers, int nb, float pCa, float d,
                                                 float dtm, int sq64, float* cum_tm, float* cum_xb, float* pabs,
                                                 bool sampling, bool absorbing, int tid, int nt) {
   if (sampling) {
@@ -186,7 +186,7 @@ __device__ __noinline__ void build_tables_block(const float* P, const float* cen
   }
 }
 
-template <int NT>
+template <int NT, bool PR>
 struct Sim {
   static constexpr int NW = NT / 32;
   // The lattice, the shared-memory carve and the layouts live in CTA-shared
@@ -200,7 +200,8 @@ struct Sim {
   char* ws;
   int b;        // caller row
   int tid, lane, warp;
-  bool dyn, precise, part;
+  static constexpr bool precise = PR;
+  bool dyn, part;
   bool regcg;   // register-resident precise Newton-CG (solve_regs)
   float Kl, nu_c, dtm;
   double zref;  // precise mode thin reference z
@@ -212,7 +213,7 @@ struct Sim {
 #ifdef MF_PHASE_TIMING
   // diagnostic build only: thread 0's clock64() totals of solver sub-phases
   long long sub_t0 = 0;
-  double sub_acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double* sub_acc = nullptr;  // the phase totals' shared array, slots 12..19
 #define MF_SUB(k)                                               \
   do {                                                          \
     __syncthreads();                                            \
@@ -872,67 +873,77 @@ struct Sim {
   }
 
   // ------------------------------------------------------------------
-  // Newton-CG (solver.py:329-427, 599-656)
+  // Newton-CG (solver.py:329-427, 599-656).  Every piece (residual,
+  // preconditioner, JVP) has one call site per solver, so each is inlined
+  // once: the first Newton residual and the later ones share the loop top,
+  // the initial preconditioned residual and the in-loop ones share the CG
+  // loop body.
   // ------------------------------------------------------------------
   __device__ __forceinline__ void solve(float zl, float& d, double& resid, int& iters, bool dyn_jdd) {
-    if (regcg) {
-      solve_regs(zl, d, resid, iters, dyn_jdd);
-      return;
+    if constexpr (PR) {
+      if (regcg) solve_regs(zl, d, resid, iters, dyn_jdd);
+      else solve_cg_gear(zl, d, resid, iters, dyn_jdd);
+    } else {
+      solve_std(zl, d, resid, iters, dyn_jdd);
     }
-    if (precise && A.n_cg > 0) {
-      solve_cg_gear(zl, d, resid, iters, dyn_jdd);
-      return;
-    }
+  }
+
+  // float32 mode: the reference's PCG recurrences and association orders.
+  __device__ __forceinline__ void solve_std(float zl, float& d, double& resid, int& iters, bool dyn_jdd) {
     const float tol = fmaxf(s.P[SOLVER_TOL], fmaxf(s.P[THICK_K] * 1e-4f, 0.25f));
-    float frad = 0.f, jdd = 0.f;
-    float fmx = residual(zl, d, &frad, &jdd, 0, nullptr);
-    // exact radial diagonal at the pre-solve point (solver.py:633-638)
-    const float J_dd_inv = dyn_jdd ? -1.0f / jdd : 0.f;
     const int n_cg = A.n_cg, n_newton = A.n_newton;
     float* __restrict__ xv = s.x;
     float* __restrict__ rv = s.r;
     float* __restrict__ zv = s.zz;
     float* __restrict__ pv = s.pv;
     float* __restrict__ dxv = s.dx;
-    int it = 0, bad = 0;
-    while (fmx > tol && it < n_newton) {
-      float r_d = frad, z_d = 0.f, p_d = 0.f, dx_d = 0.f, Ap_d = 0.f;
-      precondition_own(rv, zv);
-      float part[1] = {0.f};
-      own_nodes([&](int i, int, int, bool) {
-        pv[i] = zv[i];
-        dxv[i] = n_cg == 0 ? zv[i] : 0.f;
-        part[0] = fmaf(rv[i], zv[i], part[0]);
-      });
-      if (dyn) {
-        z_d = J_dd_inv * r_d;
-        p_d = z_d;
-        if (n_cg == 0) dx_d = z_d;
+    float frad = 0.f, jdd = 0.f, J_dd_inv = 0.f, fmx = 0.f;
+    int it = 0, bad = 0, bad_local = 0;
+    for (int nw = 0;; ++nw) {
+      fmx = residual(zl, d, &frad, nw == 0 ? &jdd : nullptr, bad_local, nw == 0 ? nullptr : &bad);
+      if (nw == 0) {
+        // exact radial diagonal at the pre-solve point (solver.py:633-638)
+        J_dd_inv = dyn_jdd ? -1.0f / jdd : 0.f;
+      } else if (bad) {
+        status |= MF_NONFINITE_BIT;
       }
-      reduce<1>(part, false);
-      float rz = part[0] + (dyn ? r_d * z_d : 0.f);
-      for (int k = 0; k < n_cg; ++k) {
-        const float pAp = neg_jvp(pv, p_d, zv, &Ap_d);
-        const float alpha = rz / (pAp + 1e-30f);
-        own_nodes([&](int i, int, int, bool) {
-          dxv[i] = fmaf(alpha, pv[i], dxv[i]);
-          rv[i] = rv[i] - alpha * zv[i];
-        });
-        dx_d = fmaf(alpha, p_d, dx_d);
-        r_d = r_d - alpha * Ap_d;
+      it = nw;
+      if (!(fmx > tol && nw < n_newton)) break;
+      float r_d = frad, z_d = 0.f, p_d = 0.f, dx_d = 0.f, Ap_d = 0.f, rz = 0.f;
+      for (int k = -1; k < n_cg; ++k) {
+        if (k >= 0) {
+          const float pAp = neg_jvp(pv, p_d, zv, &Ap_d);
+          const float alpha = rz / (pAp + 1e-30f);
+          own_nodes([&](int i, int, int, bool) {
+            dxv[i] = fmaf(alpha, pv[i], dxv[i]);
+            rv[i] = rv[i] - alpha * zv[i];
+          });
+          dx_d = fmaf(alpha, p_d, dx_d);
+          r_d = r_d - alpha * Ap_d;
+          if (k + 1 == n_cg) break;  // the last direction update is never used
+        }
         precondition_own(rv, zv);
         float rzp[1] = {0.f};
         own_nodes([&](int i, int, int, bool) { rzp[0] = fmaf(rv[i], zv[i], rzp[0]); });
         if (dyn) z_d = J_dd_inv * r_d;
         reduce<1>(rzp, false);
         const float rz_new = rzp[0] + (dyn ? r_d * z_d : 0.f);
-        const float beta = rz_new / (rz + 1e-30f);
-        own_nodes([&](int i, int, int, bool) { pv[i] = fmaf(beta, pv[i], zv[i]); });
-        p_d = fmaf(beta, p_d, z_d);
+        if (k < 0) {
+          own_nodes([&](int i, int, int, bool) {
+            pv[i] = zv[i];
+            dxv[i] = n_cg == 0 ? zv[i] : 0.f;
+          });
+          p_d = z_d;
+          if (n_cg == 0) dx_d = z_d;
+        } else {
+          const float beta = rz_new / (rz + 1e-30f);
+          own_nodes([&](int i, int, int, bool) { pv[i] = fmaf(beta, pv[i], zv[i]); });
+          p_d = fmaf(beta, p_d, z_d);
+        }
         rz = rz_new;
       }
       // x += dx with non-finite entries zeroed
-      int bad_local = 0;
+      bad_local = 0;
       own_nodes([&](int i, int, int, bool) {
         float v = dxv[i];
         if (!isfinite(v)) { v = 0.f; bad_local = 1; }
@@ -943,9 +954,6 @@ struct Sim {
         if (!isfinite(v)) v = 0.f;
         d = fmaxf(d + v, 1.0f);
       }
-      fmx = residual(zl, d, &frad, nullptr, bad_local, &bad);
-      if (bad) status |= MF_NONFINITE_BIT;
-      ++it;
     }
     resid = fmx;
     iters = it;
@@ -1041,62 +1049,66 @@ struct Sim {
   // (p_k, A p_k) = (u_k, A u_k) - beta_k^2 (p_{k-1}, A p_{k-1}).
   __device__ __forceinline__ void solve_cg_gear(float zl, float& d, double& resid, int& iters, bool dyn_jdd) {
     const float tol = fmaxf(s.P[SOLVER_TOL], fmaxf(s.P[THICK_K] * 1e-4f, 0.25f));
-    float frad = 0.f, jdd = 0.f;
-    MF_SUB(-1);
-    float fmx = residual(zl, d, &frad, &jdd, 0, nullptr);
-    MF_SUB(0);
-    const float J_dd_inv = dyn_jdd ? -1.0f / jdd : 0.f;
     const int n_cg = A.n_cg, n_newton = A.n_newton;
-    int it = 0, bad = 0;
-    while (fmx > tol && it < n_newton) {
-      int bad_local = 0;
-      float r_d = frad, u_d = 0.f, w_d = 0.f, p_d = 0.f, s_d = 0.f, dx_d = 0.f;
-      // u = M^-1 r, w = A u, gamma = (r, u), delta = (u, w)
+    float frad = 0.f, jdd = 0.f, J_dd_inv = 0.f, fmx = 0.f;
+    int it = 0, bad = 0, bad_local = 0;
+    for (int nw = 0;; ++nw) {
       MF_SUB(-1);
-      float gpart = cg_pass(0.f, 0.f, false, false, false, bad_local);
-      MF_SUB(1);
-      if (dyn) u_d = J_dd_inv * r_d;
-      float gamma;
-      float delta = neg_jvp(s.zz, u_d, s.wv, &w_d, gpart, &gamma);
-      MF_SUB(2);
-      if (dyn) gamma += r_d * u_d;
-      float alpha = 0.f, gamma_old = 1.f;
-      for (int k = 0; k < n_cg; ++k) {
+      fmx = residual(zl, d, &frad, nw == 0 ? &jdd : nullptr, bad_local, nw == 0 ? nullptr : &bad);
+      MF_SUB(0);
+      if (nw == 0) J_dd_inv = dyn_jdd ? -1.0f / jdd : 0.f;
+      else if (bad) status |= MF_NONFINITE_BIT;
+      it = nw;
+      if (!(fmx > tol && nw < n_newton)) break;
+      bad_local = 0;
+      float r_d = frad, u_d = 0.f, w_d = 0.f, p_d = 0.f, s_d = 0.f, dx_d = 0.f;
+      float alpha = 0.f, gamma = 0.f, gamma_old = 1.f, delta = 0.f;
+      for (int k = -1; k < n_cg; ++k) {
         const bool first = k == 0, last = k + 1 == n_cg;
         float beta = 0.f;
         if (first) {
           alpha = gamma / (delta + 1e-30f);
-        } else {
+        } else if (k > 0) {
           beta = gamma / (gamma_old + 1e-30f);
           alpha = gamma / (delta - beta * gamma / alpha + 1e-30f);
         }
+        // k = -1: u = M^-1 r;  k >= 0: the recurrences, then u = M^-1 r
         MF_SUB(-1);
-        gpart = cg_pass(alpha, beta, true, first, last, bad_local);
+        const float gpart = cg_pass(alpha, beta, k >= 0, first, last && k >= 0, bad_local);
         MF_SUB(1);
-        p_d = first ? u_d : fmaf(beta, p_d, u_d);
-        s_d = first ? w_d : fmaf(beta, s_d, w_d);
-        dx_d = first ? alpha * p_d : fmaf(alpha, p_d, dx_d);
-        r_d = r_d - alpha * s_d;
-        if (last) break;
+        if (k >= 0) {
+          p_d = first ? u_d : fmaf(beta, p_d, u_d);
+          s_d = first ? w_d : fmaf(beta, s_d, w_d);
+          dx_d = first ? alpha * p_d : fmaf(alpha, p_d, dx_d);
+          r_d = r_d - alpha * s_d;
+          if (last) break;
+          gamma_old = gamma;
+        }
         if (dyn) u_d = J_dd_inv * r_d;
-        gamma_old = gamma;
+        if (n_cg == 0) break;
+        // w = A u, gamma = (r, u), delta = (u, w)
         MF_SUB(-1);
         delta = neg_jvp(s.zz, u_d, s.wv, &w_d, gpart, &gamma);
         MF_SUB(2);
         if (dyn) gamma += r_d * u_d;
-        if (tid == 0) MF_COUNT(3);
+      }
+      if (n_cg == 0) {  // the preconditioned residual is the step
+        float* __restrict__ xv = s.x;
+        const float* __restrict__ uv = s.zz;
+        __syncwarp();
+        own_nodes([&](int i, int, int, bool) {
+          float v = uv[i];
+          if (!isfinite(v)) { v = 0.f; bad_local = 1; }
+          xv[i] = xv[i] + v;
+        });
+        dx_d = u_d;
       }
       if (dyn) {
         float v = dx_d;
         if (!isfinite(v)) v = 0.f;
         d = fmaxf(d + v, 1.0f);
       }
-      MF_SUB(-1);
-      fmx = residual(zl, d, &frad, nullptr, bad_local, &bad);
-      MF_SUB(0);
       if (tid == 0) MF_COUNT(4);
-      if (bad) status |= MF_NONFINITE_BIT;
-      ++it;
     }
     resid = fmx;
     iters = it;
@@ -1408,59 +1420,57 @@ struct Sim {
 #pragma unroll
     for (int k = 0; k < RF; ++k)
 #pragma unroll
-      for (int e = 0; e < RE; ++e) p[k][e] = sv[k][e] = u[k][e] = w[k][e] = dx[k][e] = 0.f;
-    float frad = 0.f, jdd = 0.f;
-    float fmx = residual_regs(zl, d, &frad, &jdd, 0, nullptr, r);
-    MF_SUB(0);
-    const float J_dd_inv = dyn_jdd ? -1.0f / jdd : 0.f;
+      for (int e = 0; e < RE; ++e) r[k][e] = p[k][e] = sv[k][e] = u[k][e] = w[k][e] = dx[k][e] = 0.f;
     const int n_cg = A.n_cg, n_newton = A.n_newton;
-    int it = 0, bad = 0;
-    while (fmx > tol && it < n_newton) {
-      float r_d = frad, u_d = 0.f, w_d = 0.f, p_d = 0.f, s_d = 0.f, dx_d = 0.f;
+    float frad = 0.f, jdd = 0.f, J_dd_inv = 0.f, fmx = 0.f;
+    int it = 0, bad = 0, bad_local = 0;
+    for (int nw = 0;; ++nw) {
       MF_SUB(-1);
-      float gpart = precond_regs(r, u);
-      MF_SUB(1);
-      if (dyn) u_d = J_dd_inv * r_d;
-      float gamma;
-      float delta = jvp_regs(u, u_d, w, &w_d, gpart, &gamma);
-      MF_SUB(2);
-      if (dyn) gamma += r_d * u_d;
-      float alpha = 0.f, gamma_old = 1.f;
-      for (int kk = 0; kk < n_cg; ++kk) {
-        const bool first = kk == 0;
-        float beta = 0.f;
-        if (first) {
-          alpha = gamma / (delta + 1e-30f);
-        } else {
-          beta = gamma / (gamma_old + 1e-30f);
-          alpha = gamma / (delta - beta * gamma / alpha + 1e-30f);
-        }
-#pragma unroll
-        for (int k = 0; k < RF; ++k)
-#pragma unroll
-          for (int e = 0; e < RE; ++e) {
-            p[k][e] = first ? u[k][e] : fmaf(beta, p[k][e], u[k][e]);
-            sv[k][e] = first ? w[k][e] : fmaf(beta, sv[k][e], w[k][e]);
-            dx[k][e] = first ? alpha * p[k][e] : fmaf(alpha, p[k][e], dx[k][e]);
-            r[k][e] = r[k][e] - alpha * sv[k][e];
+      fmx = residual_regs(zl, d, &frad, nw == 0 ? &jdd : nullptr, bad_local, nw == 0 ? nullptr : &bad, r);
+      MF_SUB(0);
+      if (nw == 0) J_dd_inv = dyn_jdd ? -1.0f / jdd : 0.f;
+      else if (bad) status |= MF_NONFINITE_BIT;
+      it = nw;
+      if (!(fmx > tol && nw < n_newton)) break;
+      float r_d = frad, u_d = 0.f, w_d = 0.f, p_d = 0.f, s_d = 0.f, dx_d = 0.f;
+      float alpha = 0.f, gamma = 0.f, gamma_old = 1.f, delta = 0.f;
+      for (int kk = -1; kk < n_cg; ++kk) {
+        if (kk >= 0) {
+          const bool first = kk == 0;
+          float beta = 0.f;
+          if (first) {
+            alpha = gamma / (delta + 1e-30f);
+          } else {
+            beta = gamma / (gamma_old + 1e-30f);
+            alpha = gamma / (delta - beta * gamma / alpha + 1e-30f);
           }
-        p_d = first ? u_d : fmaf(beta, p_d, u_d);
-        s_d = first ? w_d : fmaf(beta, s_d, w_d);
-        dx_d = first ? alpha * p_d : fmaf(alpha, p_d, dx_d);
-        r_d = r_d - alpha * s_d;
-        if (kk + 1 == n_cg) break;
+#pragma unroll
+          for (int k = 0; k < RF; ++k)
+#pragma unroll
+            for (int e = 0; e < RE; ++e) {
+              p[k][e] = first ? u[k][e] : fmaf(beta, p[k][e], u[k][e]);
+              sv[k][e] = first ? w[k][e] : fmaf(beta, sv[k][e], w[k][e]);
+              dx[k][e] = first ? alpha * p[k][e] : fmaf(alpha, p[k][e], dx[k][e]);
+              r[k][e] = r[k][e] - alpha * sv[k][e];
+            }
+          p_d = first ? u_d : fmaf(beta, p_d, u_d);
+          s_d = first ? w_d : fmaf(beta, s_d, w_d);
+          dx_d = first ? alpha * p_d : fmaf(alpha, p_d, dx_d);
+          r_d = r_d - alpha * s_d;
+          if (kk + 1 == n_cg) break;
+          gamma_old = gamma;
+        }
         MF_SUB(-1);
-        gpart = precond_regs(r, u);
+        const float gpart = precond_regs(r, u);
         MF_SUB(1);
         if (dyn) u_d = J_dd_inv * r_d;
-        gamma_old = gamma;
         delta = jvp_regs(u, u_d, w, &w_d, gpart, &gamma);
         MF_SUB(2);
         if (tid == 0) MF_COUNT(3);
         if (dyn) gamma += r_d * u_d;
       }
       // x += dx with non-finite entries zeroed
-      int bad_local = 0;
+      bad_local = 0;
 #pragma unroll
       for (int k = 0; k < RF; ++k) {
         int base, n, f;
@@ -1482,12 +1492,7 @@ struct Sim {
         if (!isfinite(v)) v = 0.f;
         d = fmaxf(d + v, 1.0f);
       }
-      MF_SUB(-1);
-      fmx = residual_regs(zl, d, &frad, nullptr, bad_local, &bad, r);
-      MF_SUB(0);
       if (tid == 0) MF_COUNT(4);
-      if (bad) status |= MF_NONFINITE_BIT;
-      ++it;
     }
     resid = fmx;
     iters = it;
@@ -1661,33 +1666,60 @@ struct Sim {
     int* win1 = reinterpret_cast<int*>(s.site);
     for (int g = tid; g < S; g += NT) { win1[g] = -1; s.win2[g] = -1; }
     __syncthreads();
-    // sample, decide binding, and bid for the two scatter targets
-    for (int i = tid; i < X; i += NT) {
-      const int thin = thin_of(i);
-      const int near = s.xb_near[i];
-      const int site = near < 0 ? 0 : (near > T.n_sites - 1 ? T.n_sites - 1 : near);
-      const int tgt = thin * T.n_sites + site;
-      const bool perm = (s.tm[tgt] == 3) && T.xb_valid[i];
-      const int key = (perm ? T.n_bins : 0) + bin_of(s.xb_ax[i]);
-      s.xb_key[i] = (int16_t)key;
-      const int old = s.xb_state[i];
-      const float* c = cum_xb + key * 36 + old * 6;
-      const float u = uniform_of(sub, X, i, A.u_xb, inj_off);
-      int ns = 0;
+    // sample, decide binding, and bid for the two scatter targets.  Heads are
+    // taken HB at a time: the table rows (global memory, usually not in L1)
+    // of all HB heads are requested before any of them is used, and the
+    // Threefry draws run while those loads are in flight.
+    constexpr int HB = 3;
+    const int nsi = T.n_sites, nbins = T.n_bins;
+    for (int i0 = tid; i0 < X; i0 += HB * NT) {
+      float cum[HB][6];
+      int tgt_h[HB], thin_h[HB], old_h[HB];
+      bool perm_h[HB];
 #pragma unroll
-      for (int k = 5; k >= 0; --k)
-        if (u < __ldg(c + k)) ns = k;
-      const bool ob = old >= 1 && old <= 3, nbd = ns >= 1 && ns <= 3;
-      const bool binding = !ob && nbd, unbinding = ob && !nbd;
-      const bool occupied = s.thin_bound[tgt] >= 0;
-      const bool can_bind = binding && perm && !occupied;
-      const int ob_site = s.xb_bound[i];
-      const int t1 = thin * T.n_sites + (ob_site < 0 ? 0 : (ob_site > T.n_sites - 1 ? T.n_sites - 1 : ob_site));
-      atomicMax(&win1[t1], i);
-      atomicMax(&s.win2[tgt], i);
-      // stash the decision in fxb (as int bits): new state | can_bind<<4 | binding<<5 | unbinding<<6
-      int code = ns | (can_bind << 4) | (binding << 5) | (unbinding << 6);
-      reinterpret_cast<int*>(s.fxb)[i] = code;
+      for (int h = 0; h < HB; ++h) {
+        const int i = i0 + h * NT;
+        if (i < X) {
+          const int thin = thin_of(i);
+          const int near = s.xb_near[i];
+          const int site = near < 0 ? 0 : (near > nsi - 1 ? nsi - 1 : near);
+          const int tgt = thin * nsi + site;
+          const bool perm = (s.tm[tgt] == 3) && T.xb_valid[i];
+          const int key = (perm ? nbins : 0) + bin_of(s.xb_ax[i]);
+          s.xb_key[i] = (int16_t)key;
+          const int old = s.xb_state[i];
+          const float* c = cum_xb + key * 36 + old * 6;
+#pragma unroll
+          for (int k = 0; k < 6; ++k) cum[h][k] = __ldg(c + k);
+          tgt_h[h] = tgt;
+          thin_h[h] = thin;
+          old_h[h] = old;
+          perm_h[h] = perm;
+        }
+      }
+#pragma unroll
+      for (int h = 0; h < HB; ++h) {
+        const int i = i0 + h * NT;
+        if (i < X) {
+          const float u = uniform_of(sub, X, i, A.u_xb, inj_off);
+          int ns = 0;
+#pragma unroll
+          for (int k = 5; k >= 0; --k)
+            if (u < cum[h][k]) ns = k;
+          const int old = old_h[h], tgt = tgt_h[h];
+          const bool ob = old >= 1 && old <= 3, nbd = ns >= 1 && ns <= 3;
+          const bool binding = !ob && nbd, unbinding = ob && !nbd;
+          const bool occupied = s.thin_bound[tgt] >= 0;
+          const bool can_bind = binding && perm_h[h] && !occupied;
+          const int ob_site = s.xb_bound[i];
+          const int t1 = thin_h[h] * nsi + (ob_site < 0 ? 0 : (ob_site > nsi - 1 ? nsi - 1 : ob_site));
+          atomicMax(&win1[t1], i);
+          atomicMax(&s.win2[tgt], i);
+          // stash the decision in fxb (as int bits): new state | can_bind<<4 | binding<<5 | unbinding<<6
+          int code = ns | (can_bind << 4) | (binding << 5) | (unbinding << 6);
+          reinterpret_cast<int*>(s.fxb)[i] = code;
+        }
+      }
     }
     __syncthreads();
     // STEP 1: the highest-index writer of each site decides whether it is cleared
