@@ -6,7 +6,7 @@ how many conditions share an SM (fewer threads: more resident CTAs, cheaper
 barriers).  The best point depends on the lattice (nodes, heads) and on how
 many conditions are in flight, so it is measured: a short run of the actual
 kernel on a synthetic batch of that lattice for every candidate size, the
-fastest kept for the lattice through ``mf_tune_threads``.
+fastest kept for the lattice and precision mode through ``mf_tune_threads_mode``.
 """
 from __future__ import annotations
 
@@ -17,7 +17,7 @@ import numpy as np
 
 from .engine import MF_FLAG_PRECISE, get_engine
 
-CANDIDATES = (128, 256, 512, 1024)
+CANDIDATES = (128, 256, 384, 512, 1024)
 _CACHE: Dict[Tuple, int] = {}
 
 
@@ -29,7 +29,7 @@ def autotune(topology, n_conditions: int = 256, steps: int = 20, precision: str 
     key = (topology.size_key(), int(n_conditions), precision)
     eng = get_engine(device)
     if key in _CACHE:
-        eng.tune_threads(topology, _CACHE[key])
+        eng.tune_threads(topology, _CACHE[key], precision)
         return _CACHE[key]
     dev = torch.device('cuda', eng.device)
     B, T = int(n_conditions), int(steps)
@@ -45,7 +45,7 @@ def autotune(topology, n_conditions: int = 256, steps: int = 20, precision: str 
     best, best_t = None, float('inf')
     for nt in candidates:
         try:
-            eng.tune_threads(topology, nt)
+            eng.tune_threads(topology, nt, precision)
         except Exception:
             continue  # does not fit in shared memory at this size
         eng.run_batch(topology, P, Z, PC, L, NS, K, flags=flags)
@@ -60,7 +60,7 @@ def autotune(topology, n_conditions: int = 256, steps: int = 20, precision: str 
             best, best_t = nt, dt
     if best is None:
         raise RuntimeError("no CTA size fits this lattice")
-    eng.tune_threads(topology, best)
+    eng.tune_threads(topology, best, precision)
     _CACHE[key] = best
     return best
 

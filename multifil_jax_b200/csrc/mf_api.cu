@@ -20,13 +20,18 @@ using namespace mf;
 
 namespace {
 
+// CTA configuration of a lattice in one precision mode.
+struct Cfg {
+  int threads = 0;          // CTA size
+  bool vec_global = false;  // CG vectors and head terms in the workspace
+  size_t smem_local = 0;    // dynamic shared memory at that size
+};
+
 struct TopoHost {
   TopoDev dev{};          // host copy with device pointers
   TopoDev* d_struct = nullptr;
   std::vector<void*> allocs;
-  size_t smem_local = 0;  // bytes with CG vectors in smem (at chosen NT)
-  int threads = 0;        // chosen CTA size
-  bool vec_global = false;
+  Cfg cfg[2];             // [0] float32 mode, [1] precise (mixed) mode
 };
 
 struct Request;
@@ -93,8 +98,12 @@ static cudaError_t launch(int nt, const StepArgs& a, int grid, int base, size_t 
   return cudaErrorInvalidValue;
 }
 
-static int default_threads(const TopoDev& t) {
-  if (t.n_dof <= 1200) return 256;
+// Default CTA size: up to 1200 nodes, 384 threads in float32 mode (one warp
+// per filament of a 2x2 lattice for the reference-order scans) and 256 in
+// precise mode (register-resident CG, two filaments per warp); 512 up to 4000
+// nodes, else 1024.  The autotuner measures and overrides.
+static int default_threads(const TopoDev& t, bool precise) {
+  if (t.n_dof <= 1200) return precise ? 256 : 384;
   if (t.n_dof <= 4000) return 512;
   return 1024;
 }
@@ -232,20 +241,23 @@ int mf_upload_topology(mf_ctx* ctx, const mf_topo_desc* d, int32_t* topo_id) {
   }
   CK(cudaMalloc(&t->d_struct, sizeof(TopoDev)));
   CK(cudaMemcpy(t->d_struct, &td, sizeof(TopoDev), cudaMemcpyHostToDevice));
-  t->threads = default_threads(td);
-  size_t sm = smem_bytes(td, t->threads, false);
-  t->vec_global = sm + kStaticSmem > (size_t)ctx->smem_optin;
-  t->smem_local = smem_bytes(td, t->threads, t->vec_global);
-  if (t->smem_local + kStaticSmem > (size_t)ctx->smem_optin)
-    return fail(ctx, MF_ERR_INVALID, "lattice needs %zu B shared memory (limit %d)", t->smem_local,
-                ctx->smem_optin);
+  for (int p = 0; p < 2; ++p) {
+    Cfg& c = t->cfg[p];
+    c.threads = default_threads(td, p != 0);
+    size_t sm = smem_bytes(td, c.threads, false);
+    c.vec_global = sm + kStaticSmem > (size_t)ctx->smem_optin;
+    c.smem_local = smem_bytes(td, c.threads, c.vec_global);
+    if (c.smem_local + kStaticSmem > (size_t)ctx->smem_optin)
+      return fail(ctx, MF_ERR_INVALID, "lattice needs %zu B shared memory (limit %d)", c.smem_local,
+                  ctx->smem_optin);
+  }
   ctx->topos.push_back(std::move(t));
   *topo_id = (int32_t)ctx->topos.size() - 1;
   return MF_OK;
 }
 
-// Choose the CTA size of a lattice (autotuner hook).  threads in {128,256,512,1024}.
-int mf_tune_threads(mf_ctx* ctx, int32_t topo_id, int32_t threads) {
+// Choose the CTA size of a lattice (autotuner hook).
+int mf_tune_threads_mode(mf_ctx* ctx, int32_t topo_id, int32_t precise, int32_t threads) {
   if (!ctx || topo_id < 0 || topo_id >= (int)ctx->topos.size())
     return fail(ctx, MF_ERR_NOTFOUND, "unknown topology");
   if (threads != 128 && threads != 256 && threads != 384 && threads != 512 && threads != 1024)
@@ -255,10 +267,16 @@ int mf_tune_threads(mf_ctx* ctx, int32_t topo_id, int32_t threads) {
   bool vg = sm + kStaticSmem > (size_t)ctx->smem_optin;
   sm = smem_bytes(t.dev, threads, vg);
   if (sm + kStaticSmem > (size_t)ctx->smem_optin) return fail(ctx, MF_ERR_INVALID, "does not fit");
-  t.threads = threads;
-  t.vec_global = vg;
-  t.smem_local = sm;
+  Cfg& c = t.cfg[precise ? 1 : 0];
+  c.threads = threads;
+  c.vec_global = vg;
+  c.smem_local = sm;
   return MF_OK;
+}
+
+int mf_tune_threads(mf_ctx* ctx, int32_t topo_id, int32_t threads) {
+  int rc = mf_tune_threads_mode(ctx, topo_id, 0, threads);
+  return rc ? rc : mf_tune_threads_mode(ctx, topo_id, 1, threads);
 }
 
 static size_t slot_bytes(const TopoDev& t) {
@@ -364,9 +382,11 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
   // order: group by (threads, vec_global), longest work first inside a group
   std::vector<int> order(B);
   for (int i = 0; i < B; ++i) order[i] = i;
+  const int pm = (bt->flags & MF_FLAG_PRECISE) ? 1 : 0;
   auto key_of = [&](int i) {
     const TopoHost& t = *ctx->topos[bt->topo_id[i]];
-    return std::make_pair(t.threads * 2 + (t.vec_global ? 1 : 0), -(long)n_steps[i] * t.dev.n_dof);
+    const Cfg& c = t.cfg[pm];
+    return std::make_pair(c.threads * 2 + (c.vec_global ? 1 : 0), -(long)n_steps[i] * t.dev.n_dof);
   };
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key_of(a) < key_of(b); });
   off = 0;
@@ -403,12 +423,12 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
   struct Group { int begin, end, threads; bool vg; size_t smem; };
   std::vector<Group> groups;
   for (int k = 0; k < B;) {
-    const TopoHost& t0 = *ctx->topos[bt->topo_id[order[k]]];
-    Group g{k, k, t0.threads, t0.vec_global, 0};
+    const Cfg& c0 = ctx->topos[bt->topo_id[order[k]]]->cfg[pm];
+    Group g{k, k, c0.threads, c0.vec_global, 0};
     while (g.end < B) {
-      const TopoHost& tk = *ctx->topos[bt->topo_id[order[g.end]]];
-      if (tk.threads != g.threads || tk.vec_global != g.vg) break;
-      g.smem = std::max(g.smem, tk.smem_local);
+      const Cfg& ck = ctx->topos[bt->topo_id[order[g.end]]]->cfg[pm];
+      if (ck.threads != g.threads || ck.vec_global != g.vg) break;
+      g.smem = std::max(g.smem, ck.smem_local);
       ++g.end;
     }
     groups.push_back(g);
@@ -585,9 +605,11 @@ int mf_run_batch_static(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
   // group by CTA configuration exactly as mf_run_batch does
   std::vector<int> order(B);
   for (int i = 0; i < B; ++i) order[i] = i;
+  const int pm = (bt->flags & MF_FLAG_PRECISE) ? 1 : 0;
   auto key_of = [&](int i) {
     const TopoHost& t = *ctx->topos[bt->topo_id[i]];
-    return std::make_pair(t.threads * 2 + (t.vec_global ? 1 : 0), -(long)n_steps[i] * t.dev.n_dof);
+    const Cfg& c = t.cfg[pm];
+    return std::make_pair(c.threads * 2 + (c.vec_global ? 1 : 0), -(long)n_steps[i] * t.dev.n_dof);
   };
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key_of(a) < key_of(b); });
   CondDesc* d_desc = reinterpret_cast<CondDesc*>(base);
@@ -629,17 +651,17 @@ int mf_run_batch_static(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
   if (bt->flags & MF_FLAG_PRECISE) flags |= FLAG_PRECISE;
   if (bt->flags & MF_FLAG_ORIGINAL_PRNG) flags |= FLAG_ORIG_PRNG;
   for (int k = 0; k < B;) {
-    const TopoHost& t0 = *ctx->topos[bt->topo_id[order[k]]];
+    const Cfg& c0 = ctx->topos[bt->topo_id[order[k]]]->cfg[pm];
     int e = k;
     size_t smem = 0;
     while (e < B) {
-      const TopoHost& tk = *ctx->topos[bt->topo_id[order[e]]];
-      if (tk.threads != t0.threads || tk.vec_global != t0.vec_global) break;
-      smem = std::max(smem, tk.smem_local);
+      const Cfg& ck = ctx->topos[bt->topo_id[order[e]]]->cfg[pm];
+      if (ck.threads != c0.threads || ck.vec_global != c0.vec_global) break;
+      smem = std::max(smem, ck.smem_local);
       ++e;
     }
-    StepArgs a = make_args(bt, d_desc, flags | (t0.vec_global ? 64 : 0), max_dof, max_x, max_s);
-    cudaError_t err = launch(t0.threads, a, e - k, k, smem, st);
+    StepArgs a = make_args(bt, d_desc, flags | (c0.vec_global ? 64 : 0), max_dof, max_x, max_s);
+    cudaError_t err = launch(c0.threads, a, e - k, k, smem, st);
     if (err != cudaSuccess) return fail(ctx, MF_ERR_CUDA, "static launch: %s", cudaGetErrorString(err));
     k = e;
   }

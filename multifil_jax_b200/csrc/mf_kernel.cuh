@@ -40,6 +40,7 @@ __host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, bool vec_
   add(X);                                  // xb_state
   add(2 * S);                              // tm tm_new
   add(sizeof(float) * 27 * 16);            // cum_tm
+  add(sizeof(float) * 6 * t.n_bins);       // pabs
   add(sizeof(float) * cl.total);           // coef
   add(sizeof(float) * nw * scan);          // scan
   add(sizeof(float) * kNParams);           // P
@@ -88,6 +89,7 @@ __device__ void carve(Sim<NT, PR>& m, char* base, bool vec_global) {
   int8_t* t2 = (int8_t*)take(2 * S);
   m.s.tm = t2; m.s.tm_new = t2 + S;
   m.s.cum_tm = (float*)take(sizeof(float) * 27 * 16);
+  m.s.pabs = (float*)take(sizeof(float) * 6 * t.n_bins);
   m.s.coef = (float*)take(sizeof(float) * m.cl.total);
   m.s.scan = (float*)take(sizeof(float) * NT / 32 * scan);
   m.s.P = (float*)take(sizeof(float) * kNParams);
@@ -128,7 +130,7 @@ __device__ void metrics(Sim<NT, PR>& m, int t, float zl, float pCa, float new_ls
   const TopoDev& T = m.T;
   const int X = T.total_xbs, S = T.n_sites_total, NTN = T.n_thick_nodes;
   const int tid = m.tid;
-  const float* pabs = reinterpret_cast<const float*>(m.ws + m.L.pabs);
+  const float* pabs = m.s.pabs;
   const float* old_x = m.s.old_thick;
   // per-thread partials: counts (exact in float), sums, extrema
   float c_xb[7] = {0, 0, 0, 0, 0, 0, 0};  // 6 states + bound
@@ -389,6 +391,7 @@ __device__ void run_condition(const StepArgs& A, int ci) {
   int8_t* tm_g = reinterpret_cast<int8_t*>(m.ws + m.L.tm);
   int16_t* tb_g = reinterpret_cast<int16_t*>(m.ws + m.L.thin_bound);
   float* cum_tm_g = reinterpret_cast<float*>(m.ws + m.L.cum_tm);
+  float* pabs_g = reinterpret_cast<float*>(m.ws + m.L.pabs);
   float* coef_g = reinterpret_cast<float*>(m.ws + m.L.coef);
 
   for (int i = m.tid; i < kNParams; i += NT) m.s.P[i] = cd.params[i];
@@ -448,6 +451,7 @@ __device__ void run_condition(const StepArgs& A, int ci) {
     }
     for (int i = m.tid; i < m.cl.total; i += NT) m.s.coef[i] = coef_g[i];
     for (int i = m.tid; i < 27 * 16; i += NT) m.s.cum_tm[i] = cum_tm_g[i];
+    for (int i = m.tid; i < 6 * T.n_bins; i += NT) m.s.pabs[i] = pabs_g[i];
     if (m.tid == 0) {
       const uint32_t* kk = reinterpret_cast<const uint32_t*>(misc + MS_KEY);
       key_s[0] = kk[0];
@@ -641,6 +645,7 @@ __device__ void run_condition(const StepArgs& A, int ci) {
     tb_g[g] = m.s.thin_bound[g];
   }
   for (int i = m.tid; i < 27 * 16; i += NT) cum_tm_g[i] = m.s.cum_tm[i];
+  for (int i = m.tid; i < 6 * T.n_bins; i += NT) pabs_g[i] = m.s.pabs[i];
   const int st_all = __syncthreads_or(m.status);
   if (m.tid == 0) {
     uint32_t* kk = reinterpret_cast<uint32_t*>(misc + MS_KEY);

@@ -102,6 +102,8 @@ struct Smem {
   int8_t* tm;
   int8_t* tm_new;
   float* cum_tm;  // [27*16]
+  float* pabs;    // [2*n_bins*3] absorbing-chain entries read by the metrics (kept
+                  // in the workspace between launches)
   float* coef;    // Thomas scan coefficients (thick fwd, thick back, thin fwd, thin back, inv)
   float* scan;    // per-warp scan scratch
   float* P;       // [44]
@@ -1504,7 +1506,7 @@ struct Sim {
   // ------------------------------------------------------------------
   __device__ void build_tables(float pCa, float d, bool sampling, bool absorbing) {
     build_tables_block(s.P, T.centers, T.n_bins, pCa, d, dtm, A.sq64_from, s.cum_tm,
-                       reinterpret_cast<float*>(ws + L.cum_xb), reinterpret_cast<float*>(ws + L.pabs), sampling,
+                       reinterpret_cast<float*>(ws + L.cum_xb), s.pabs, sampling,
                        absorbing, tid, NT);
   }
 
@@ -1666,60 +1668,37 @@ struct Sim {
     int* win1 = reinterpret_cast<int*>(s.site);
     for (int g = tid; g < S; g += NT) { win1[g] = -1; s.win2[g] = -1; }
     __syncthreads();
-    // sample, decide binding, and bid for the two scatter targets.  Heads are
-    // taken HB at a time: the table rows (global memory, usually not in L1)
-    // of all HB heads are requested before any of them is used, and the
-    // Threefry draws run while those loads are in flight.
-    constexpr int HB = 3;
+    // sample, decide binding, and bid for the two scatter targets
     const int nsi = T.n_sites, nbins = T.n_bins;
-    for (int i0 = tid; i0 < X; i0 += HB * NT) {
-      float cum[HB][6];
-      int tgt_h[HB], thin_h[HB], old_h[HB];
-      bool perm_h[HB];
+    for (int i = tid; i < X; i += NT) {
+      const int thin = thin_of(i);
+      const int near = s.xb_near[i];
+      const int site = near < 0 ? 0 : (near > nsi - 1 ? nsi - 1 : near);
+      const int tgt = thin * nsi + site;
+      const bool perm = (s.tm[tgt] == 3) && T.xb_valid[i];
+      const int key = (perm ? nbins : 0) + bin_of(s.xb_ax[i]);
+      s.xb_key[i] = (int16_t)key;
+      const int old = s.xb_state[i];
+      const float* c = cum_xb + key * 36 + old * 6;
+      float cum[6];
 #pragma unroll
-      for (int h = 0; h < HB; ++h) {
-        const int i = i0 + h * NT;
-        if (i < X) {
-          const int thin = thin_of(i);
-          const int near = s.xb_near[i];
-          const int site = near < 0 ? 0 : (near > nsi - 1 ? nsi - 1 : near);
-          const int tgt = thin * nsi + site;
-          const bool perm = (s.tm[tgt] == 3) && T.xb_valid[i];
-          const int key = (perm ? nbins : 0) + bin_of(s.xb_ax[i]);
-          s.xb_key[i] = (int16_t)key;
-          const int old = s.xb_state[i];
-          const float* c = cum_xb + key * 36 + old * 6;
+      for (int k = 0; k < 6; ++k) cum[k] = __ldg(c + k);  // requested before the draw is computed
+      const float u = uniform_of(sub, X, i, A.u_xb, inj_off);
+      int ns = 0;
 #pragma unroll
-          for (int k = 0; k < 6; ++k) cum[h][k] = __ldg(c + k);
-          tgt_h[h] = tgt;
-          thin_h[h] = thin;
-          old_h[h] = old;
-          perm_h[h] = perm;
-        }
-      }
-#pragma unroll
-      for (int h = 0; h < HB; ++h) {
-        const int i = i0 + h * NT;
-        if (i < X) {
-          const float u = uniform_of(sub, X, i, A.u_xb, inj_off);
-          int ns = 0;
-#pragma unroll
-          for (int k = 5; k >= 0; --k)
-            if (u < cum[h][k]) ns = k;
-          const int old = old_h[h], tgt = tgt_h[h];
-          const bool ob = old >= 1 && old <= 3, nbd = ns >= 1 && ns <= 3;
-          const bool binding = !ob && nbd, unbinding = ob && !nbd;
-          const bool occupied = s.thin_bound[tgt] >= 0;
-          const bool can_bind = binding && perm_h[h] && !occupied;
-          const int ob_site = s.xb_bound[i];
-          const int t1 = thin_h[h] * nsi + (ob_site < 0 ? 0 : (ob_site > nsi - 1 ? nsi - 1 : ob_site));
-          atomicMax(&win1[t1], i);
-          atomicMax(&s.win2[tgt], i);
-          // stash the decision in fxb (as int bits): new state | can_bind<<4 | binding<<5 | unbinding<<6
-          int code = ns | (can_bind << 4) | (binding << 5) | (unbinding << 6);
-          reinterpret_cast<int*>(s.fxb)[i] = code;
-        }
-      }
+      for (int k = 5; k >= 0; --k)
+        if (u < cum[k]) ns = k;
+      const bool ob = old >= 1 && old <= 3, nbd = ns >= 1 && ns <= 3;
+      const bool binding = !ob && nbd, unbinding = ob && !nbd;
+      const bool occupied = s.thin_bound[tgt] >= 0;
+      const bool can_bind = binding && perm && !occupied;
+      const int ob_site = s.xb_bound[i];
+      const int t1 = thin * nsi + (ob_site < 0 ? 0 : (ob_site > nsi - 1 ? nsi - 1 : ob_site));
+      atomicMax(&win1[t1], i);
+      atomicMax(&s.win2[tgt], i);
+      // stash the decision in fxb (as int bits): new state | can_bind<<4 | binding<<5 | unbinding<<6
+      int code = ns | (can_bind << 4) | (binding << 5) | (unbinding << 6);
+      reinterpret_cast<int*>(s.fxb)[i] = code;
     }
     __syncthreads();
     // STEP 1: the highest-index writer of each site decides whether it is cleared

@@ -85,6 +85,7 @@ _SIGNATURES = {
     'mf_upload_topology': (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(mf_topo_desc),
                                           ctypes.POINTER(ctypes.c_int32)]),
     'mf_tune_threads': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]),
+    'mf_tune_threads_mode': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
     'mf_run_batch': (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(mf_batch), ctypes.c_void_p]),
     'mf_run_batch_static': (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(mf_batch), ctypes.c_void_p]),
     'mf_workspace_bytes': (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(mf_batch),
@@ -229,9 +230,14 @@ class Engine:
         self._topos[key] = up
         return up
 
-    def tune_threads(self, topo, threads: int):
+    def tune_threads(self, topo, threads: int, precision: Optional[str] = None):
+        """Set the CTA size of a lattice for one precision mode, or both when None."""
         up = self.upload(topo)
-        self._check(self.lib.mf_tune_threads(self.h, up.topo_id, int(threads)), 'mf_tune_threads')
+        if precision is None:
+            self._check(self.lib.mf_tune_threads(self.h, up.topo_id, int(threads)), 'mf_tune_threads')
+        else:
+            self._check(self.lib.mf_tune_threads_mode(self.h, up.topo_id, int(precision == 'mixed'), int(threads)),
+                        'mf_tune_threads_mode')
 
     # ------------------------------------------------------------------
     def run_batch(self, topos, params, z, pCa, ls, n_steps, keys, K_lat=None, nu=None, dt=None,
