@@ -253,7 +253,8 @@ class Engine:
         B, T = z.shape
         if not isinstance(topos, (list, tuple)):
             topos = [topos] * B
-        ups = [self.upload(t) for t in topos]
+        by_obj = {}  # one lookup per distinct lattice object, not per condition
+        ups = [by_obj[id(t)] if id(t) in by_obj else by_obj.setdefault(id(t), self.upload(t)) for t in topos]
         tid = np.array([u.topo_id for u in ups], dtype=np.int32)
         max_dof = max(u.n_dof for u in ups)
         max_x = max(u.total_xbs for u in ups)

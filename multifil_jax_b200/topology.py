@@ -468,10 +468,15 @@ class SarcTopology:
         return idx, self.xb_to_thin_id[idx], self.xb_to_thin_face[idx]
 
     def size_key(self) -> tuple:
-        """Identity of the lattice for caching device copies."""
-        return (self.n_thick, self.n_crowns, self.n_thin, self.n_sites, self.total_xbs,
-                self.max_sites_per_face, self.nrows, self.ncols,
-                self.binding_offsets.tobytes(), self.xb_to_site_indices.tobytes())
+        """Identity of the lattice for caching device copies (computed once: the
+        lattice is immutable, and the key holds two array byte strings)."""
+        key = self.__dict__.get('_size_key')
+        if key is None:
+            key = (self.n_thick, self.n_crowns, self.n_thin, self.n_sites, self.total_xbs,
+                   self.max_sites_per_face, self.nrows, self.ncols,
+                   self.binding_offsets.tobytes(), self.xb_to_site_indices.tobytes())
+            self.__dict__['_size_key'] = key
+        return key
 
     def __repr__(self) -> str:
         return (f"SarcTopology(n_thick={self.n_thick}, n_crowns={self.n_crowns}, "
