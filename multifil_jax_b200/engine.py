@@ -329,13 +329,15 @@ def _flags_for(plan, precision: str) -> int:
 
 
 def execute_plan(topology, plan, static_params, precision: str = 'float32', device: Optional[int] = None,
-                 minibatch_size="auto", chunk_steps: int = 0, stream=None) -> np.ndarray:
-    """Run every condition of a BatchPlan on the GPU; returns host metrics [B, 52, T]."""
+                 minibatch_size="auto", chunk_steps: int = 0, stream=None, key_major: bool = False) -> np.ndarray:
+    """Run every condition of a BatchPlan on the GPU; returns host metrics [B, 52, T]
+    (``key_major``: [52, B, T], transposed on the device so that every metric is
+    one contiguous block on the host)."""
     torch = _torch()
     eng = get_engine(device)
     dev = torch.device('cuda', eng.device)
     B, T = plan.total, plan.n_steps
-    out = np.zeros((B, N_METRICS, T), dtype=np.float32)
+    out = np.zeros((N_METRICS, B, T) if key_major else (B, N_METRICS, T), dtype=np.float32)
     if B == 0 or T == 0:
         return out
     if minibatch_size in (None, "auto"):
@@ -358,5 +360,11 @@ def execute_plan(topology, plan, static_params, precision: str = 'float32', devi
                                 n_newton=static_params.n_newton_steps, n_cg=static_params.n_cg_steps,
                                 flags=flags, chunk_steps=chunk_steps,
                                 residual_warn=static_params.solver_residual_tol, stream=stream)
-            out[s:e] = res['metrics'].cpu().numpy()
+            if key_major:
+                km = res['metrics'].permute(1, 0, 2).contiguous().cpu().numpy()
+                if s == 0 and e == B:
+                    return km
+                out[:, s:e] = km
+            else:
+                out[s:e] = res['metrics'].cpu().numpy()
     return out

@@ -403,13 +403,15 @@ def plan_batch(topology: SarcTopology, duration_ms: float = 1000.0, dt: float = 
 
 
 def assemble_result(plan: BatchPlan, metrics: np.ndarray, static_params: StaticParams, rng_seed: int,
-                    verbose: bool = False) -> SimulationResult:
-    """[B, 52, T] metrics -> data-cube SimulationResult with the residual warning."""
+                    verbose: bool = False, key_major: bool = False) -> SimulationResult:
+    """[B, 52, T] metrics ([52, B, T] with ``key_major``) -> data-cube
+    SimulationResult with the residual warning.  Float metrics are views of
+    ``metrics`` (no copies); ``newton_iters`` is converted to int32."""
     shape = plan.grid_shape + (plan.replicates, plan.n_steps)
     md = MetricsDict()
     for k, name in enumerate(METRIC_KEYS):
-        v = metrics[:, k, :].reshape(shape)
-        md[name] = v.astype(np.int32) if name == 'newton_iters' else v.astype(np.float32)
+        v = (metrics[k] if key_major else metrics[:, k, :]).reshape(shape)
+        md[name] = v.astype(np.int32) if name == 'newton_iters' else np.asarray(v, dtype=np.float32)
     max_res = float(np.max(md['solver_residual'])) if md['solver_residual'].size else 0.0
     tol = static_params.solver_residual_tol
     if max_res > tol:
@@ -453,8 +455,8 @@ def run(topology: SarcTopology, duration_ms: float = 1000.0, dt: float = 1.0,
         print(f"Grid shape: {plan.grid_shape}, axes: {plan.axis_names}, total: {plan.total}")
     from .engine import execute_plan
     metrics = execute_plan(topology, plan, sp, precision=precision, device=device,
-                           minibatch_size=minibatch_size, chunk_steps=chunk_steps)
-    return assemble_result(plan, metrics, sp, rng_seed, verbose)
+                           minibatch_size=minibatch_size, chunk_steps=chunk_steps, key_major=True)
+    return assemble_result(plan, metrics, sp, rng_seed, verbose, key_major=True)
 
 
 def run_conditions(conditions: List[dict], *, static_params: Optional[StaticParams] = None,
