@@ -30,6 +30,9 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
 B_SWEEP, T_SWEEP = 256, 500
+# DRAM bytes (read + write) of one launch of the mixed-precision sweep, from
+# ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum on this workload
+TRAFFIC_PER_LAUNCH = 3.40e6 + 39.57e6
 METRIC = 'condition-timesteps/s'
 
 
@@ -250,8 +253,11 @@ def bench_gpu(args):
     fp32_peak = fp32_peak_tflops(sm_mhz)
     achieved_tf = flops * (B * T) / (t_dev / args.steps / world * 1.0) / 1e12 if world == 1 else \
         flops * (B * T) / (t_dev / args.steps) / 1e12
-    peaks = json.load(open(os.path.join(REPO, 'MEASURED_PEAKS.json'))) if os.path.exists(
-        os.path.join(REPO, 'MEASURED_PEAKS.json')) else {'hbm_gbs': 6650.0}
+    peaks_path = os.path.join(REPO, 'MEASURED_PEAKS.json')
+    if os.path.exists(peaks_path):
+        peaks, peak_source = json.load(open(peaks_path)), 'measured (copy bandwidth of this pool)'
+    else:
+        peaks, peak_source = {'hbm_gbs': 6650.0}, 'fallback (earlier measurement on this pool)'
     hbm_bytes_step = B * T * (52 * 4 + 3 * 4)  # metrics written + drivers read (algorithmic)
     launch_s = t_dev / args.steps / world if world == 1 else t_dev / args.steps
     hbm_gbs = hbm_bytes_step / launch_s / 1e9
@@ -274,8 +280,13 @@ def bench_gpu(args):
         'e2e': {'value': e2e_value, 'unit': METRIC, 'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': int(d2h)},
         'gpu_launches': args.steps,
         'roofline': {'bound': 'hbm', 'achieved': hbm_gbs, 'peak': peaks['hbm_gbs'], 'unit': 'GB/s',
-                     'frac': hbm_gbs / peaks['hbm_gbs'], 'traffic': args.traffic,
-                     'note': 'state stays in shared memory; algorithmic HBM bytes = 220 B per condition-step'},
+                     'frac': hbm_gbs / peaks['hbm_gbs'], 'peak_source': peak_source,
+                     'traffic': args.traffic if args.traffic is not None else (
+                         TRAFFIC_PER_LAUNCH if (B, T, args.precision) == (256, 500, 'mixed') else None),
+                     'traffic_unit': 'bytes per launch',
+                     'note': 'state stays in shared memory; algorithmic HBM bytes = 220 B per condition-step '
+                             '(28.16 MB per launch); traffic = dram__bytes_read.sum + dram__bytes_write.sum of '
+                             'one full launch of this workload (ncu, one pass)'},
         'roofline_fp32': {'bound': 'fp32 cuda-core issue', 'achieved': achieved_tf, 'peak': fp32_peak,
                           'unit': 'TFLOP/s', 'frac': achieved_tf / fp32_peak,
                           'flops_per_condition_step': flops,
