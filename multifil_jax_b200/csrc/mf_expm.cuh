@@ -71,35 +71,52 @@ __device__ int expm_pade6(float* A, int sq64_from) {
   }
   mm<N>(A, T, U);
   // Solve (V - U) R = (V + U) by LU with partial pivoting (first maximum).
+  // Every index is a compile-time constant -- the row exchange is a select on
+  // each candidate row -- so the factors stay in registers.
   float L[N * N], R[N * N];
 #pragma unroll
   for (int i = 0; i < N * N; ++i) {
     L[i] = V[i] - U[i];
     R[i] = V[i] + U[i];
   }
+#pragma unroll
   for (int k = 0; k < N; ++k) {
     int piv = k;
     float best = fabsf(L[k * N + k]);
+#pragma unroll
     for (int i = k + 1; i < N; ++i) {
-      float v = fabsf(L[i * N + k]);
+      const float v = fabsf(L[i * N + k]);
       if (v > best) { best = v; piv = i; }
     }
-    if (piv != k) {
+#pragma unroll
+    for (int i = k + 1; i < N; ++i) {
+      const bool sw = piv == i;
+#pragma unroll
       for (int j = 0; j < N; ++j) {
-        float t = L[k * N + j]; L[k * N + j] = L[piv * N + j]; L[piv * N + j] = t;
-        t = R[k * N + j]; R[k * N + j] = R[piv * N + j]; R[piv * N + j] = t;
+        const float lk = L[k * N + j], li = L[i * N + j];
+        L[k * N + j] = sw ? li : lk;
+        L[i * N + j] = sw ? lk : li;
+        const float rk = R[k * N + j], ri = R[i * N + j];
+        R[k * N + j] = sw ? ri : rk;
+        R[i * N + j] = sw ? rk : ri;
       }
     }
     const float dkk = L[k * N + k];
+#pragma unroll
     for (int i = k + 1; i < N; ++i) {
       const float l = L[i * N + k] / dkk;
+#pragma unroll
       for (int j = k + 1; j < N; ++j) L[i * N + j] = L[i * N + j] - l * L[k * N + j];
+#pragma unroll
       for (int j = 0; j < N; ++j) R[i * N + j] = R[i * N + j] - l * R[k * N + j];
     }
   }
+#pragma unroll
   for (int i = N - 1; i >= 0; --i)
+#pragma unroll
     for (int j = 0; j < N; ++j) {
       float acc = R[i * N + j];
+#pragma unroll
       for (int m = i + 1; m < N; ++m) acc = acc - L[i * N + m] * A[m * N + j];
       A[i * N + j] = acc / L[i * N + i];
     }
