@@ -126,8 +126,9 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* batch, void* stream);
 /* CTA size of a lattice's conditions: 128, 256, 384, 512 or 1024 threads
  * (no counterpart in the reference, whose XLA compiler picks the launch
  * shapes).  mf_tune_threads_mode sets it for one precision mode (precise = 1:
- * MF_FLAG_PRECISE batches), mf_tune_threads for both.  Defaults: 384 (float32)
- * and 256 (precise) threads up to 1200 nodes, 512 up to 4000, else 1024;
+ * MF_FLAG_PRECISE batches), mf_tune_threads for both.  Defaults up to 1200
+ * nodes: 384 threads (precise mode: 256 when the lattice has more than 12
+ * filaments); 512 up to 4000 nodes, else 1024;
  * multifil_jax_b200.autotune measures and sets the best one.  MF_ERR_INVALID
  * when the lattice does not fit in shared memory at that size. */
 int mf_tune_threads_mode(mf_ctx* ctx, int32_t topo_id, int32_t precise, int32_t threads);

@@ -98,12 +98,13 @@ static cudaError_t launch(int nt, const StepArgs& a, int grid, int base, size_t 
   return cudaErrorInvalidValue;
 }
 
-// Default CTA size: up to 1200 nodes, 384 threads in float32 mode (one warp
-// per filament of a 2x2 lattice for the reference-order scans) and 256 in
-// precise mode (register-resident CG, two filaments per warp); 512 up to 4000
-// nodes, else 1024.  The autotuner measures and overrides.
+// Default CTA size.  Up to 1200 nodes: 384 threads (one warp per filament of
+// a 2x2 lattice) in float32 mode, and in precise mode whenever the lattice
+// has at most 12 filaments (the register-resident CG then holds one filament
+// per warp), else 256 (two per warp).  512 up to 4000 nodes, else 1024.  The
+// autotuner measures and overrides.
 static int default_threads(const TopoDev& t, bool precise) {
-  if (t.n_dof <= 1200) return precise ? 256 : 384;
+  if (t.n_dof <= 1200) return (!precise || t.n_thick + t.n_thin <= 12) ? 384 : 256;
   if (t.n_dof <= 4000) return 512;
   return 1024;
 }

@@ -1129,7 +1129,9 @@ struct Sim {
   // dependent index chains.  Same Chronopoulos-Gear recurrences as
   // solve_cg_gear.
   // ------------------------------------------------------------------
-  static constexpr int RE = 3, RF = 2;
+  // RF filaments per warp: one at 384 threads (a 2x2 lattice has 12 filaments
+  // for 12 warps), two otherwise
+  static constexpr int RE = 3, RF = NT == 384 ? 1 : 2;
   using RVec = float[RF][RE];
 
   __device__ __forceinline__ bool slot(int k, int& base, int& n, int& f, bool& thick) const {
