@@ -355,26 +355,68 @@ struct Sim {
   // ------------------------------------------------------------------
   // Thomas preconditioner: per-filament affine scans in JAX association order
   // ------------------------------------------------------------------
-  __device__ void scan_b(const ScanPlan& pl, const float* Acoef, float* buf) {
-    // buf[0..n) holds b of level 0; levels above are built in place.
-    for (int l = 0; l + 1 < pl.levels; ++l) {
-      const int nn = pl.len[l + 1];
-      const float* Al = Acoef + pl.off[l];
-      const float* El = buf + pl.off[l];
-      float* En = buf + pl.off[l + 1];
-      for (int k = lane; k < nn; k += 32) En[k] = fmaf(Al[2 * k + 1], El[2 * k], El[2 * k + 1]);
-      __syncwarp();
+  // The reference's lax.associative_scan dataflow (JAX's odd/even
+  // recursion) for the b-components of an affine-map scan whose a-components
+  // per tree node are precomputed (Acoef, ScanPlan level offsets), evaluated
+  // in registers for one filament of n <= 128 nodes.  Lane L holds level-0
+  // elements [4L, 4L+4) in e[], level-1 elements [2L, 2L+2), and for every
+  // level >= 2 element L.  Up-sweep: level l+1 element k = fmaf(A_l[2k+1],
+  // E_l[2k], E_l[2k+1]).  Down-sweep, from the scanned level l+1 S:
+  // E_l[2k+1] = S[k], E_l[2k] = fmaf(A_l[2k], S[k-1], E_l[2k]) for k >= 1.
+  // Level changes move data by warp shuffles.
+  __device__ __forceinline__ void scan_regs(const ScanPlan& pl, const float* __restrict__ Acoef,
+                                            float (&e)[4]) const {
+    constexpr int ML = 8;  // levels of a 128-element scan
+    int len[ML], off[ML];
+    const int levels = pl.levels;
+#pragma unroll
+    for (int l = 0; l < ML; ++l) {
+      len[l] = l < levels ? pl.len[l] : 0;
+      off[l] = l < levels ? pl.off[l] : 0;
     }
-    for (int l = pl.levels - 2; l >= 0; --l) {
-      const int nl = pl.len[l], nn = pl.len[l + 1];
-      const float* Al = Acoef + pl.off[l];
-      float* El = buf + pl.off[l];
-      const float* Sn = buf + pl.off[l + 1];
-      for (int k = lane; 2 * k < nl; k += 32) {
-        if (k >= 1) El[2 * k] = fmaf(Al[2 * k], Sn[k - 1], El[2 * k]);
-        if (k < nn) El[2 * k + 1] = Sn[k];
+    const int L = lane;
+    float l1[2];
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const int k = 2 * L + c;
+      l1[c] = k < len[1] ? fmaf(Acoef[off[0] + 2 * k + 1], e[2 * c], e[2 * c + 1]) : 0.f;
+    }
+    float v[ML];
+#pragma unroll
+    for (int l = 0; l < ML; ++l) v[l] = 0.f;
+    v[2] = L < len[2] ? fmaf(Acoef[off[1] + 2 * L + 1], l1[0], l1[1]) : 0.f;
+#pragma unroll
+    for (int l = 2; l + 1 < ML; ++l) {
+      const float a = __shfl_sync(0xffffffffu, v[l], (2 * L) & 31);
+      const float b = __shfl_sync(0xffffffffu, v[l], (2 * L + 1) & 31);
+      if (L < len[l + 1]) v[l + 1] = fmaf(Acoef[off[l] + 2 * L + 1], a, b);
+    }
+    // down-sweep from the top: level l from the scanned level l + 1
+#pragma unroll
+    for (int l = ML - 2; l >= 2; --l) {
+      const int src = (L & 1) ? (L - 1) >> 1 : (L >> 1) - 1;
+      const float sv = __shfl_sync(0xffffffffu, v[l + 1], src & 31);
+      if (l + 1 < levels && L < len[l]) {
+        if (L & 1) v[l] = sv;                                              // E[2k+1] = S[k]
+        else if (L >= 2) v[l] = fmaf(Acoef[off[l] + L], sv, v[l]);         // E[2k] += A[2k] S[k-1]
       }
-      __syncwarp();
+    }
+    {
+      const float sp = __shfl_up_sync(0xffffffffu, v[2], 1);
+      if (2 < levels) {
+        if (2 * L + 1 < len[1]) l1[1] = v[2];
+        if (2 * L < len[1] && L >= 1) l1[0] = fmaf(Acoef[off[1] + 2 * L], sp, l1[0]);
+      }
+    }
+    {
+      const float sp = __shfl_up_sync(0xffffffffu, l1[1], 1);
+      if (1 < levels) {
+        const int n0 = len[0];
+        if (4 * L < n0 && L >= 1) e[0] = fmaf(Acoef[off[0] + 4 * L], sp, e[0]);
+        if (4 * L + 1 < n0) e[1] = l1[0];
+        if (4 * L + 2 < n0) e[2] = fmaf(Acoef[off[0] + 4 * L + 2], l1[0], e[2]);
+        if (4 * L + 3 < n0) e[3] = l1[1];
+      }
     }
   }
 
@@ -498,21 +540,35 @@ struct Sim {
       const float* Af = s.coef + (thick ? cl.thick_fwd : cl.thin_fwd);
       const float* Ab = s.coef + (thick ? cl.thick_back : cl.thin_back);
       const float* inv = s.coef + (thick ? cl.thick_inv : cl.thin_inv);
-      for (int i = lane; i < n; i += 32) buf[i] = in[base + i];
+      // forward scan in registers, (y * inv) reversed through this warp's
+      // scratch, backward scan, reversed store
+      float e[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int i = 4 * lane + c;
+        e[c] = i < n ? in[base + i] : 0.f;
+      }
+      scan_regs(pl, Af, e);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int i = 4 * lane + c;
+        if (i < n) buf[n - 1 - i] = e[c] * inv[i];
+      }
       __syncwarp();
-      scan_b(pl, Af, buf);
-      // back substitution input: (y * inv) reversed
-      float tmp[4];
-      int cnt = 0;
-      for (int i = lane; i < n; i += 32) tmp[cnt++] = buf[i] * inv[i];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int i = 4 * lane + c;
+        e[c] = i < n ? buf[i] : 0.f;
+      }
       __syncwarp();
-      cnt = 0;
-      for (int i = lane; i < n; i += 32) buf[n - 1 - i] = tmp[cnt++];
-      __syncwarp();
-      scan_b(pl, Ab, buf);
-      for (int i = lane; i < n; i += 32) out[base + i] = buf[n - 1 - i];
-      __syncwarp();
+      scan_regs(pl, Ab, e);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int i = 4 * lane + c;
+        if (i < n) out[base + n - 1 - i] = e[c];
+      }
     }
+    __syncwarp();
   }
 
   // One-barrier block reduction of K floats (sum) with an optional max in
@@ -902,7 +958,9 @@ struct Sim {
     float frad = 0.f, jdd = 0.f, J_dd_inv = 0.f, fmx = 0.f;
     int it = 0, bad = 0, bad_local = 0;
     for (int nw = 0;; ++nw) {
+      MF_SUB(-1);
       fmx = residual(zl, d, &frad, nw == 0 ? &jdd : nullptr, bad_local, nw == 0 ? nullptr : &bad);
+      MF_SUB(0);
       if (nw == 0) {
         // exact radial diagonal at the pre-solve point (solver.py:633-638)
         J_dd_inv = dyn_jdd ? -1.0f / jdd : 0.f;
@@ -911,10 +969,14 @@ struct Sim {
       }
       it = nw;
       if (!(fmx > tol && nw < n_newton)) break;
+      if (tid == 0) MF_COUNT(4);
       float r_d = frad, z_d = 0.f, p_d = 0.f, dx_d = 0.f, Ap_d = 0.f, rz = 0.f;
       for (int k = -1; k < n_cg; ++k) {
         if (k >= 0) {
+          MF_SUB(-1);
           const float pAp = neg_jvp(pv, p_d, zv, &Ap_d);
+          MF_SUB(2);
+          if (tid == 0) MF_COUNT(3);
           const float alpha = rz / (pAp + 1e-30f);
           own_nodes([&](int i, int, int, bool) {
             dxv[i] = fmaf(alpha, pv[i], dxv[i]);
@@ -924,7 +986,9 @@ struct Sim {
           r_d = r_d - alpha * Ap_d;
           if (k + 1 == n_cg) break;  // the last direction update is never used
         }
+        MF_SUB(-1);
         precondition_own(rv, zv);
+        MF_SUB(1);
         float rzp[1] = {0.f};
         own_nodes([&](int i, int, int, bool) { rzp[0] = fmaf(rv[i], zv[i], rzp[0]); });
         if (dyn) z_d = J_dd_inv * r_d;
