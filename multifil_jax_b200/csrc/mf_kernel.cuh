@@ -381,18 +381,10 @@ __device__ void run_condition(const StepArgs& A, int ci) {
   }
   const int b = m.b;
   const int N = T.n_dof, X = T.total_xbs, S = T.n_sites_total, NTN = T.n_thick_nodes;
-  double* misc = reinterpret_cast<double*>(m.ws + m.L.misc);
-  float* xg = reinterpret_cast<float*>(m.ws + m.L.x);
-  int8_t* xbs_g = reinterpret_cast<int8_t*>(m.ws + m.L.xb_state);
-  int16_t* xbb_g = reinterpret_cast<int16_t*>(m.ws + m.L.xb_bound);
-  int16_t* xbn_g = reinterpret_cast<int16_t*>(m.ws + m.L.xb_near);
-  int16_t* xbk_g = reinterpret_cast<int16_t*>(m.ws + m.L.xb_key);
-  float* xba_g = reinterpret_cast<float*>(m.ws + m.L.xb_ax);
-  int8_t* tm_g = reinterpret_cast<int8_t*>(m.ws + m.L.tm);
-  int16_t* tb_g = reinterpret_cast<int16_t*>(m.ws + m.L.thin_bound);
-  float* cum_tm_g = reinterpret_cast<float*>(m.ws + m.L.cum_tm);
-  float* pabs_g = reinterpret_cast<float*>(m.ws + m.L.pabs);
-  float* coef_g = reinterpret_cast<float*>(m.ws + m.L.coef);
+  // Workspace arrays of this condition, formed where they are used (launch
+  // start and end) so that none of the pointers stays live across the step
+  // loop.
+#define MF_WS(type, field) reinterpret_cast<type*>(m.ws + m.L.field)
 
   for (int i = m.tid; i < kNParams; i += NT) m.s.P[i] = cd.params[i];
   m.Kl = cd.K_lat;
@@ -427,42 +419,42 @@ __device__ void run_condition(const StepArgs& A, int ci) {
       m.s.tm[g] = 0;
       m.s.thin_bound[g] = -1;
     }
-    m.build_precond_coef(coef_g);
+    m.build_precond_coef(MF_WS(float, coef));
     __syncthreads();
     __threadfence_block();
-    for (int i = m.tid; i < m.cl.total; i += NT) m.s.coef[i] = coef_g[i];
+    for (int i = m.tid; i < m.cl.total; i += NT) m.s.coef[i] = MF_WS(float, coef)[i];
     __syncthreads();
     // the initial equilibrium itself runs as step -1 of the loop below, so
     // that the nearest-site search and the solver have one call site each
   } else {
     // ---- resume a condition from its resident workspace ----
-    m.zref = misc[MS_ZREF];
-    for (int i = m.tid; i < N; i += NT) m.s.x[i] = xg[i];
+    m.zref = MF_WS(double, misc)[MS_ZREF];
+    for (int i = m.tid; i < N; i += NT) m.s.x[i] = MF_WS(float, x)[i];
     for (int i = m.tid; i < X; i += NT) {
-      m.s.xb_state[i] = xbs_g[i];
-      m.s.xb_bound[i] = xbb_g[i];
-      m.s.xb_near[i] = xbn_g[i];
-      m.s.xb_ax[i] = xba_g[i];
-      m.s.xb_key[i] = xbk_g[i];
+      m.s.xb_state[i] = MF_WS(int8_t, xb_state)[i];
+      m.s.xb_bound[i] = MF_WS(int16_t, xb_bound)[i];
+      m.s.xb_near[i] = MF_WS(int16_t, xb_near)[i];
+      m.s.xb_ax[i] = MF_WS(float, xb_ax)[i];
+      m.s.xb_key[i] = MF_WS(int16_t, xb_key)[i];
     }
     for (int g = m.tid; g < S; g += NT) {
-      m.s.tm[g] = tm_g[g];
-      m.s.thin_bound[g] = tb_g[g];
+      m.s.tm[g] = MF_WS(int8_t, tm)[g];
+      m.s.thin_bound[g] = MF_WS(int16_t, thin_bound)[g];
     }
-    for (int i = m.tid; i < m.cl.total; i += NT) m.s.coef[i] = coef_g[i];
-    for (int i = m.tid; i < 27 * 16; i += NT) m.s.cum_tm[i] = cum_tm_g[i];
-    for (int i = m.tid; i < 6 * T.n_bins; i += NT) m.s.pabs[i] = pabs_g[i];
+    for (int i = m.tid; i < m.cl.total; i += NT) m.s.coef[i] = MF_WS(float, coef)[i];
+    for (int i = m.tid; i < 27 * 16; i += NT) m.s.cum_tm[i] = MF_WS(float, cum_tm)[i];
+    for (int i = m.tid; i < 6 * T.n_bins; i += NT) m.s.pabs[i] = MF_WS(float, pabs)[i];
     if (m.tid == 0) {
-      const uint32_t* kk = reinterpret_cast<const uint32_t*>(misc + MS_KEY);
+      const uint32_t* kk = reinterpret_cast<const uint32_t*>(MF_WS(double, misc) + MS_KEY);
       key_s[0] = kk[0];
       key_s[1] = kk[1];
-      ls_s = (float)misc[MS_CUR_LS];
-      m.status = (int)misc[MS_STATUS];
-      tab_key[0] = misc[MS_TAB_PCA];
-      tab_key[1] = misc[MS_TAB_D];
-      tab_key[2] = misc[MS_ABS_PCA];
-      tab_key[3] = misc[MS_ABS_D];
-      tab_key[4] = misc[MS_L0];
+      ls_s = (float)MF_WS(double, misc)[MS_CUR_LS];
+      m.status = (int)MF_WS(double, misc)[MS_STATUS];
+      tab_key[0] = MF_WS(double, misc)[MS_TAB_PCA];
+      tab_key[1] = MF_WS(double, misc)[MS_TAB_D];
+      tab_key[2] = MF_WS(double, misc)[MS_ABS_PCA];
+      tab_key[3] = MF_WS(double, misc)[MS_ABS_D];
+      tab_key[4] = MF_WS(double, misc)[MS_L0];
     }
     __syncthreads();
   }
@@ -632,37 +624,38 @@ __device__ void run_condition(const StepArgs& A, int ci) {
   }
 #endif
   // ---- write back resident state ----
-  for (int i = m.tid; i < N; i += NT) xg[i] = m.s.x[i];
+  for (int i = m.tid; i < N; i += NT) MF_WS(float, x)[i] = m.s.x[i];
   for (int i = m.tid; i < X; i += NT) {
-    xbs_g[i] = m.s.xb_state[i];
-    xbb_g[i] = m.s.xb_bound[i];
-    xbn_g[i] = m.s.xb_near[i];
-    xba_g[i] = m.s.xb_ax[i];
-    xbk_g[i] = m.s.xb_key[i];
+    MF_WS(int8_t, xb_state)[i] = m.s.xb_state[i];
+    MF_WS(int16_t, xb_bound)[i] = m.s.xb_bound[i];
+    MF_WS(int16_t, xb_near)[i] = m.s.xb_near[i];
+    MF_WS(float, xb_ax)[i] = m.s.xb_ax[i];
+    MF_WS(int16_t, xb_key)[i] = m.s.xb_key[i];
   }
   for (int g = m.tid; g < S; g += NT) {
-    tm_g[g] = m.s.tm[g];
-    tb_g[g] = m.s.thin_bound[g];
+    MF_WS(int8_t, tm)[g] = m.s.tm[g];
+    MF_WS(int16_t, thin_bound)[g] = m.s.thin_bound[g];
   }
-  for (int i = m.tid; i < 27 * 16; i += NT) cum_tm_g[i] = m.s.cum_tm[i];
-  for (int i = m.tid; i < 6 * T.n_bins; i += NT) pabs_g[i] = m.s.pabs[i];
+  for (int i = m.tid; i < 27 * 16; i += NT) MF_WS(float, cum_tm)[i] = m.s.cum_tm[i];
+  for (int i = m.tid; i < 6 * T.n_bins; i += NT) MF_WS(float, pabs)[i] = m.s.pabs[i];
   const int st_all = __syncthreads_or(m.status);
   if (m.tid == 0) {
-    uint32_t* kk = reinterpret_cast<uint32_t*>(misc + MS_KEY);
+    uint32_t* kk = reinterpret_cast<uint32_t*>(MF_WS(double, misc) + MS_KEY);
     kk[0] = key_s[0];
     kk[1] = key_s[1];
-    misc[MS_CUR_LS] = ls_s;
-    misc[MS_ZREF] = m.zref;
-    misc[MS_STATUS] = (double)(m.status | st_all);
-    misc[MS_TAB_PCA] = tab_key[0];
-    misc[MS_TAB_D] = tab_key[1];
-    misc[MS_ABS_PCA] = tab_key[2];
-    misc[MS_ABS_D] = tab_key[3];
-    misc[MS_L0] = tab_key[4];
+    MF_WS(double, misc)[MS_CUR_LS] = ls_s;
+    MF_WS(double, misc)[MS_ZREF] = m.zref;
+    MF_WS(double, misc)[MS_STATUS] = (double)(m.status | st_all);
+    MF_WS(double, misc)[MS_TAB_PCA] = tab_key[0];
+    MF_WS(double, misc)[MS_TAB_D] = tab_key[1];
+    MF_WS(double, misc)[MS_ABS_PCA] = tab_key[2];
+    MF_WS(double, misc)[MS_ABS_D] = tab_key[3];
+    MF_WS(double, misc)[MS_L0] = tab_key[4];
     if (cd.status) *cd.status = m.status | st_all;
     if (cd.key_out) { cd.key_out[0] = key_s[0]; cd.key_out[1] = key_s[1]; }
   }
 }
+#undef MF_WS
 
 // Register cap of 128 per thread (80 at 384 threads, 64 at 1024) so that
 // several conditions share an SM; the table builder's 6x6 temporaries spill
