@@ -480,9 +480,10 @@ def study_uneven(args):
         torch.cuda.synchronize()
         return time.perf_counter() - t0
 
-    out['default_threads'] = 'library default: 256 threads up to 1200 nodes, 512 up to 4000, else 1024'
+    out['default_threads'] = ('library default with the spacing solved as an unknown: 512 threads up to '
+                              '4000 nodes, else 1024')
     t_def = timed()
-    tuned = autotune_many(list(topos.values()), precision=args.precision)
+    tuned = autotune_many(list(topos.values()), precision=args.precision, dynamic_ls=True)
     t_tuned = timed()
     out['tuned_threads'] = {f'{r}x{c}': v for (r, c), v in sorted(tuned.items())}
     out['default_value'] = total / t_def

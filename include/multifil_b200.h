@@ -128,7 +128,8 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* batch, void* stream);
  * shapes).  mf_tune_threads_mode sets it for one precision mode (precise = 1:
  * MF_FLAG_PRECISE batches), mf_tune_threads for both.  Defaults up to 1200
  * nodes: 384 threads (precise mode: 256 when the lattice has more than 12
- * filaments); 512 up to 4000 nodes, else 1024;
+ * filaments); 512 up to 4000 nodes, else 1024; batches with MF_FLAG_DYNAMIC_LS
+ * use at least 512 unless the size was set here;
  * multifil_jax_b200.autotune measures and sets the best one.  MF_ERR_INVALID
  * when the lattice does not fit in shared memory at that size. */
 int mf_tune_threads_mode(mf_ctx* ctx, int32_t topo_id, int32_t precise, int32_t threads);

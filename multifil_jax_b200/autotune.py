@@ -22,11 +22,16 @@ _CACHE: Dict[Tuple, int] = {}
 
 
 def autotune(topology, n_conditions: int = 256, steps: int = 20, precision: str = 'float32',
-             candidates: Iterable[int] = CANDIDATES, device: Optional[int] = None, verbose: bool = False) -> int:
-    """Measure every candidate CTA size on this lattice; keep and return the best."""
+             candidates: Iterable[int] = CANDIDATES, device: Optional[int] = None, verbose: bool = False,
+             dynamic_ls: bool = False) -> int:
+    """Measure every candidate CTA size on this lattice; keep and return the best.
+
+    ``dynamic_ls`` measures with the lattice spacing solved as an unknown
+    (K_lat 5, nu 0.5), where the per-step table rebuilds dominate.
+    """
     import torch
     from .params import get_skeletal_params
-    key = (topology.size_key(), int(n_conditions), precision)
+    key = (topology.size_key(), int(n_conditions), precision, bool(dynamic_ls))
     eng = get_engine(device)
     if key in _CACHE:
         eng.tune_threads(topology, _CACHE[key], precision)
@@ -42,16 +47,22 @@ def autotune(topology, n_conditions: int = 256, steps: int = 20, precision: str 
     NS = torch.full((B,), T, dtype=torch.int32, device=dev)
     K = torch.as_tensor(prng_split(prng_key(0), B).astype(np.int64), device=dev).to(torch.int32)
     flags = MF_FLAG_PRECISE if precision == 'mixed' else 0
+    kw = {}
+    if dynamic_ls:
+        from .engine import MF_FLAG_DYNAMIC_LS
+        flags |= MF_FLAG_DYNAMIC_LS
+        kw = dict(K_lat=torch.full((B,), 5.0 * topology.n_thick, device=dev),
+                  nu=torch.full((B,), 0.5, device=dev))
     best, best_t = None, float('inf')
     for nt in candidates:
         try:
             eng.tune_threads(topology, nt, precision)
         except Exception:
             continue  # does not fit in shared memory at this size
-        eng.run_batch(topology, P, Z, PC, L, NS, K, flags=flags)
+        eng.run_batch(topology, P, Z, PC, L, NS, K, flags=flags, **kw)
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
-        eng.run_batch(topology, P, Z, PC, L, NS, K, flags=flags)
+        eng.run_batch(topology, P, Z, PC, L, NS, K, flags=flags, **kw)
         torch.cuda.synchronize(dev)
         dt = time.perf_counter() - t0
         if verbose:

@@ -25,6 +25,7 @@ struct Cfg {
   int threads = 0;          // CTA size
   bool vec_global = false;  // CG vectors and head terms in the workspace
   size_t smem_local = 0;    // dynamic shared memory at that size
+  bool tuned = false;       // set through mf_tune_threads[_mode]
 };
 
 struct TopoHost {
@@ -107,6 +108,25 @@ static int default_threads(const TopoDev& t, bool precise) {
   if (t.n_dof <= 1200) return (!precise || t.n_thick + t.n_thin <= 12) ? 384 : 256;
   if (t.n_dof <= 4000) return 512;
   return 1024;
+}
+
+// The configuration a batch uses.  With the lattice spacing solved as an
+// unknown both transition tables (827 matrix exponentials) are rebuilt every
+// step, one matrix per thread: an untuned default below 512 threads is raised
+// to 512 (measured fastest for every lattice of 1x1 to 4x4 in that mode).
+static Cfg batch_cfg(const TopoHost& t, int pm, bool dyn, int smem_optin) {
+  Cfg c = t.cfg[pm];
+  if (dyn && !c.tuned && c.threads < 512) {
+    size_t sm = smem_bytes(t.dev, 512, false);
+    const bool vg = sm + kStaticSmem > (size_t)smem_optin;
+    const size_t need = smem_bytes(t.dev, 512, vg);
+    if (need + kStaticSmem <= (size_t)smem_optin) {
+      c.threads = 512;
+      c.vec_global = vg;
+      c.smem_local = need;
+    }
+  }
+  return c;
 }
 
 extern "C" {
@@ -272,6 +292,7 @@ int mf_tune_threads_mode(mf_ctx* ctx, int32_t topo_id, int32_t precise, int32_t 
   c.threads = threads;
   c.vec_global = vg;
   c.smem_local = sm;
+  c.tuned = true;
   return MF_OK;
 }
 
@@ -384,9 +405,10 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
   std::vector<int> order(B);
   for (int i = 0; i < B; ++i) order[i] = i;
   const int pm = (bt->flags & MF_FLAG_PRECISE) ? 1 : 0;
+  const bool dynb = (bt->flags & MF_FLAG_DYNAMIC_LS) != 0;
   auto key_of = [&](int i) {
     const TopoHost& t = *ctx->topos[bt->topo_id[i]];
-    const Cfg& c = t.cfg[pm];
+    const Cfg c = batch_cfg(t, pm, dynb, ctx->smem_optin);
     return std::make_pair(c.threads * 2 + (c.vec_global ? 1 : 0), -(long)n_steps[i] * t.dev.n_dof);
   };
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key_of(a) < key_of(b); });
@@ -424,10 +446,10 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
   struct Group { int begin, end, threads; bool vg; size_t smem; };
   std::vector<Group> groups;
   for (int k = 0; k < B;) {
-    const Cfg& c0 = ctx->topos[bt->topo_id[order[k]]]->cfg[pm];
+    const Cfg c0 = batch_cfg(*ctx->topos[bt->topo_id[order[k]]], pm, dynb, ctx->smem_optin);
     Group g{k, k, c0.threads, c0.vec_global, 0};
     while (g.end < B) {
-      const Cfg& ck = ctx->topos[bt->topo_id[order[g.end]]]->cfg[pm];
+      const Cfg ck = batch_cfg(*ctx->topos[bt->topo_id[order[g.end]]], pm, dynb, ctx->smem_optin);
       if (ck.threads != g.threads || ck.vec_global != g.vg) break;
       g.smem = std::max(g.smem, ck.smem_local);
       ++g.end;
@@ -607,9 +629,10 @@ int mf_run_batch_static(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
   std::vector<int> order(B);
   for (int i = 0; i < B; ++i) order[i] = i;
   const int pm = (bt->flags & MF_FLAG_PRECISE) ? 1 : 0;
+  const bool dynb = (bt->flags & MF_FLAG_DYNAMIC_LS) != 0;
   auto key_of = [&](int i) {
     const TopoHost& t = *ctx->topos[bt->topo_id[i]];
-    const Cfg& c = t.cfg[pm];
+    const Cfg c = batch_cfg(t, pm, dynb, ctx->smem_optin);
     return std::make_pair(c.threads * 2 + (c.vec_global ? 1 : 0), -(long)n_steps[i] * t.dev.n_dof);
   };
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key_of(a) < key_of(b); });
@@ -652,11 +675,11 @@ int mf_run_batch_static(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
   if (bt->flags & MF_FLAG_PRECISE) flags |= FLAG_PRECISE;
   if (bt->flags & MF_FLAG_ORIGINAL_PRNG) flags |= FLAG_ORIG_PRNG;
   for (int k = 0; k < B;) {
-    const Cfg& c0 = ctx->topos[bt->topo_id[order[k]]]->cfg[pm];
+    const Cfg c0 = batch_cfg(*ctx->topos[bt->topo_id[order[k]]], pm, dynb, ctx->smem_optin);
     int e = k;
     size_t smem = 0;
     while (e < B) {
-      const Cfg& ck = ctx->topos[bt->topo_id[order[e]]]->cfg[pm];
+      const Cfg ck = batch_cfg(*ctx->topos[bt->topo_id[order[e]]], pm, dynb, ctx->smem_optin);
       if (ck.threads != c0.threads || ck.vec_global != c0.vec_global) break;
       smem = std::max(smem, ck.smem_local);
       ++e;

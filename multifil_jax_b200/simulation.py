@@ -525,7 +525,7 @@ def run_conditions(conditions: List[dict], *, static_params: Optional[StaticPara
     topos = [c['topology'] for c in conditions]
     if autotune:
         from .autotune import autotune_many
-        autotune_many(topos, precision=precision, device=device)
+        autotune_many(topos, precision=precision, device=device, dynamic_ls=all(dyn))
     eng = get_engine(device)
     dev = torch.device('cuda', eng.device)
     flags = (MF_FLAG_DYNAMIC_LS if all(dyn) else 0) | (MF_FLAG_PRECISE if precision == 'mixed' else 0)
