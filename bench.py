@@ -439,7 +439,7 @@ def profile_case(args):
 
 
 # ---------------------------------------------------------------------------
-# workload studies (one JSON line each; not the driver's bench line)
+# workload studies (one JSON line each, separate from the benchmark line)
 # ---------------------------------------------------------------------------
 def uneven_conditions(n=512, seed=0):
     """512 conditions: lattices nrows, ncols ~ U{1..4}, z ~ U[850, 1000] nm,
