@@ -117,9 +117,9 @@ static int default_threads(const TopoDev& t, bool precise) {
 static Cfg batch_cfg(const TopoHost& t, int pm, bool dyn, int smem_optin) {
   Cfg c = t.cfg[pm];
   if (dyn && !c.tuned && c.threads < 512) {
-    size_t sm = smem_bytes(t.dev, 512, false);
+    size_t sm = smem_bytes(t.dev, 512, false, pm != 0);
     const bool vg = sm + kStaticSmem > (size_t)smem_optin;
-    const size_t need = smem_bytes(t.dev, 512, vg);
+    const size_t need = smem_bytes(t.dev, 512, vg, pm != 0);
     if (need + kStaticSmem <= (size_t)smem_optin) {
       c.threads = 512;
       c.vec_global = vg;
@@ -265,9 +265,9 @@ int mf_upload_topology(mf_ctx* ctx, const mf_topo_desc* d, int32_t* topo_id) {
   for (int p = 0; p < 2; ++p) {
     Cfg& c = t->cfg[p];
     c.threads = default_threads(td, p != 0);
-    size_t sm = smem_bytes(td, c.threads, false);
+    size_t sm = smem_bytes(td, c.threads, false, p != 0);
     c.vec_global = sm + kStaticSmem > (size_t)ctx->smem_optin;
-    c.smem_local = smem_bytes(td, c.threads, c.vec_global);
+    c.smem_local = smem_bytes(td, c.threads, c.vec_global, p != 0);
     if (c.smem_local + kStaticSmem > (size_t)ctx->smem_optin)
       return fail(ctx, MF_ERR_INVALID, "lattice needs %zu B shared memory (limit %d)", c.smem_local,
                   ctx->smem_optin);
@@ -284,9 +284,9 @@ int mf_tune_threads_mode(mf_ctx* ctx, int32_t topo_id, int32_t precise, int32_t 
   if (threads != 128 && threads != 256 && threads != 384 && threads != 512 && threads != 1024)
     return fail(ctx, MF_ERR_INVALID, "threads must be 128, 256, 384, 512 or 1024");
   TopoHost& t = *ctx->topos[topo_id];
-  size_t sm = smem_bytes(t.dev, threads, false);
+  size_t sm = smem_bytes(t.dev, threads, false, precise != 0);
   bool vg = sm + kStaticSmem > (size_t)ctx->smem_optin;
-  sm = smem_bytes(t.dev, threads, vg);
+  sm = smem_bytes(t.dev, threads, vg, precise != 0);
   if (sm + kStaticSmem > (size_t)ctx->smem_optin) return fail(ctx, MF_ERR_INVALID, "does not fit");
   Cfg& c = t.cfg[precise ? 1 : 0];
   c.threads = threads;

@@ -22,16 +22,24 @@ __host__ __device__ inline size_t site_region_bytes(const TopoDev& t) {
 }
 
 // Shared-memory bytes needed by one condition of this lattice with NT threads.
-__host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, bool vec_global) {
+// Reduction scratch: 29 partials per warp (the metrics' fused reduction),
+// two double-buffered 96-float slots for the one-barrier reductions, and the
+// force broadcast.
+__host__ __device__ constexpr int red_floats(int nw) { return 29 * nw + 2 * 96 + 1; }
+
+// Shared-memory bytes of one condition of this lattice with nt threads in one
+// precision mode (mirrors carve() below: every array both modes use, plus
+// the float32 scan-reversal buffers or the precise-mode CG vectors w, s and
+// the partner lists).
+__host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, bool vec_global, bool precise) {
   const int N = t.n_dof, X = t.total_xbs, S = t.n_sites_total;
   const int nw = nt / 32;
-  const int scan = t.plan_thin.total > t.plan_thick.total ? t.plan_thin.total : t.plan_thick.total;
   const CoefLayout cl = coef_layout(t);
   size_t o = 0;
   auto add = [&](size_t bytes) { o = align_up(o + bytes, 16); };
   add(sizeof(double) * 64);                // redd
-  add(sizeof(float) * 1536);               // red
-  if (!vec_global) add(sizeof(float) * 7 * N);  // x r dx pv zz wv sv
+  add(sizeof(float) * red_floats(nw));     // red
+  if (!vec_global) add(sizeof(float) * (precise ? 7 : 5) * N);  // x r dx pv zz (+ wv sv)
   if (!vec_global) add(sizeof(float) * 4 * X);  // fxb fdx fdd frdd
   add(sizeof(float) * X);                  // xb_ax
   add(site_region_bytes(t));               // site / win1 | win2, overlaid by face_pos and site_h
@@ -42,7 +50,7 @@ __host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, bool vec_
   add(sizeof(float) * 27 * 16);            // cum_tm
   add(sizeof(float) * 6 * t.n_bins);       // pabs
   add(sizeof(float) * cl.total);           // coef
-  add(sizeof(float) * nw * scan);          // scan
+  if (!precise) add(sizeof(float) * nw * 128);  // scan reversal buffer per warp (filaments <= 128)
   add(sizeof(float) * kNParams);           // P
   add(sizeof(float) * 4 * t.n_thick);      // tvec
   add(sizeof(int16_t) * X);                // blist
@@ -50,7 +58,7 @@ __host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, bool vec_
   add(sizeof(int) * 32);                   // wsum
   add(sizeof(int16_t) * X);                // xb_key
   add(sizeof(int16_t) * X);                // hsite
-  if (!vec_global) add(sizeof(int16_t) * 6 * N);  // nb_node nb_head
+  if (!vec_global && precise) add(sizeof(int16_t) * 6 * N);  // nb_node nb_head
   add(3 * t.n_thin * 3);                   // face_mono face_kl face_kh
   if (!vec_global) {                       // old-state snapshot
     add(sizeof(float) * t.n_thick_nodes);
@@ -64,14 +72,16 @@ template <int NT, bool PR>
 __device__ void carve(Sim<NT, PR>& m, char* base, bool vec_global) {
   const TopoDev& t = m.T;
   const int N = t.n_dof, X = t.total_xbs, S = t.n_sites_total;
-  const int scan = t.plan_thin.total > t.plan_thick.total ? t.plan_thin.total : t.plan_thick.total;
   size_t o = 0;
   auto take = [&](size_t bytes) { char* p = base + o; o = align_up(o + bytes, 16); return p; };
   m.s.redd = (double*)take(sizeof(double) * 64);
-  m.s.red = (float*)take(sizeof(float) * 1536);
-  float* v7 = vec_global ? reinterpret_cast<float*>(m.ws + m.L.vec) : (float*)take(sizeof(float) * 7 * N);
+  m.s.red = (float*)take(sizeof(float) * red_floats(NT / 32));
+  // the workspace keeps room for all seven vectors; shared memory only for
+  // the ones this mode uses
+  float* v7 = vec_global ? reinterpret_cast<float*>(m.ws + m.L.vec) : (float*)take(sizeof(float) * (PR ? 7 : 5) * N);
   m.s.x = v7; m.s.r = v7 + N; m.s.dx = v7 + 2 * N; m.s.pv = v7 + 3 * N; m.s.zz = v7 + 4 * N;
-  m.s.wv = v7 + 5 * N; m.s.sv = v7 + 6 * N;
+  m.s.wv = PR ? v7 + 5 * N : nullptr;
+  m.s.sv = PR ? v7 + 6 * N : nullptr;
   float* f4 = vec_global ? reinterpret_cast<float*>(m.ws + m.L.vec) + 7 * N : (float*)take(sizeof(float) * 4 * X);
   m.s.fxb = f4; m.s.fdx = f4 + X; m.s.fdd = f4 + 2 * X; m.s.frdd = f4 + 3 * X;
   m.s.xb_ax = (float*)take(sizeof(float) * X);
@@ -91,7 +101,7 @@ __device__ void carve(Sim<NT, PR>& m, char* base, bool vec_global) {
   m.s.cum_tm = (float*)take(sizeof(float) * 27 * 16);
   m.s.pabs = (float*)take(sizeof(float) * 6 * t.n_bins);
   m.s.coef = (float*)take(sizeof(float) * m.cl.total);
-  m.s.scan = (float*)take(sizeof(float) * NT / 32 * scan);
+  m.s.scan = PR ? nullptr : (float*)take(sizeof(float) * NT / 32 * 128);
   m.s.P = (float*)take(sizeof(float) * kNParams);
   m.s.tvec = (float*)take(sizeof(float) * 4 * t.n_thick);
   m.s.blist = (int16_t*)take(sizeof(int16_t) * X);
@@ -102,7 +112,7 @@ __device__ void carve(Sim<NT, PR>& m, char* base, bool vec_global) {
   m.s.face_mono = (int8_t*)take(3 * t.n_thin * 3);
   m.s.face_kl = m.s.face_mono + t.n_thin * 3;
   m.s.face_kh = m.s.face_kl + t.n_thin * 3;
-  if (!vec_global) {
+  if (!vec_global && PR) {
     m.s.nb_node = (int16_t*)take(sizeof(int16_t) * 6 * N);
     m.s.nb_head = m.s.nb_node + 3 * N;
   } else {
@@ -588,10 +598,10 @@ __device__ void run_condition(const StepArgs& A, int ci) {
         const float u = m.precise ? m.s.x[n0] : m.s.x[n0] - T.crown_off[n0];
         force += u * m.s.P[THICK_K];
       }
-      m.s.red[1535] = force;
+      m.s.red[red_floats(NT / 32) - 1] = force;
     }
     __syncthreads();
-    force = m.s.red[1535];
+    force = m.s.red[red_floats(NT / 32) - 1];
     __syncthreads();
     metrics(m, t, zl, pCa, new_ls, force, resid, iters, Mo);
     if (resid > (double)A.resid_warn) m.status |= 2;

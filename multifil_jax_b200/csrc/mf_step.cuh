@@ -105,7 +105,7 @@ struct Smem {
   float* pabs;    // [2*n_bins*3] absorbing-chain entries read by the metrics (kept
                   // in the workspace between launches)
   float* coef;    // Thomas scan coefficients (thick fwd, thick back, thin fwd, thin back, inv)
-  float* scan;    // per-warp scan scratch
+  float* scan;    // per-warp scan reversal buffer (float32 mode)
   float* P;       // [44]
   float* red;     // reduction scratch [64]
   double* redd;   // [64]
@@ -529,8 +529,7 @@ struct Sim {
       __syncwarp();
       return;
     }
-    float* buf = s.scan + warp * (T.plan_thin.total > T.plan_thick.total ? T.plan_thin.total
-                                                                          : T.plan_thick.total);
+    float* buf = s.scan + warp * 128;  // this warp's reversal buffer (filaments <= 128 nodes)
     __syncwarp();
     for (int f = warp; f < nf; f += NW) {
       const bool thick = f < T.n_thick;
@@ -577,7 +576,7 @@ struct Sim {
   __device__ __forceinline__ void reduce(float (&v)[K], bool max0) {
 #pragma unroll
     for (int k = 0; k < K; ++k) v[k] = (max0 && k == 0) ? warp_max(v[k]) : warp_sum(v[k]);
-    float* rb = s.red + 1024 + redbuf * 96;  // clear of bred/bsum_* (red[0, 1024)) and red[1535]
+    float* rb = s.red + 29 * NW + redbuf * 96;  // clear of the 29 * NW partials and the force slot
     redbuf ^= 1;
     if (lane == 0)
 #pragma unroll
