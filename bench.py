@@ -325,7 +325,8 @@ def bench_serving(args, device):
         reqs.append((key, float(rng.uniform(4, 7)), float(rng.uniform(850, 1000)), dur,
                      prng_split(prng_key(1000 + i), 1)[0]))
     total_steps = sum(int(r[3]) for r in reqs)
-    srv = SimulationServer(mem_budget=args.serve_budget_gb << 30, chunk_steps=args.serve_chunk, device=device)
+    srv = SimulationServer(mem_budget=args.serve_budget_gb << 30, chunk_steps=args.serve_chunk, device=device,
+                           precision=args.precision)
     # arrival rate: a fraction of the measured batched capacity for this mix
     lam = args.serve_rate
     t_arr = np.cumsum(rng.exponential(1.0 / lam, n))
@@ -356,7 +357,7 @@ def bench_serving(args, device):
             'p99_latency_s': float(np.percentile(lat, 99)) if lat.size else None,
             'condition_timesteps_per_s': total_steps / t_end, 'wall_s': t_end,
             'mix': f'lattice 1..{args.serve_max_lattice} square/rect, duration U[{args.serve_min_ms},{args.serve_max_ms}] ms, '
-                   f'skeletal/cardiac 50/50, chunk {args.serve_chunk} steps'}
+                   f'skeletal/cardiac 50/50, chunk {args.serve_chunk} steps, {args.precision} precision'}
 
 
 def _oracle_sample(args_tuple):

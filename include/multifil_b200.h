@@ -172,8 +172,12 @@ typedef struct {
 } mf_request;
 
 /* Start a server on ctx with a device-memory budget (bytes) for resident
- * slots and a chunk of steps per scheduling tick. */
+ * slots and a chunk of steps per scheduling tick.  mf_server_start runs every
+ * request in float32 mode (the reference's arithmetic); mf_server_start_mode
+ * with precise = 1 runs them with MF_FLAG_PRECISE. */
 int mf_server_start(mf_ctx* ctx, uint64_t mem_budget, int32_t chunk_steps, int32_t max_slots);
+int mf_server_start_mode(mf_ctx* ctx, uint64_t mem_budget, int32_t chunk_steps, int32_t max_slots,
+                         int32_t precise);
 /* Queue a request; returns its id.  MF_ERR_NOMEM if it can never fit. */
 int mf_server_submit(mf_ctx* ctx, const mf_request* req, uint64_t* req_id);
 /* Run up to max_ticks scheduling ticks (admit, launch one chunk, retire). */

@@ -95,6 +95,8 @@ _SIGNATURES = {
     'mf_prng_uniform': (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32,
                                        ctypes.c_void_p]),
     'mf_server_start': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int32, ctypes.c_int32]),
+    'mf_server_start_mode': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int32, ctypes.c_int32,
+                                            ctypes.c_int32]),
     'mf_server_submit': (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(mf_request),
                                         ctypes.POINTER(ctypes.c_uint64)]),
     'mf_server_step': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),

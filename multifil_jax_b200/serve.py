@@ -38,16 +38,21 @@ class ServedResult:
 class SimulationServer:
     """Admit / run / retire simulation requests on one GPU.
 
+    ``precision`` is the arithmetic of every request: ``'mixed'`` (default,
+    as ``run(..., precision='mixed')``) or ``'float32'`` (the reference's).
     ``mem_budget`` bounds the device bytes of resident slots (state, tables,
     metric buffers); ``chunk_steps`` is the scheduling tick in timesteps.
     """
 
     def __init__(self, mem_budget: int = 2 << 30, chunk_steps: int = 50, max_slots: int = 4096,
-                 device: Optional[int] = None):
+                 device: Optional[int] = None, precision: str = 'mixed'):
+        if precision not in ('float32', 'mixed'):
+            raise ValueError("precision must be 'float32' or 'mixed'")
         self.eng = get_engine(device)
         self.lib = self.eng.lib
-        self._check(self.lib.mf_server_start(self.eng.h, int(mem_budget), int(chunk_steps), int(max_slots)),
-                    'mf_server_start')
+        self.precision = precision
+        self._check(self.lib.mf_server_start_mode(self.eng.h, int(mem_budget), int(chunk_steps), int(max_slots),
+                                                  int(precision == 'mixed')), 'mf_server_start_mode')
         self._steps: Dict[int, int] = {}
         self._open = True
 

@@ -4,7 +4,7 @@ import pytest
 
 from multifil_jax_b200 import SarcTopology, get_skeletal_params, get_cardiac_params
 from multifil_jax_b200.serve import SimulationServer
-from multifil_jax_b200.engine import EngineError
+from multifil_jax_b200.engine import EngineError, MF_FLAG_PRECISE
 from multifil_jax_b200.simulation import METRIC_KEYS
 from oracle import prng
 from tests.gpu_helpers import run_engine
@@ -24,16 +24,18 @@ def _requests(n, seed=1, lo=1, hi=3):
     return out
 
 
-def _alone(engine, q):
+def _alone(engine, q, precision='mixed'):
     T = int(q['dur'])
     res = run_engine(engine, q['topo'], q['params'].param_row()[None], np.full((1, T), q['z']),
-                     np.full((1, T), q['pCa']), np.full((1, T), 14.0), q['key'][None])
+                     np.full((1, T), q['pCa']), np.full((1, T), 14.0), q['key'][None],
+                     flags=MF_FLAG_PRECISE if precision == 'mixed' else 0)
     return res['metrics'][0]
 
 
-def test_served_equals_alone_with_late_arrivals(engine):
+@pytest.mark.parametrize('precision', ['mixed', 'float32'])
+def test_served_equals_alone_with_late_arrivals(engine, precision):
     reqs = _requests(12)
-    with SimulationServer(mem_budget=256 << 20, chunk_steps=7) as srv:
+    with SimulationServer(mem_budget=256 << 20, chunk_steps=7, precision=precision) as srv:
         ids = [srv.submit(q['topo'], q['params'], q['pCa'], q['z'], q['dur'], q['key']) for q in reqs[:6]]
         srv.step(2)  # the first six are on the GPU when the rest arrive
         ids += [srv.submit(q['topo'], q['params'], q['pCa'], q['z'], q['dur'], q['key']) for q in reqs[6:]]
@@ -41,7 +43,7 @@ def test_served_equals_alone_with_late_arrivals(engine):
         for rid, q in zip(ids, reqs):
             r = srv.poll(rid)
             assert r is not None and r.latency_s >= 0
-            ref = _alone(engine, q)
+            ref = _alone(engine, q, precision)
             got = np.stack([r.metrics[k].astype(np.float32) for k in METRIC_KEYS])
             assert np.array_equal(got, ref), q
 
