@@ -109,6 +109,9 @@ class ClockSampler:
                 'reasons': reasons, 'samples': len(rows)}
 
 
+E2E_WARMUP = 2
+
+
 def sweep_inputs():
     from multifil_jax_b200 import SarcTopology, get_skeletal_params
     from multifil_jax_b200.simulation import plan_batch
@@ -204,15 +207,18 @@ def bench_gpu(args):
     nbound_mean = float(met[:, 5, :].mean())
     clocks = clk.summary()
 
-    # e2e: the public API with host buffers (plan, H2D, kernel, D2H inside)
+    # e2e: the public API with host buffers (plan, H2D, kernel, D2H inside).  The
+    # untimed calls first let the page-locked result blocks reach their steady
+    # state (each call's result is dropped after the next one returns).
     e2e_times = []
-    for k in range(max(1, args.steps)):
+    for k in range(E2E_WARMUP + max(1, args.steps)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         r = run(topo, duration_ms=T_SWEEP, pCa=pcas, z_line=900.0, dynamic_params=d, static_params=s,
                 rng_seed=0, precision=args.precision)
         t1 = time.perf_counter()
-        e2e_times.append(t1 - t0)
+        if k >= E2E_WARMUP:
+            e2e_times.append(t1 - t0)
     t_e2e = _max_over_ranks(float(np.sum(e2e_times)), world, dev)
     e2e_value = B * T * len(e2e_times) * world / t_e2e
     h2d = plan.params.nbytes + plan.z.nbytes + plan.pCa.nbytes + plan.ls.nbytes + plan.keys.nbytes + \
@@ -277,7 +283,8 @@ def bench_gpu(args):
                    'precision_modes': 'mixed = node displacements + float64 residual test + renormalised '
                                       'float64 expm squaring (<=1e-5 force error vs the FP64 oracle); '
                                       'float32 = the reference\'s single-precision arithmetic'},
-        'e2e': {'value': e2e_value, 'unit': METRIC, 'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': int(d2h)},
+        'e2e': {'value': e2e_value, 'unit': METRIC, 'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': int(d2h),
+                'warmup_calls': E2E_WARMUP},
         'gpu_launches': args.steps,
         'roofline': {'bound': 'hbm', 'achieved': hbm_gbs, 'peak': peaks['hbm_gbs'], 'unit': 'GB/s',
                      'frac': hbm_gbs / peaks['hbm_gbs'], 'peak_source': peak_source,

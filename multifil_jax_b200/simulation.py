@@ -293,10 +293,14 @@ def plan_batch(topology: SarcTopology, duration_ms: float = 1000.0, dt: float = 
         if isinstance(value, list):
             if not value:
                 raise ValueError(f"{name} sweep list is empty")
-            rows = [as_trace(v) for v in value]
-            if any(r.shape != (n_steps,) for r in rows):
-                raise ValueError(f"{name} trace length != n_steps {n_steps}")
-            wf_tables[name] = np.stack(rows).astype(np.float32)
+            if all(np.ndim(v) == 0 for v in value):  # scalar sweep: one constant trace per value
+                col = np.asarray(value, dtype=float).astype(np.float32)[:, None]
+                wf_tables[name] = np.repeat(col, n_steps, axis=1)
+            else:
+                rows = [as_trace(v) for v in value]
+                if any(r.shape != (n_steps,) for r in rows):
+                    raise ValueError(f"{name} trace length != n_steps {n_steps}")
+                wf_tables[name] = np.stack(rows).astype(np.float32)
             trace_sweep = any(not isinstance(v, (int, float)) and np.asarray(v).ndim == 1
                               and len(np.asarray(v)) == n_steps for v in value)
             coords = ([np.asarray(wf_tables[name][i]) for i in range(len(value))] if trace_sweep
