@@ -11,6 +11,8 @@ namespace mf {
 
 constexpr int kNParams = 44;
 constexpr int kNMetrics = 52;
+// per-warp partials of the metrics' fused block reduction (one per lane)
+constexpr int kRedPartials = 32;
 constexpr int kMaxLevels = 12;
 
 // DynamicParams field indices (reference core/params.py:73-556 order).

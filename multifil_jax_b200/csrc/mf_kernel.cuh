@@ -22,10 +22,10 @@ __host__ __device__ inline size_t site_region_bytes(const TopoDev& t) {
 }
 
 // Shared-memory bytes needed by one condition of this lattice with NT threads.
-// Reduction scratch: 29 partials per warp (the metrics' fused reduction),
+// Reduction scratch: 32 partials per warp (the metrics' fused reduction),
 // two double-buffered 96-float slots for the one-barrier reductions, and the
 // force broadcast.
-__host__ __device__ constexpr int red_floats(int nw) { return 29 * nw + 2 * 96 + 1; }
+__host__ __device__ constexpr int red_floats(int nw) { return kRedPartials * nw + 2 * 96 + 1; }
 
 // Shared-memory bytes of one condition of this lattice with nt threads in one
 // precision mode (mirrors carve() below: every array both modes use, plus
@@ -134,14 +134,50 @@ __device__ void carve(Sim<NT, PR>& m, char* base, bool vec_global) {
 // ---------------------------------------------------------------------------
 // metrics epilogue (metrics_fn.py:154-417), written to metrics[b][k][t]
 // ---------------------------------------------------------------------------
+// Every thread accumulates its share of the 31 block totals (counts, sums,
+// extrema and the thick-filament energies), the warps reduce them with one
+// transposed exchange and meet at a single barrier.  After it every warp
+// forms the totals from the per-warp partials and stores its share of the
+// 18 output groups (group q = lane * NW + warp), so no warp carries the
+// whole epilogue.  The axial force is summed in filament order by thread 0
+// during the partial pass and handed over through the same barrier.
 template <int NT, bool PR>
-__device__ void metrics(Sim<NT, PR>& m, int t, float zl, float pCa, float new_ls, float force, double resid,
-                        int iters, float* Mo) {
+__device__ void metrics(Sim<NT, PR>& m, int t, float zl, float pCa, float new_ls, double resid, int iters,
+                        float* Mo) {
   const TopoDev& T = m.T;
   const int X = T.total_xbs, S = T.n_sites_total, NTN = T.n_thick_nodes;
   const int tid = m.tid;
+  constexpr int NW = NT / 32;
+  const int lane = m.lane, warp = m.warp;
   const float* pabs = m.s.pabs;
   const float* old_x = m.s.old_thick;
+  const float* P = m.s.P;
+  float* red = m.s.red;
+  float* force_slot = red + red_floats(NW) - 1;
+#ifdef MF_PHASE_TIMING
+  // diagnostic build only: thread 0's own timeline through the epilogue
+  long long mt0 = clock64();
+#define MF_MT(k)                                       \
+  do {                                                 \
+    if (tid == 0) {                                    \
+      const long long now_ = clock64();                \
+      m.sub_acc[8 + (k)] += (double)(now_ - mt0);      \
+      mt0 = now_;                                      \
+    }                                                  \
+  } while (0)
+#else
+#define MF_MT(k) do { } while (0)
+#endif
+  if (tid == 0) {
+    // axial force: sum over thick filaments in filament order
+    float force = 0.f;
+    for (int th = 0; th < T.n_thick; ++th) {
+      const int n0 = th * T.n_crowns;
+      const float u = m.precise ? m.s.x[n0] : m.s.x[n0] - T.crown_off[n0];
+      force += u * P[THICK_K];
+    }
+    *force_slot = force;
+  }
   // per-thread partials: counts (exact in float), sums, extrema
   float c_xb[7] = {0, 0, 0, 0, 0, 0, 0};  // 6 states + bound
   float c_tm[4] = {0, 0, 0, 0};
@@ -202,36 +238,14 @@ __device__ void metrics(Sim<NT, PR>& m, int t, float zl, float pCa, float new_ls
     nmin = fminf(nmin, dsp);
     nmax = fmaxf(nmax, dsp);
   }
-  float r[29] = {-tmin, tmax, -nmin, nmax,
-                 c_xb[0], c_xb[1], c_xb[2], c_xb[3], c_xb[4], c_xb[5], c_xb[6],
-                 c_tm[0], c_tm[1], c_tm[2], c_tm[3], ov, ov2, ov3, atp, newly,
-                 tsum, tsq, nsum, nsq, dxs, atp_p, tear, 0.f, 0.f};
-  // block reduction: warp partials to shared memory, then warp 0 finishes
-  // the 29 totals one per lane and writes the 52 metrics in parallel
-  constexpr int NW = NT / 32;
-  const int lane = m.lane, warp = m.warp;
-#pragma unroll
-  for (int k = 0; k < 29; ++k) r[k] = k < 4 ? warp_max(r[k]) : warp_sum(r[k]);
-  float* red = m.s.red;
-  __syncthreads();
-  if (lane == 0)
-#pragma unroll
-    for (int k = 0; k < 29; ++k) red[k * NW + warp] = r[k];
-  __syncthreads();
-  if (warp != 0) return;
-  float R = 0.f;
-  if (lane < 29) {
-    R = red[lane * NW];
-    for (int w = 1; w < NW; ++w) R = lane < 4 ? fmaxf(R, red[lane * NW + w]) : R + red[lane * NW + w];
-  }
-  auto tot = [&](int k) { return __shfl_sync(0xffffffffu, R, k); };
-  // energies over thick filaments (metrics_fn.py:262-288), one filament per lane
-  const float* P = m.s.P;
+  // energies of the thick backbone's first spring and of titin
+  // (metrics_fn.py:262-288), one filament per thread counted from the last
+  // thread (the first threads carry the force sum and the loop remainders)
   float e_new = 0.f, e_delta = 0.f, te_new = 0.f, te_delta = 0.f;
   {
     const float k = P[THICK_K];
     const float a = P[TITIN_A], bb = P[TITIN_B], r0 = P[TITIN_REST];
-    for (int th = lane; th < T.n_thick; th += 32) {
+    for (int th = NT - 1 - tid; th < T.n_thick; th += NT) {
       const int n0 = th * T.n_crowns;
       const float u_new = m.precise ? m.s.x[n0] : m.s.x[n0] - T.crown_off[n0];
       const float u_old = m.precise ? old_x[n0] : old_x[n0] - T.crown_off[n0];
@@ -256,72 +270,89 @@ __device__ void metrics(Sim<NT, PR>& m, int t, float zl, float pCa, float new_ls
       te_new += tn;
       te_delta += tn - to;
     }
-    e_new = warp_sum(e_new);
-    e_delta = warp_sum(e_delta);
-    te_new = warp_sum(te_new);
-    te_delta = warp_sum(te_delta);
   }
+  MF_MT(0);
+  // values 0-3 are maxima (minima negated), the rest sums
+  float r[32] = {-tmin, tmax, -nmin, nmax,
+                 c_xb[0], c_xb[1], c_xb[2], c_xb[3], c_xb[4], c_xb[5], c_xb[6],
+                 c_tm[0], c_tm[1], c_tm[2], c_tm[3], ov, ov2, ov3, atp, newly,
+                 tsum, tsq, nsum, nsq, dxs, atp_p, tear, e_new, e_delta, te_new, te_delta, 0.f};
+  red[lane * NW + warp] = warp_reduce_transposed<4>(r, lane);
+  MF_MT(1);
+  __syncthreads();
+  MF_MT(2);
+  // block totals, lane k holding total k (every warp forms them itself)
+  float R = red[lane * NW];
+#pragma unroll 4
+  for (int w = 1; w < NW; ++w) R = lane < 4 ? fmaxf(R, red[lane * NW + w]) : R + red[lane * NW + w];
+  const float force = *force_slot;
+  auto tot = [&](int k) { return __shfl_sync(0xffffffffu, R, k); };
+  MF_MT(3);
+  const int q = lane * NW + warp;  // this lane's output group
+  // every shuffle is executed by all 32 lanes; the branches below only store
+  const float own = tot(q < 6 ? 4 + q : (q < 10 ? 5 + q : 14));
   const float tmin_ = -tot(0), tmax_ = tot(1), nmin_ = -tot(2), nmax_ = tot(3);
   const float nb = tot(10), nov = tot(15), n2 = tot(16), n3 = tot(17);
   const float r18 = tot(18), r19 = tot(19), r20 = tot(20), r21 = tot(21), r22 = tot(22), r23 = tot(23);
   const float r24 = tot(24), r25 = tot(25), r26 = tot(26);
+  const float en_new = tot(27), en_delta = tot(28), ten_new = tot(29), ten_delta = tot(30);
+  MF_MT(4);
   const float nx = (float)X, nt = (float)S;
-  // every shuffle above and here is executed by all 32 lanes; the branches
-  // below only store
-  const float own = tot(lane < 6 ? 4 + lane : (lane < 10 ? 5 + lane : 14));
   auto put = [&](int k, float v) { Mo[(size_t)k * m.Tstride + t] = v; };
-  if (lane < 6) {
-    put(M_N_XB_DRX + lane, own);
-    put(M_FRAC_XB_DRX + lane, own / nx);
-  } else if (lane < 10) {
-    const int j = lane - 6;
+  if (q < 6) {
+    put(M_N_XB_DRX + q, own);
+    put(M_FRAC_XB_DRX + q, own / nx);
+  } else if (q < 10) {
+    const int j = q - 6;
     put(M_N_TM_0 + j, own);
     put(M_FRAC_TM_0 + j, own / nt);
-  } else if (lane == 10) {
+  } else if (q == 10) {
     put(M_AXIAL_FORCE, force);
     put(M_SOLVER_RESIDUAL, (float)resid);
     put(M_Z_LINE, zl);
     put(M_PCA, pCa);
     put(M_LATTICE_SPACING, new_ls);
-  } else if (lane == 11) {
+  } else if (q == 11) {
     put(M_N_BOUND, nb);
     put(M_FRAC_XB_BOUND, nb / nx);
     put(M_ACTIN_PERM, own / nt);
-  } else if (lane == 12) {
+  } else if (q == 12) {
     put(M_FRAC_TM_2_OV, n2 / nov);
     put(M_FRAC_TM_3_OV, n3 / nov);
     put(M_FRAC_TM_AVAIL_OV, (n2 + n3) / nov);
     put(M_N_OVERLAP, nov);
-  } else if (lane == 13) {
+  } else if (q == 13) {
     put(M_ATP_CONSUMED, r18);
     put(M_NEWLY_BOUND, r19);
     put(M_ATP_EXPECTED_P, r25);
     put(M_XB_TEAR, r26);
     put(M_NEWTON_ITERS, (float)iters);
-  } else if (lane == 14) {
+  } else if (q == 14) {
     const float tmean_c = r20 / (float)NTN;
     put(M_THICK_D_MEAN, t_shift + tmean_c);
     put(M_THICK_D_MAX, tmax_);
     put(M_THICK_D_MIN, tmin_);
     put(M_THICK_D_STD, sqrtf(fmaxf(r21 / (float)NTN - tmean_c * tmean_c, 0.f)));
-  } else if (lane == 15) {
+  } else if (q == 15) {
     const float nmean_c = r22 / (float)S;
     put(M_THIN_D_MEAN, n_shift + nmean_c);
     put(M_THIN_D_MAX, nmax_);
     put(M_THIN_D_MIN, nmin_);
     put(M_THIN_D_STD, sqrtf(fmaxf(r23 / (float)S - nmean_c * nmean_c, 0.f)));
-  } else if (lane == 16) {
+  } else if (q == 16) {
     const float fth = (float)T.n_thick;
-    put(M_THICK_E_AVG, e_new / fth);
-    put(M_THICK_E_DELTA, e_delta / fth);
-    put(M_TITIN_E_AVG, te_new / fth);
-    put(M_TITIN_E_DELTA, te_delta / fth);
-  } else if (lane == 17) {
+    put(M_THICK_E_AVG, en_new / fth);
+    put(M_THICK_E_DELTA, en_delta / fth);
+    put(M_TITIN_E_AVG, ten_new / fth);
+    put(M_TITIN_E_DELTA, ten_delta / fth);
+  } else if (q == 17) {
     const float work = force * (r24 / (float)NTN);
     put(M_WORK_THICK, work);
     put(M_WORK_THICK_MEAN, work / (float)NTN);
     put(M_WORK_PER_ATP, r25 > 0.01f ? work / r25 : 0.0f);
   }
+  MF_MT(5);
+#undef MF_MT
 }
 
 // ---------------------------------------------------------------------------
@@ -349,8 +380,8 @@ __device__ void run_condition(const StepArgs& A, int ci) {
 #ifdef MF_PHASE_TIMING
   // totals in shared memory: a runtime-indexed local array would add a
   // local-memory round trip to every marker
-  __shared__ double ph_sh[20];
-  if (threadIdx.x < 20) ph_sh[threadIdx.x] = 0.0;
+  __shared__ double ph_sh[28];
+  if (threadIdx.x < 28) ph_sh[threadIdx.x] = 0.0;
   long long ph_t0 = clock64();
   int ph_cur = 0;
 #endif
@@ -469,14 +500,22 @@ __device__ void run_condition(const StepArgs& A, int ci) {
     __syncthreads();
   }
 
-  // pre-step snapshot buffers live in global workspace is avoided: keep the
-  // old thick positions / states in the spare CG vectors between phases
-  float* Mo = cd.metrics;
   __shared__ uint32_t sub_thin[2], sub_thick[2];
-  // drivers of step t are loaded during step t - 1 (their latency overlaps a
-  // whole step instead of opening one)
-  float nx_z = t0 < t1 ? zt[t0] : 0.0f, nx_p = t0 < t1 ? pt[t0] : 0.0f, nx_l = t0 < t1 ? lt[t0] : 0.0f;
-  float prev_z = t0 > 0 ? zt[t0 - 1] : 0.0f;
+  // Drivers (z, pCa, ls) of step t in drv[t & 1].  Thread 0 copies those of
+  // step t + 1 with cp.async during step t: their latency overlaps a whole
+  // step, and no register holds them (or the driver pointers) across the
+  // step's phases, whose peak register demand is the solver's.
+  __shared__ float drv[2][3];
+  __shared__ float prev_z_s;
+  if (m.tid == 0) {
+    if (t0 < t1) {
+      drv[t0 & 1][0] = zt[t0];
+      drv[t0 & 1][1] = pt[t0];
+      drv[t0 & 1][2] = lt[t0];
+    }
+    prev_z_s = t0 > 0 ? zt[t0 - 1] : 0.0f;
+  }
+  __syncthreads();
   // t = -1: the initial equilibrium with the constants (A1): nearest sites
   // at the constant spacing, table rows of the initial geometry, one solve
   // at the constant z_line with the spacing held fixed.
@@ -487,15 +526,15 @@ __device__ void run_condition(const StepArgs& A, int ci) {
       zl = m.s.P[Z_LINE];
       d_kin = m.s.P[LATTICE_SPACING];
     } else {
-      zl = nx_z;
-      pCa = nx_p;
-      ls_t = nx_l;
-      const float dz = t > 0 ? zl - prev_z : 0.0f;
-      prev_z = zl;
-      if (t + 1 < t1) {
-        nx_z = zt[t + 1];
-        nx_p = pt[t + 1];
-        nx_l = lt[t + 1];
+      zl = drv[t & 1][0];
+      pCa = drv[t & 1][1];
+      ls_t = drv[t & 1][2];
+      const float dz = t > 0 ? zl - prev_z_s : 0.0f;
+      if (m.tid == 0 && t + 1 < t1) {
+        float* nx = drv[(t + 1) & 1];
+        cp_async4(nx + 0, cd.z + t + 1);
+        cp_async4(nx + 1, cd.pCa + t + 1);
+        cp_async4(nx + 2, cd.ls + t + 1);
       }
       // 1. rigid shift of the thin filaments
       if (!m.precise) {
@@ -568,16 +607,21 @@ __device__ void run_condition(const StepArgs& A, int ci) {
       if (m.tid == 0) {
         key_s[0] = cd.key[0];
         key_s[1] = cd.key[1];
-        ls_s = lt[0];
+        ls_s = cd.ls[0];
         tab_key[0] = NAN;
         tab_key[1] = NAN;
         tab_key[2] = NAN;
         tab_key[3] = NAN;
-        tab_key[4] = (double)zt[0];
+        tab_key[4] = (double)cd.z[0];
       }
       __syncthreads();
       continue;
     }
+    // the step's drivers again from shared memory: their registers are free
+    // during the solve
+    zl = drv[t & 1][0];
+    pCa = drv[t & 1][1];
+    ls_t = drv[t & 1][2];
     const float new_ls = m.dyn ? d : ls_t;
     if (m.tid == 0) ls_s = new_ls;
     // absorbing table for the metrics at (pCa, new_ls)
@@ -591,19 +635,7 @@ __device__ void run_condition(const StepArgs& A, int ci) {
     __syncthreads();
     MF_PH(9);
     // 6. force + metrics
-    float force = 0.f;
-    if (m.tid == 0) {
-      for (int th = 0; th < T.n_thick; ++th) {
-        const int n0 = th * T.n_crowns;
-        const float u = m.precise ? m.s.x[n0] : m.s.x[n0] - T.crown_off[n0];
-        force += u * m.s.P[THICK_K];
-      }
-      m.s.red[red_floats(NT / 32) - 1] = force;
-    }
-    __syncthreads();
-    force = m.s.red[red_floats(NT / 32) - 1];
-    __syncthreads();
-    metrics(m, t, zl, pCa, new_ls, force, resid, iters, Mo);
+    metrics(m, t, zl, pCa, new_ls, resid, iters, cd.metrics);
     if (resid > (double)A.resid_warn) m.status |= 2;
     MF_PH(10);
     // optional traces
@@ -624,13 +656,17 @@ __device__ void run_condition(const StepArgs& A, int ci) {
       for (int i = m.tid; i < X; i += NT) { st[i] = m.s.xb_state[i]; bt[i] = m.s.xb_bound[i]; }
       for (int g = m.tid; g < S; g += NT) { st[A.max_xbs + g] = m.s.tm[g]; bt[A.max_xbs + g] = m.s.thin_bound[g]; }
     }
+    if (m.tid == 0) {
+      prev_z_s = zl;
+      cp_async_wait_all();  // step t + 1's drivers, published by the barrier below
+    }
     __syncthreads();
   }
   MF_PH(11);
 #ifdef MF_PHASE_TIMING
   if (m.tid == 0 && A.x_trace) {
     float* o = A.x_trace + (size_t)b * A.T * A.max_dof;
-    for (int k = 0; k < 20; ++k) o[k] = (float)ph_sh[k];
+    for (int k = 0; k < 28; ++k) o[k] = (float)ph_sh[k];
   }
 #endif
   // ---- write back resident state ----

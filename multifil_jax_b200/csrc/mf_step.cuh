@@ -55,6 +55,13 @@ struct StepArgs {
 
 constexpr int FLAG_DYN = 1, FLAG_PRECISE = 2, FLAG_ORIG_PRNG = 4;
 
+// 4-byte asynchronous global -> shared copy (no register holds the value)
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -65,6 +72,27 @@ __device__ __forceinline__ double warp_sum_d(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
+// Transposed warp reduction of 32 values per lane: after it lane l holds the
+// warp total of value l (max for l < NMAX, sum otherwise).  Each of the five
+// exchange steps halves the values a lane keeps, so it takes 31 shuffles
+// where 32 separate butterfly reductions take 160.
+template <int NMAX>
+__device__ __forceinline__ float warp_reduce_transposed(float (&v)[32], int lane) {
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) {
+    const bool up = (lane & o) != 0;
+    const int base = lane & (32 - o);  // value index of position 0 after this step, minus j
+#pragma unroll
+    for (int j = 0; j < o; ++j) {
+      const float send = up ? v[j] : v[j + o];
+      const float keep = up ? v[j + o] : v[j];
+      const float recv = __shfl_xor_sync(0xffffffffu, send, o);
+      v[j] = base + j < NMAX ? fmaxf(keep, recv) : keep + recv;
+    }
+  }
+  return v[0];
+}
+
 __device__ __forceinline__ float warp_max(float v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -576,7 +604,7 @@ struct Sim {
   __device__ __forceinline__ void reduce(float (&v)[K], bool max0) {
 #pragma unroll
     for (int k = 0; k < K; ++k) v[k] = (max0 && k == 0) ? warp_max(v[k]) : warp_sum(v[k]);
-    float* rb = s.red + 29 * NW + redbuf * 96;  // clear of the 29 * NW partials and the force slot
+    float* rb = s.red + kRedPartials * NW + redbuf * 96;  // clear of the metrics partials and the force slot
     redbuf ^= 1;
     if (lane == 0)
 #pragma unroll
