@@ -1,9 +1,9 @@
 """Compile the CUDA engine in-tree for sm_100a: ``python -m multifil_jax_b200.build``.
 
-The ten instances of the step kernel (CTA size x precision mode) are separate
-translation units of ``csrc/mf_kernels.cu`` and compile in parallel with the
-host/ABI unit ``csrc/mf_api.cu``; the objects are linked into
-``libmultifil_b200.so``.
+The twenty instances of the step kernel (CTA size x precision mode x
+dynamic spacing) are separate translation units of ``csrc/mf_kernels.cu`` and
+compile in parallel with the host/ABI unit ``csrc/mf_api.cu``; the objects are
+linked into ``libmultifil_b200.so``.
 """
 from __future__ import annotations
 
@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, 'csrc')
 OUT = os.path.join(HERE, 'libmultifil_b200.so')
 DEPS = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [
     os.path.join(os.path.dirname(HERE), 'include', 'multifil_b200.h')]
-INSTANCES = [(nt, p) for nt in (128, 256, 384, 512, 1024) for p in (0, 1)]
+INSTANCES = [(nt, p, d) for nt in (128, 256, 384, 512, 1024) for p in (0, 1) for d in (0, 1)]
 
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 NVCC_FLAGS = ARCH + ['-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC']
@@ -54,9 +54,9 @@ def build(force: bool = False, verbose: bool = False, out: str = OUT, extra_flag
     flags = NVCC_FLAGS + list(extra_flags) + (['-Xptxas=-v'] if verbose else [])
     with tempfile.TemporaryDirectory(prefix='mf_build_') as tmp:
         jobs = [[nvcc(), *flags, '-c', os.path.join(CSRC, 'mf_api.cu'), '-o', os.path.join(tmp, 'mf_api.o')]]
-        for nt, p in INSTANCES:
-            jobs.append([nvcc(), *flags, f'-DMF_NT={nt}', f'-DMF_P={p}', '-c', os.path.join(CSRC, 'mf_kernels.cu'),
-                         '-o', os.path.join(tmp, f'mf_k_{nt}_{p}.o')])
+        for nt, p, d in INSTANCES:
+            jobs.append([nvcc(), *flags, f'-DMF_NT={nt}', f'-DMF_P={p}', f'-DMF_D={d}', '-c',
+                         os.path.join(CSRC, 'mf_kernels.cu'), '-o', os.path.join(tmp, f'mf_k_{nt}_{p}_{d}.o')])
         with ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
             logs = list(ex.map(_run, jobs))
         objs = [j[-1] for j in jobs]

@@ -79,21 +79,21 @@ static int fail(mf_ctx* c, int code, const char* fmt, ...) {
 // ---------------------------------------------------------------------------
 // kernel dispatch by CTA size and precision (instances in mf_kernels.cu)
 // ---------------------------------------------------------------------------
-static cudaError_t prepare(int nt, bool precise, size_t smem) {
-#define MF_PREPARE_CASE(NT, P) \
-  if (nt == NT && precise == (P != 0)) return prepare_##NT##_##P(smem);
+static cudaError_t prepare(int nt, bool precise, bool dyn, size_t smem) {
+#define MF_PREPARE_CASE(NT, P, D) \
+  if (nt == NT && precise == (P != 0) && dyn == (D != 0)) return prepare_##NT##_##P##_##D(smem);
   MF_FOR_EACH_INSTANCE(MF_PREPARE_CASE)
 #undef MF_PREPARE_CASE
   return cudaErrorInvalidValue;
 }
 
 static cudaError_t launch(int nt, const StepArgs& a, int grid, int base, size_t smem, cudaStream_t st) {
-  const bool precise = (a.flags & FLAG_PRECISE) != 0;
-  cudaError_t e = prepare(nt, precise, smem);
+  const bool precise = (a.flags & FLAG_PRECISE) != 0, dyn = (a.flags & FLAG_DYN) != 0;
+  cudaError_t e = prepare(nt, precise, dyn, smem);
   if (e != cudaSuccess) return e;
   cudaGetLastError();  // clear a stale non-sticky error of an earlier, already reported call
-#define MF_LAUNCH_CASE(NT, P) \
-  if (nt == NT && precise == (P != 0)) return launch_##NT##_##P(a, grid, base, smem, st);
+#define MF_LAUNCH_CASE(NT, P, D) \
+  if (nt == NT && precise == (P != 0) && dyn == (D != 0)) return launch_##NT##_##P##_##D(a, grid, base, smem, st);
   MF_FOR_EACH_INSTANCE(MF_LAUNCH_CASE)
 #undef MF_LAUNCH_CASE
   return cudaErrorInvalidValue;
@@ -513,7 +513,8 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
       CK(cudaEventCreateWithFlags(&ctx->cap_event, cudaEventDisableTiming));
     }
     launch_st = ctx->cap_stream;
-    for (const Group& g : groups) CK(prepare(g.threads, (base_flags & FLAG_PRECISE) != 0, g.smem));
+    for (const Group& g : groups)
+      CK(prepare(g.threads, (base_flags & FLAG_PRECISE) != 0, (base_flags & FLAG_DYN) != 0, g.smem));
     CK(cudaEventRecord(ctx->cap_event, st));
     CK(cudaStreamWaitEvent(launch_st, ctx->cap_event, 0));
     CK(cudaStreamBeginCapture(launch_st, cudaStreamCaptureModeThreadLocal));

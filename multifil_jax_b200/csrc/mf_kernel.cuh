@@ -68,8 +68,8 @@ __host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, bool vec_
   return o;
 }
 
-template <int NT, bool PR>
-__device__ void carve(Sim<NT, PR>& m, char* base, bool vec_global) {
+template <int NT, bool PR, bool DY>
+__device__ void carve(Sim<NT, PR, DY>& m, char* base, bool vec_global) {
   const TopoDev& t = m.T;
   const int N = t.n_dof, X = t.total_xbs, S = t.n_sites_total;
   size_t o = 0;
@@ -141,8 +141,8 @@ __device__ void carve(Sim<NT, PR>& m, char* base, bool vec_global) {
 // 18 output groups (group q = lane * NW + warp), so no warp carries the
 // whole epilogue.  The axial force is summed in filament order by thread 0
 // during the partial pass and handed over through the same barrier.
-template <int NT, bool PR>
-__device__ void metrics(Sim<NT, PR>& m, int t, float zl, float pCa, float new_ls, double resid, int iters,
+template <int NT, bool PR, bool DY>
+__device__ void metrics(Sim<NT, PR, DY>& m, int t, float zl, float pCa, float new_ls, double resid, int iters,
                         float* Mo) {
   const TopoDev& T = m.T;
   const int X = T.total_xbs, S = T.n_sites_total, NTN = T.n_thick_nodes;
@@ -375,7 +375,7 @@ __device__ void metrics(Sim<NT, PR>& m, int t, float zl, float pCa, float new_ls
 #define MF_PH(k) do { } while (0)
 #endif
 
-template <int NT, bool PR>
+template <int NT, bool PR, bool DY>
 __device__ void run_condition(const StepArgs& A, int ci) {
 #ifdef MF_PHASE_TIMING
   // totals in shared memory: a runtime-indexed local array would add a
@@ -400,7 +400,7 @@ __device__ void run_condition(const StepArgs& A, int ci) {
   __syncthreads();
   const CondDesc& cd = sh_cd;
   const TopoDev& T = sh_T;
-  Sim<NT, PR> m(T, A, sh_s, sh_cl, sh_L);
+  Sim<NT, PR, DY> m(T, A, sh_s, sh_cl, sh_L);
 #ifdef MF_PHASE_TIMING
   m.sub_acc = ph_sh + 12;
 #endif
@@ -409,7 +409,7 @@ __device__ void run_condition(const StepArgs& A, int ci) {
   m.warp = m.tid >> 5;
   m.b = cd.index;
   m.ws = cd.ws;
-  m.dyn = (A.flags & FLAG_DYN) != 0;
+  m.set_dyn(DY);
   m.part = (A.flags & FLAG_ORIG_PRNG) == 0;
   m.status = 0;
   m.Tstride = cd.T;
@@ -417,8 +417,8 @@ __device__ void run_condition(const StepArgs& A, int ci) {
   __syncthreads();
   {
     const int nf = T.n_thick + T.n_thin;
-    m.regcg = PR && A.n_cg > 0 && (A.flags & 64) == 0 && nf <= Sim<NT, PR>::RF * (NT / 32) &&
-              T.n_crowns <= 32 * Sim<NT, PR>::RE && T.n_sites <= 32 * Sim<NT, PR>::RE && T.nxb <= 3;
+    m.regcg = PR && A.n_cg > 0 && (A.flags & 64) == 0 && nf <= Sim<NT, PR, DY>::RF * (NT / 32) &&
+              T.n_crowns <= 32 * Sim<NT, PR, DY>::RE && T.n_sites <= 32 * Sim<NT, PR, DY>::RE && T.nxb <= 3;
   }
   const int b = m.b;
   const int N = T.n_dof, X = T.total_xbs, S = T.n_sites_total, NTN = T.n_thick_nodes;
@@ -596,13 +596,13 @@ __device__ void run_condition(const StepArgs& A, int ci) {
     double resid;
     int iters;
     const bool dyn_save = m.dyn;
-    m.dyn = dyn_save && !init;
+    m.set_dyn(dyn_save && !init);
     float d = init ? d_kin : (m.dyn ? cur_ls : ls_t);
     m.build_bound_list();
     MF_PH(7);
     m.solve(zl, d, resid, iters, m.dyn);
     MF_PH(8);
-    m.dyn = dyn_save;
+    m.set_dyn(dyn_save);
     if (init) {
       if (m.tid == 0) {
         key_s[0] = cd.key[0];
@@ -709,11 +709,13 @@ __device__ void run_condition(const StepArgs& A, int ci) {
 constexpr int min_ctas(int nt) { return nt == 384 ? 2 : ((65536 / (nt * 128)) > 0 ? 65536 / (nt * 128) : 1); }
 
 // PR: precise (mixed) mode, a compile-time choice so that each kernel holds
-// only its own solver.
-template <int NT, bool PR>
+// only its own solver.  DY: dynamic lattice spacing; without it the radial
+// unknown and its recurrences are compiled out of the solver, which frees
+// the registers they hold through the CG loop.
+template <int NT, bool PR, bool DY>
 __global__ void __launch_bounds__(NT, min_ctas(NT))
     step_kernel(StepArgs A, int cond_base) {
-  run_condition<NT, PR>(A, cond_base + blockIdx.x);
+  run_condition<NT, PR, DY>(A, cond_base + blockIdx.x);
 }
 
 }  // namespace mf

@@ -1,22 +1,23 @@
-// One instance of the fused step kernel: step_kernel<MF_NT, MF_P> and its
-// launch entry points (declared in mf_launch.cuh).  Built once per instance:
-//   nvcc ... -DMF_NT=256 -DMF_P=1 -c mf_kernels.cu
+// One instance of the fused step kernel: step_kernel<MF_NT, MF_P, MF_D> and
+// its launch entry points (declared in mf_launch.cuh).  Built once per
+// instance:
+//   nvcc ... -DMF_NT=256 -DMF_P=1 -DMF_D=0 -c mf_kernels.cu
 #include "mf_kernel.cuh"
 #include "mf_launch.cuh"
 
-#if !defined(MF_NT) || !defined(MF_P)
-#error "compile with -DMF_NT=<CTA size> -DMF_P=<0|1>"
+#if !defined(MF_NT) || !defined(MF_P) || !defined(MF_D)
+#error "compile with -DMF_NT=<CTA size> -DMF_P=<0|1> -DMF_D=<0|1>"
 #endif
 
-#define MF_PASTE(a, b, c) a##b##_##c
-#define MF_NAME(a, b, c) MF_PASTE(a, b, c)
+#define MF_PASTE(a, b, c, d) a##b##_##c##_##d
+#define MF_NAME(a, b, c, d) MF_PASTE(a, b, c, d)
 
 namespace mf {
 
-cudaError_t MF_NAME(prepare_, MF_NT, MF_P)(size_t smem) {
+cudaError_t MF_NAME(prepare_, MF_NT, MF_P, MF_D)(size_t smem) {
   static size_t attr_bytes = 0;
   if (smem > attr_bytes) {
-    cudaError_t e = cudaFuncSetAttribute(step_kernel<MF_NT, (MF_P != 0)>,
+    cudaError_t e = cudaFuncSetAttribute(step_kernel<MF_NT, (MF_P != 0), (MF_D != 0)>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attr_bytes = smem;
@@ -24,8 +25,8 @@ cudaError_t MF_NAME(prepare_, MF_NT, MF_P)(size_t smem) {
   return cudaSuccess;
 }
 
-cudaError_t MF_NAME(launch_, MF_NT, MF_P)(const StepArgs& a, int grid, int base, size_t smem, cudaStream_t st) {
-  step_kernel<MF_NT, (MF_P != 0)><<<grid, MF_NT, smem, st>>>(a, base);
+cudaError_t MF_NAME(launch_, MF_NT, MF_P, MF_D)(const StepArgs& a, int grid, int base, size_t smem, cudaStream_t st) {
+  step_kernel<MF_NT, (MF_P != 0), (MF_D != 0)><<<grid, MF_NT, smem, st>>>(a, base);
   return cudaPeekAtLastError();
 }
 

@@ -216,8 +216,23 @@ static __device__ __noinline__ void build_tables_block(const float* P, const flo
   }
 }
 
-template <int NT, bool PR>
-struct Sim {
+// The dynamic-spacing flag: a runtime member in kernels built for dynamic
+// spacing (the initial equilibrium still holds the spacing fixed), a
+// compile-time false elsewhere.
+template <bool DY>
+struct SimDyn {
+  bool dyn;
+  __device__ void set_dyn(bool v) { dyn = v; }
+};
+template <>
+struct SimDyn<false> {
+  static constexpr bool dyn = false;
+  __device__ void set_dyn(bool) {}
+};
+
+template <int NT, bool PR, bool DY>
+struct Sim : SimDyn<DY> {
+  using SimDyn<DY>::dyn;
   static constexpr int NW = NT / 32;
   // The lattice, the shared-memory carve and the layouts live in CTA-shared
   // structs at fixed addresses: reading a field is one shared load, and none
@@ -231,7 +246,7 @@ struct Sim {
   int b;        // caller row
   int tid, lane, warp;
   static constexpr bool precise = PR;
-  bool dyn, part;
+  bool part;
   bool regcg;   // register-resident precise Newton-CG (solve_regs)
   float Kl, nu_c, dtm;
   double zref;  // precise mode thin reference z
