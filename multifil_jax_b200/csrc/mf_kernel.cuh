@@ -58,7 +58,7 @@ __host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, bool vec_
   add(sizeof(int) * 32);                   // wsum
   add(sizeof(int16_t) * X);                // xb_key
   add(sizeof(int16_t) * X);                // hsite
-  if (!vec_global && precise) add(sizeof(int16_t) * 6 * N);  // nb_node nb_head
+  if (!vec_global && precise) add(sizeof(int32_t) * 3 * N);  // nb
   add(3 * t.n_thin * 3);                   // face_mono face_kl face_kh
   if (!vec_global) {                       // old-state snapshot
     add(sizeof(float) * t.n_thick_nodes);
@@ -113,10 +113,9 @@ __device__ void carve(Sim<NT, PR, DY>& m, char* base, bool vec_global) {
   m.s.face_kl = m.s.face_mono + t.n_thin * 3;
   m.s.face_kh = m.s.face_kl + t.n_thin * 3;
   if (!vec_global && PR) {
-    m.s.nb_node = (int16_t*)take(sizeof(int16_t) * 6 * N);
-    m.s.nb_head = m.s.nb_node + 3 * N;
+    m.s.nb = (int32_t*)take(sizeof(int32_t) * 3 * N);
   } else {
-    m.s.nb_node = m.s.nb_head = nullptr;
+    m.s.nb = nullptr;
   }
   if (!vec_global) {
     m.s.old_thick = (float*)take(sizeof(float) * t.n_thick_nodes);
@@ -277,14 +276,14 @@ __device__ void metrics(Sim<NT, PR, DY>& m, int t, float zl, float pCa, float ne
                  c_xb[0], c_xb[1], c_xb[2], c_xb[3], c_xb[4], c_xb[5], c_xb[6],
                  c_tm[0], c_tm[1], c_tm[2], c_tm[3], ov, ov2, ov3, atp, newly,
                  tsum, tsq, nsum, nsq, dxs, atp_p, tear, e_new, e_delta, te_new, te_delta, 0.f};
-  red[lane * NW + warp] = warp_reduce_transposed<4>(r, lane);
+  red[warp * 32 + lane] = warp_reduce_transposed<4>(r, lane);  // warp-major: no bank conflicts
   MF_MT(1);
   __syncthreads();
   MF_MT(2);
   // block totals, lane k holding total k (every warp forms them itself)
-  float R = red[lane * NW];
+  float R = red[lane];
 #pragma unroll 4
-  for (int w = 1; w < NW; ++w) R = lane < 4 ? fmaxf(R, red[lane * NW + w]) : R + red[lane * NW + w];
+  for (int w = 1; w < NW; ++w) R = lane < 4 ? fmaxf(R, red[w * 32 + lane]) : R + red[w * 32 + lane];
   const float force = *force_slot;
   auto tot = [&](int k) { return __shfl_sync(0xffffffffu, R, k); };
   MF_MT(3);

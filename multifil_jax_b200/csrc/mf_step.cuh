@@ -55,6 +55,12 @@ struct StepArgs {
 
 constexpr int FLAG_DYN = 1, FLAG_PRECISE = 2, FLAG_ORIG_PRNG = 4;
 
+// Partner-list words: the partner node (int16, -1 none, -2 a site holding
+// three or more heads) in the low half, the head behind it in the high half.
+__device__ __forceinline__ int nb_pack(int node, int head) { return (int)((uint32_t)(uint16_t)node | ((uint32_t)head << 16)); }
+__device__ __forceinline__ int nb_node_of(int w) { return (int)(int16_t)(w & 0xffff); }
+__device__ __forceinline__ int nb_head_of(int w) { return (int)((uint32_t)w >> 16); }
+
 // 4-byte asynchronous global -> shared copy (no register holds the value)
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
@@ -143,8 +149,8 @@ struct Smem {
   int16_t* blist; // [X] heads carrying force this step, increasing index
   int16_t* hsite; // [X] global site of a force-carrying head, else -1
   int16_t* site_h;// [2S] first two force-carrying heads of every site (over site)
-  int16_t* nb_node; // [3N] partner nodes of every node (register CG only)
-  int16_t* nb_head; // [3N] the heads behind them
+  int32_t* nb;      // [3][N] partners of every node (register CG only): low 16 bits the
+                    // partner node, high 16 bits the head behind it
   double* face_pos; // [n_thin*3*width] staged candidate positions, NaN = invalid (over site, win2)
   int8_t* face_mono;// [n_thin*3] 0 scan, 1 increasing, 2 decreasing, 3 no candidate
   int8_t* face_kl;  // [n_thin*3] first valid candidate
@@ -1231,7 +1237,7 @@ struct Sim : SimDyn<DY> {
   // the whole solve, only u (read by the node's neighbours and partners)
   // and x (read by the head forces) are written to shared memory.  The
   // crossbridge coupling of every node is a fixed list of <= 3 partner
-  // nodes built once per step (nb_node / nb_head), so the JVP has no
+  // nodes built once per step (nb), so the JVP has no
   // dependent index chains.  Same Chronopoulos-Gear recurrences as
   // solve_cg_gear.
   // ------------------------------------------------------------------
@@ -1249,12 +1255,11 @@ struct Sim : SimDyn<DY> {
   }
 
   // Partner lists of every node for this step: crown i -> the sites of its
-  // heads, site g -> the crowns of the heads bound to it (nb_node = -2 on
+  // heads, site g -> the crowns of the heads bound to it (partner node -2 on
   // sites holding 3+ heads, summed in head order by site_sum instead).
   __device__ __forceinline__ void build_partner_lists() {
     const int N = T.n_dof, ntn = T.n_thick_nodes, nxb = T.nxb;
-    int16_t* __restrict__ nbn = s.nb_node;
-    int16_t* __restrict__ nbh = s.nb_head;
+    int32_t* __restrict__ nb = s.nb;
     for (int i = tid; i < N; i += NT) {
       // three scalar slots (a runtime-indexed array would live in local memory)
       int p0 = -1, p1 = -1, p2 = -1, h0 = 0, h1 = 0, h2 = 0;
@@ -1288,12 +1293,10 @@ struct Sim : SimDyn<DY> {
           }
         }
       }
-      nbn[3 * i] = (int16_t)p0;
-      nbn[3 * i + 1] = (int16_t)p1;
-      nbn[3 * i + 2] = (int16_t)p2;
-      nbh[3 * i] = (int16_t)h0;
-      nbh[3 * i + 1] = (int16_t)h1;
-      nbh[3 * i + 2] = (int16_t)h2;
+      // slot-major: lanes reading consecutive nodes hit distinct banks
+      nb[i] = nb_pack(p0, h0);
+      nb[N + i] = nb_pack(p1, h1);
+      nb[2 * N + i] = nb_pack(p2, h2);
     }
     __syncthreads();
   }
@@ -1306,8 +1309,8 @@ struct Sim : SimDyn<DY> {
     const float* __restrict__ x = s.x;
     float* __restrict__ fxb = s.fxb;
     float* __restrict__ tvec = s.tvec;
-    const int16_t* __restrict__ nbn = s.nb_node;
-    const int16_t* __restrict__ nbh = s.nb_head;
+    const int32_t* __restrict__ nbl = s.nb;
+    const int N = T.n_dof;
     float rad_part = 0.f, jdd_part = 0.f;
     const int any_bad = __syncthreads_or(bad_in);
     if (bad_out) *bad_out = any_bad;
@@ -1367,12 +1370,13 @@ struct Sim : SimDyn<DY> {
           } else {
             const int g = i - ntn;
             float acc = 0.f;
-            const int p0 = nbn[3 * i];
+            const int w0 = nbl[i], w1 = nbl[N + i];
+            const int p0 = nb_node_of(w0);
             if (p0 == -2) {
               acc = site_sum(g, [&](int h) { return fxb[h]; });
             } else {
-              if (p0 >= 0) acc = acc + (-fxb[nbh[3 * i]]);
-              if (nbn[3 * i + 1] >= 0) acc = acc + (-fxb[nbh[3 * i + 1]]);
+              if (p0 >= 0) acc = acc + (-fxb[nb_head_of(w0)]);
+              if (nb_node_of(w1) >= 0) acc = acc + (-fxb[nb_head_of(w1)]);
             }
             double e_j = (xn - xi) + (double)tnc[g];
             if (j + 1 == n) e_j += zoff;
@@ -1436,8 +1440,8 @@ struct Sim : SimDyn<DY> {
     const float* __restrict__ fdd = s.fdd;
     const float* __restrict__ frdd = s.frdd;
     const float* __restrict__ tvec = s.tvec;
-    const int16_t* __restrict__ nbn = s.nb_node;
-    const int16_t* __restrict__ nbh = s.nb_head;
+    const int32_t* __restrict__ nb = s.nb;
+    const int N = T.n_dof;
     const float kth = s.P[THICK_K], ktn = s.P[THIN_K];
     float rad_part = 0.f, dot = 0.f;
     __syncthreads();  // u of every node stored
@@ -1472,7 +1476,7 @@ struct Sim : SimDyn<DY> {
             float xs = 0.f;
 #pragma unroll
             for (int q = 0; q < 3; ++q) {
-              const int pn = nbn[3 * i + q];
+              const int pn = nb_node_of(nb[q * N + i]);
               float wq = 0.f;
               if (pn >= 0) {
                 const int h = i * nxb + q;
@@ -1495,12 +1499,13 @@ struct Sim : SimDyn<DY> {
               return wh;
             };
             float acc = 0.f;
-            const int p0 = nbn[3 * i], p1 = nbn[3 * i + 1];
+            const int w0 = nb[i], w1 = nb[N + i];
+            const int p0 = nb_node_of(w0), p1 = nb_node_of(w1);
             if (p0 == -2) {
               acc = site_sum(i - T.n_thick_nodes, [&](int h) { return head_w(h, us[h / nxb]); });
             } else {
-              if (p0 >= 0) acc = acc + (-head_w(nbh[3 * i], us[p0]));
-              if (p1 >= 0) acc = acc + (-head_w(nbh[3 * i + 1], us[p1]));
+              if (p0 >= 0) acc = acc + (-head_w(nb_head_of(w0), us[p0]));
+              if (p1 >= 0) acc = acc + (-head_w(nb_head_of(w1), us[p1]));
             }
             J = (sj - sm) + acc;
           }
