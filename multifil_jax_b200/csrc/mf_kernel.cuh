@@ -417,7 +417,7 @@ __device__ void run_condition(const StepArgs& A, int ci) {
   {
     const int nf = T.n_thick + T.n_thin;
     m.regcg = PR && A.n_cg > 0 && (A.flags & 64) == 0 && nf <= Sim<NT, PR, DY>::RF * (NT / 32) &&
-              T.n_crowns <= 32 * Sim<NT, PR, DY>::RE && T.n_sites <= 32 * Sim<NT, PR, DY>::RE && T.nxb <= 3;
+              T.n_crowns <= 32 * Sim<NT, PR, DY>::RE && T.n_sites <= 32 * Sim<NT, PR, DY>::RE && T.nxb == 3;
   }
   const int b = m.b;
   const int N = T.n_dof, X = T.total_xbs, S = T.n_sites_total, NTN = T.n_thick_nodes;

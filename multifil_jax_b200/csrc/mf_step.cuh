@@ -149,7 +149,7 @@ struct Smem {
   int16_t* blist; // [X] heads carrying force this step, increasing index
   int16_t* hsite; // [X] global site of a force-carrying head, else -1
   int16_t* site_h;// [2S] first two force-carrying heads of every site (over site)
-  int32_t* nb;      // [3][N] partners of every node (register CG only): low 16 bits the
+  int32_t* nb;      // [N][3] partners of every node (register CG only): low 16 bits the
                     // partner node, high 16 bits the head behind it
   double* face_pos; // [n_thin*3*width] staged candidate positions, NaN = invalid (over site, win2)
   int8_t* face_mono;// [n_thin*3] 0 scan, 1 increasing, 2 decreasing, 3 no candidate
@@ -1231,7 +1231,7 @@ struct Sim : SimDyn<DY> {
   static constexpr int MF_NONFINITE_BIT = 1;
   // ------------------------------------------------------------------
   // Register-resident precise Newton-CG (lattices with at most RF filaments
-  // per warp and filaments of at most 32*RE nodes, crowns of <= 3 heads).
+  // per warp and filaments of at most 32*RE nodes, crowns of 3 heads).
   // Lane l of a warp owns nodes [l*RE, l*RE+RE) of each of its filaments;
   // the CG vectors r, p, s, u, w, dx of those nodes stay in registers for
   // the whole solve, only u (read by the node's neighbours and partners)
@@ -1258,7 +1258,8 @@ struct Sim : SimDyn<DY> {
   // heads, site g -> the crowns of the heads bound to it (partner node -2 on
   // sites holding 3+ heads, summed in head order by site_sum instead).
   __device__ __forceinline__ void build_partner_lists() {
-    const int N = T.n_dof, ntn = T.n_thick_nodes, nxb = T.nxb;
+    const int N = T.n_dof, ntn = T.n_thick_nodes;
+    constexpr int nxb = 3;  // the register path's lattices (three heads per crown)
     int32_t* __restrict__ nb = s.nb;
     for (int i = tid; i < N; i += NT) {
       // three scalar slots (a runtime-indexed array would live in local memory)
@@ -1293,10 +1294,11 @@ struct Sim : SimDyn<DY> {
           }
         }
       }
-      // slot-major: lanes reading consecutive nodes hit distinct banks
-      nb[i] = nb_pack(p0, h0);
-      nb[N + i] = nb_pack(p1, h1);
-      nb[2 * N + i] = nb_pack(p2, h2);
+      // three words per node: lanes owning three consecutive nodes read with
+      // a stride of nine words, which hits 32 distinct banks
+      nb[3 * i] = nb_pack(p0, h0);
+      nb[3 * i + 1] = nb_pack(p1, h1);
+      nb[3 * i + 2] = nb_pack(p2, h2);
     }
     __syncthreads();
   }
@@ -1344,7 +1346,8 @@ struct Sim : SimDyn<DY> {
     const float* __restrict__ thc = T.thick_c;
     const float* __restrict__ tnc = T.thin_c;
     const double zoff = (double)zl - zref;
-    const int ntn = T.n_thick_nodes, nxb = T.nxb;
+    const int ntn = T.n_thick_nodes;
+    constexpr int nxb = 3;
     float fmax = 0.f;
 #pragma unroll
     for (int k = 0; k < RF; ++k) {
@@ -1370,7 +1373,7 @@ struct Sim : SimDyn<DY> {
           } else {
             const int g = i - ntn;
             float acc = 0.f;
-            const int w0 = nbl[i], w1 = nbl[N + i];
+            const int w0 = nbl[3 * i], w1 = nbl[3 * i + 1];
             const int p0 = nb_node_of(w0);
             if (p0 == -2) {
               acc = site_sum(g, [&](int h) { return fxb[h]; });
@@ -1434,7 +1437,8 @@ struct Sim : SimDyn<DY> {
   // w = -J [u, ud] on the lane's nodes; returns (u, w) (augmented) and the
   // block sum of extra_part in *extra, *w_d the radial component.
   __device__ __forceinline__ float jvp_regs(const RVec& u, float ud, RVec& w, float* w_d, float extra_part, float* extra) {
-    const int nthk = T.n_thick, nxb = T.nxb;
+    const int nthk = T.n_thick;
+    constexpr int nxb = 3;
     const float* __restrict__ us = s.zz;
     const float* __restrict__ fdx = s.fdx;
     const float* __restrict__ fdd = s.fdd;
@@ -1476,7 +1480,7 @@ struct Sim : SimDyn<DY> {
             float xs = 0.f;
 #pragma unroll
             for (int q = 0; q < 3; ++q) {
-              const int pn = nb_node_of(nb[q * N + i]);
+              const int pn = nb_node_of(nb[3 * i + q]);
               float wq = 0.f;
               if (pn >= 0) {
                 const int h = i * nxb + q;
@@ -1499,7 +1503,7 @@ struct Sim : SimDyn<DY> {
               return wh;
             };
             float acc = 0.f;
-            const int w0 = nb[i], w1 = nb[N + i];
+            const int w0 = nb[3 * i], w1 = nb[3 * i + 1];
             const int p0 = nb_node_of(w0), p1 = nb_node_of(w1);
             if (p0 == -2) {
               acc = site_sum(i - T.n_thick_nodes, [&](int h) { return head_w(h, us[h / nxb]); });
