@@ -1392,9 +1392,15 @@ struct Sim : SimDyn<DY> {
         r[k][e] = Fv;
       }
     }
+    float m;
+    if constexpr (!DY) {
+      float v[1] = {fmax};
+      reduce<1>(v, true);
+      return v[0];
+    }
     float v[3] = {fmax, rad_part, jdd_part};
     reduce<3>(v, true);
-    float m = v[0];
+    m = v[0];
     if (dyn) {
       const float Fr = -Kl * (d - d_ref) + (-v[1]);
       *frad = Fr;
@@ -1519,6 +1525,12 @@ struct Sim : SimDyn<DY> {
         w[k][e] = o;
       }
     }
+    if constexpr (!DY) {
+      float r2[2] = {dot, extra_part};
+      reduce<2>(r2, false);
+      *extra = r2[1];
+      return r2[0];
+    }
     float r3[3] = {dot, rad_part, extra_part};
     reduce<3>(r3, false);
     *extra = r3[2];
@@ -1535,11 +1547,7 @@ struct Sim : SimDyn<DY> {
     MF_SUB(-1);
     build_partner_lists();
     MF_SUB(5);
-    RVec r, p, sv, u, w, dx;
-#pragma unroll
-    for (int k = 0; k < RF; ++k)
-#pragma unroll
-      for (int e = 0; e < RE; ++e) r[k][e] = p[k][e] = sv[k][e] = u[k][e] = w[k][e] = dx[k][e] = 0.f;
+    RVec r;
     const int n_cg = A.n_cg, n_newton = A.n_newton;
     float frad = 0.f, jdd = 0.f, J_dd_inv = 0.f, fmx = 0.f;
     int it = 0, bad = 0, bad_local = 0;
@@ -1551,34 +1559,14 @@ struct Sim : SimDyn<DY> {
       else if (bad) status |= MF_NONFINITE_BIT;
       it = nw;
       if (!(fmx > tol && nw < n_newton)) break;
-      float r_d = frad, u_d = 0.f, w_d = 0.f, p_d = 0.f, s_d = 0.f, dx_d = 0.f;
-      float alpha = 0.f, gamma = 0.f, gamma_old = 1.f, delta = 0.f;
-      for (int kk = -1; kk < n_cg; ++kk) {
-        if (kk >= 0) {
-          const bool first = kk == 0;
-          float beta = 0.f;
-          if (first) {
-            alpha = gamma / (delta + 1e-30f);
-          } else {
-            beta = gamma / (gamma_old + 1e-30f);
-            alpha = gamma / (delta - beta * gamma / alpha + 1e-30f);
-          }
-#pragma unroll
-          for (int k = 0; k < RF; ++k)
-#pragma unroll
-            for (int e = 0; e < RE; ++e) {
-              p[k][e] = first ? u[k][e] : fmaf(beta, p[k][e], u[k][e]);
-              sv[k][e] = first ? w[k][e] : fmaf(beta, sv[k][e], w[k][e]);
-              dx[k][e] = first ? alpha * p[k][e] : fmaf(alpha, p[k][e], dx[k][e]);
-              r[k][e] = r[k][e] - alpha * sv[k][e];
-            }
-          p_d = first ? u_d : fmaf(beta, p_d, u_d);
-          s_d = first ? w_d : fmaf(beta, s_d, w_d);
-          dx_d = first ? alpha * p_d : fmaf(alpha, p_d, dx_d);
-          r_d = r_d - alpha * s_d;
-          if (kk + 1 == n_cg) break;
-          gamma_old = gamma;
-        }
+      // The CG vectors live within one Newton iteration: the first update is
+      // peeled off the loop so that none of them is live across the
+      // residual evaluation.  n_cg >= 1 on this path.
+      RVec p, sv, u, w, dx;
+      float r_d = frad, u_d = 0.f, w_d = 0.f, p_d, s_d, dx_d;
+      float alpha, gamma = 0.f, gamma_old, delta;
+      // u = M^-1 r, w = -J u and both inner products (one reduction)
+      auto precond_jvp = [&]() {
         MF_SUB(-1);
         const float gpart = precond_regs(r, u);
         MF_SUB(1);
@@ -1587,6 +1575,40 @@ struct Sim : SimDyn<DY> {
         MF_SUB(2);
         if (tid == 0) MF_COUNT(3);
         if (dyn) gamma += r_d * u_d;
+      };
+      precond_jvp();
+      alpha = gamma / (delta + 1e-30f);
+#pragma unroll
+      for (int k = 0; k < RF; ++k)
+#pragma unroll
+        for (int e = 0; e < RE; ++e) {
+          p[k][e] = u[k][e];
+          sv[k][e] = w[k][e];
+          dx[k][e] = alpha * p[k][e];
+          r[k][e] = r[k][e] - alpha * sv[k][e];
+        }
+      p_d = u_d;
+      s_d = w_d;
+      dx_d = alpha * p_d;
+      r_d = r_d - alpha * s_d;
+      for (int kk = 1; kk < n_cg; ++kk) {
+        gamma_old = gamma;
+        precond_jvp();
+        const float beta = gamma / (gamma_old + 1e-30f);
+        alpha = gamma / (delta - beta * gamma / alpha + 1e-30f);
+#pragma unroll
+        for (int k = 0; k < RF; ++k)
+#pragma unroll
+          for (int e = 0; e < RE; ++e) {
+            p[k][e] = fmaf(beta, p[k][e], u[k][e]);
+            sv[k][e] = fmaf(beta, sv[k][e], w[k][e]);
+            dx[k][e] = fmaf(alpha, p[k][e], dx[k][e]);
+            r[k][e] = r[k][e] - alpha * sv[k][e];
+          }
+        p_d = fmaf(beta, p_d, u_d);
+        s_d = fmaf(beta, s_d, w_d);
+        dx_d = fmaf(alpha, p_d, dx_d);
+        r_d = r_d - alpha * s_d;
       }
       // x += dx with non-finite entries zeroed
       bad_local = 0;
