@@ -293,9 +293,8 @@ def plan_batch(topology: SarcTopology, duration_ms: float = 1000.0, dt: float = 
         if isinstance(value, list):
             if not value:
                 raise ValueError(f"{name} sweep list is empty")
-            if all(np.ndim(v) == 0 for v in value):  # scalar sweep: one constant trace per value
-                col = np.asarray(value, dtype=float).astype(np.float32)[:, None]
-                wf_tables[name] = np.repeat(col, n_steps, axis=1)
+            if all(np.ndim(v) == 0 for v in value):  # scalar sweep: one constant per value, broadcast in wave()
+                wf_tables[name] = np.asarray(value, dtype=float).astype(np.float32)[:, None]
             else:
                 rows = [as_trace(v) for v in value]
                 if any(r.shape != (n_steps,) for r in rows):
@@ -356,7 +355,7 @@ def plan_batch(topology: SarcTopology, duration_ms: float = 1000.0, dt: float = 
     def wave(name):
         tab = wf_tables[name]
         if name in wf_sweeps:
-            return tab[flat[name]]
+            return np.broadcast_to(tab[flat[name]], (total, n_steps))
         return np.broadcast_to(tab[0], (total, n_steps))
     z_b = np.ascontiguousarray(wave('z_line'), dtype=np.float32)
     p_b = np.ascontiguousarray(wave('pCa'), dtype=np.float32)
@@ -533,13 +532,14 @@ def run_conditions(conditions: List[dict], *, static_params: Optional[StaticPara
     eng = get_engine(device)
     dev = torch.device('cuda', eng.device)
     flags = (MF_FLAG_DYNAMIC_LS if all(dyn) else 0) | (MF_FLAG_PRECISE if precision == 'mixed' else 0)
-    f = lambda a: torch.as_tensor(a, device=dev)
+    from .engine import upload, to_host
     with torch.cuda.device(dev):
-        res = eng.run_batch(topos, f(P), f(Z), f(PC), f(L), f(np.asarray(steps, np.int32)),
-                            f(KEYS.astype(np.int64)).to(torch.int32), K_lat=f(K), nu=f(NU), dt=f(DT),
+        dP, dZ, dPC, dL, dN, dKY, dK, dNU, dDT = upload(dev, P, Z, PC, L, np.asarray(steps, np.int32),
+                                                        KEYS.view(np.int32), K, NU, DT)
+        res = eng.run_batch(topos, dP, dZ, dPC, dL, dN, dKY, K_lat=dK, nu=dNU, dt=dDT,
                             n_newton=sp.n_newton_steps, n_cg=sp.n_cg_steps, flags=flags, chunk_steps=chunk_steps,
                             residual_warn=sp.solver_residual_tol)
-        m = res['metrics'].cpu().numpy()
+        m = to_host(res['metrics'])
     out = []
     for i, n in enumerate(steps):
         md = MetricsDict()
