@@ -474,7 +474,7 @@ def study_uneven(args):
     """Uneven batch in one launch: default CTA sizes vs the autotuner's."""
     import torch
     from multifil_jax_b200 import run_conditions
-    from multifil_jax_b200.autotune import autotune_many
+    from multifil_jax_b200.autotune import autotune_many, choose_batch_sizes
     conds, topos = uneven_conditions()
     total = sum(int(c['duration_ms']) for c in conds)
     out = {'study': 'uneven', 'metric': METRIC, 'conditions': len(conds), 'condition_timesteps': total,
@@ -492,8 +492,19 @@ def study_uneven(args):
                               '4000 nodes, else 1024')
     t_def = timed()
     tuned = autotune_many(list(topos.values()), precision=args.precision, dynamic_ls=True)
+    # the per-lattice sizes checked on the batch itself (20 steps of it)
+    short = [dict(c, duration_ms=min(float(c['duration_ms']), 20.0)) for c in conds]
+
+    def run_short():
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        run_conditions(short, precision=args.precision)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0
+    kept = choose_batch_sizes(list(topos.values()), tuned, run_short, precision=args.precision)
     t_tuned = timed()
     out['tuned_threads'] = {f'{r}x{c}': v for (r, c), v in sorted(tuned.items())}
+    out['kept_threads'] = {f'{r}x{c}': v for (r, c), v in sorted(kept.items())}
     out['default_value'] = total / t_def
     out['tuned_value'] = total / t_tuned
     out['wall_s'] = {'default': t_def, 'tuned': t_tuned}

@@ -130,8 +130,9 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* batch, void* stream);
  * nodes: 384 threads (precise mode: 256 when the lattice has more than 12
  * filaments); 512 up to 4000 nodes, else 1024; batches with MF_FLAG_DYNAMIC_LS
  * use at least 512 unless the size was set here;
- * multifil_jax_b200.autotune measures and sets the best one.  MF_ERR_INVALID
- * when the lattice does not fit in shared memory at that size. */
+ * multifil_jax_b200.autotune measures and sets the best one; threads = 0
+ * restores the default.  MF_ERR_INVALID when the lattice does not fit in
+ * shared memory at that size. */
 int mf_tune_threads_mode(mf_ctx* ctx, int32_t topo_id, int32_t precise, int32_t threads);
 int mf_tune_threads(mf_ctx* ctx, int32_t topo_id, int32_t threads);
 

@@ -87,3 +87,45 @@ def autotune_many(topologies, n_conditions: int = 256, **kw) -> Dict[Tuple[int, 
         seen.add(k)
         out[(t.nrows, t.ncols)] = autotune(t, n_conditions=n_conditions, **kw)
     return out
+
+
+def choose_batch_sizes(topologies, picks: Dict[Tuple[int, int], int], run_short, precision: str = 'float32',
+                       device: Optional[int] = None, repeats: int = 2) -> Dict[Tuple[int, int], int]:
+    """Check the per-lattice sizes on the batch itself.
+
+    Per-lattice sizes are measured on a batch of one lattice.  In an uneven
+    batch every distinct CTA size becomes its own launch, and several partly
+    filled launches can lose to one fuller launch at a common size.
+    ``run_short()`` runs the actual batch for a few steps and returns its time
+    in seconds.  The per-lattice sizes and the largest of them used for every
+    lattice are both timed, and the faster one is kept.  Returns the kept
+    sizes.
+    """
+    eng = get_engine(device)
+    distinct = {}
+    for t in topologies:
+        distinct.setdefault((t.nrows, t.ncols), t)
+    sizes = {picks[k] for k in distinct if k in picks}
+    if len(sizes) <= 1:
+        return dict(picks)
+
+    def timed():
+        run_short()  # warm-up (graph and allocation of this grouping)
+        return min(run_short() for _ in range(repeats))
+
+    t_per = timed()
+    common = max(sizes)
+    uniform = {}
+    for k, t in distinct.items():
+        try:
+            eng.tune_threads(t, common, precision)
+            uniform[k] = common
+        except Exception:
+            eng.tune_threads(t, picks[k], precision)  # the common size does not fit this lattice
+            uniform[k] = picks[k]
+    t_uni = timed()
+    if t_uni <= t_per:
+        return uniform
+    for k, t in distinct.items():
+        eng.tune_threads(t, picks[k], precision)
+    return dict(picks)

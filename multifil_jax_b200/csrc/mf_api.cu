@@ -281,9 +281,11 @@ int mf_upload_topology(mf_ctx* ctx, const mf_topo_desc* d, int32_t* topo_id) {
 int mf_tune_threads_mode(mf_ctx* ctx, int32_t topo_id, int32_t precise, int32_t threads) {
   if (!ctx || topo_id < 0 || topo_id >= (int)ctx->topos.size())
     return fail(ctx, MF_ERR_NOTFOUND, "unknown topology");
-  if (threads != 128 && threads != 256 && threads != 384 && threads != 512 && threads != 1024)
-    return fail(ctx, MF_ERR_INVALID, "threads must be 128, 256, 384, 512 or 1024");
   TopoHost& t = *ctx->topos[topo_id];
+  const bool reset = threads == 0;  // back to the default (and the dynamic-spacing floor)
+  if (reset) threads = default_threads(t.dev, precise != 0);
+  if (threads != 128 && threads != 256 && threads != 384 && threads != 512 && threads != 1024)
+    return fail(ctx, MF_ERR_INVALID, "threads must be 0, 128, 256, 384, 512 or 1024");
   size_t sm = smem_bytes(t.dev, threads, false, precise != 0);
   bool vg = sm + kStaticSmem > (size_t)ctx->smem_optin;
   sm = smem_bytes(t.dev, threads, vg, precise != 0);
@@ -292,7 +294,7 @@ int mf_tune_threads_mode(mf_ctx* ctx, int32_t topo_id, int32_t precise, int32_t 
   c.threads = threads;
   c.vec_global = vg;
   c.smem_local = sm;
-  c.tuned = true;
+  c.tuned = !reset;
   return MF_OK;
 }
 

@@ -414,6 +414,7 @@ __device__ void run_condition(const StepArgs& A, int ci) {
   m.Tstride = cd.T;
   if (m.tid == 0) carve(m, smem_raw, (A.flags & 64) != 0);
   __syncthreads();
+  m.lazy_tab = DY && m.lazy_tables_fit();
   {
     const int nf = T.n_thick + T.n_thin;
     m.regcg = PR && A.n_cg > 0 && (A.flags & 64) == 0 && nf <= Sim<NT, PR, DY>::RF * (NT / 32) &&
@@ -550,8 +551,17 @@ __device__ void run_condition(const StepArgs& A, int ci) {
         d_kin = ls_t;
       }
       MF_PH(1);
-      // probability tables for (pCa, d_kin)
-      if (!((double)pCa == tab_key[0] && (double)d_kin == tab_key[1])) {
+      // probability tables for (pCa, d_kin); with a dynamic spacing the
+      // crossbridge rows are built after the tropomyosin update instead
+      if (DY && m.lazy_tab) {
+        if ((double)pCa != tab_key[0]) {
+          __syncthreads();
+          m.build_tm_tables(pCa);
+          __syncthreads();
+          if (m.tid == 0) tab_key[0] = pCa;
+          __syncthreads();
+        }
+      } else if (!((double)pCa == tab_key[0] && (double)d_kin == tab_key[1])) {
         __syncthreads();
         m.build_tables(pCa, d_kin, true, false);
         __syncthreads();
@@ -587,6 +597,7 @@ __device__ void run_condition(const StepArgs& A, int ci) {
       const size_t inj_t = ((size_t)b * A.T + t) * (size_t)S;
       const size_t inj_x = ((size_t)b * A.T + t) * (size_t)X;
       m.thin_step(sub_thin, inj_t);
+      if (DY && m.lazy_tab) m.build_needed_tables(pCa, d_kin, false);
       MF_PH(5);
       m.thick_step(sub_thick, inj_x);
       MF_PH(6);
@@ -624,7 +635,9 @@ __device__ void run_condition(const StepArgs& A, int ci) {
     const float new_ls = m.dyn ? d : ls_t;
     if (m.tid == 0) ls_s = new_ls;
     // absorbing table for the metrics at (pCa, new_ls)
-    if (!((double)pCa == tab_key[2] && (double)new_ls == tab_key[3])) {
+    if (DY && m.lazy_tab) {
+      m.build_needed_tables(pCa, new_ls, true);
+    } else if (!((double)pCa == tab_key[2] && (double)new_ls == tab_key[3])) {
       __syncthreads();
       m.build_tables(pCa, new_ls, false, true);
       __syncthreads();

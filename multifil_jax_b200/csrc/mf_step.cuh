@@ -188,10 +188,14 @@ __host__ __device__ inline CoefLayout coef_layout(const TopoDev& t) {
 // the three absorbing-chain entries the metrics read ("absorbing", global).
 // Out of line: it runs only when pCa or the spacing changes, and its
 // unrolled Pade arithmetic would otherwise sit in the step loop's code.
+// tm: the 27 tropomyosin tables; sampling / absorbing: the crossbridge
+// tables of every key, or with `keys` only the nkeys listed ones (of the one
+// kind selected).
 static __device__ __noinline__ void build_tables_block(const float* P, const float* centers, int nb, float pCa, float d,
                                                 float dtm, int sq64, float* cum_tm, float* cum_xb, float* pabs,
-                                                bool sampling, bool absorbing, int tid, int nt) {
-  if (sampling) {
+                                                bool tm, bool sampling, bool absorbing, const int16_t* keys,
+                                                int nkeys, int tid, int nt) {
+  if (tm) {
     for (int m = tid; m < 27; m += nt) {
       float Q[16];
       tm_generator(P, pCa, m, Q);
@@ -200,10 +204,10 @@ static __device__ __noinline__ void build_tables_block(const float* P, const flo
       for (int r = 0; r < 4; ++r) cum4(Q + 4 * r, cum_tm + m * 16 + 4 * r);
     }
   }
-  const int nwork = (sampling ? 2 * nb : 0) + (absorbing ? 2 * nb : 0);
+  const int nwork = keys ? nkeys : (sampling ? 2 * nb : 0) + (absorbing ? 2 * nb : 0);
   for (int w = tid; w < nwork; w += nt) {
-    const bool is_abs = !sampling || w >= 2 * nb;
-    const int key = is_abs && sampling ? w - 2 * nb : w;
+    const bool is_abs = keys ? absorbing : (!sampling || w >= 2 * nb);
+    const int key = keys ? (int)keys[w] : (is_abs && sampling ? w - 2 * nb : w);
     const int bin = key % nb;
     const float perm = key >= nb ? 1.0f : 0.0f;
     float Q[36];
@@ -254,6 +258,7 @@ struct Sim : SimDyn<DY> {
   static constexpr bool precise = PR;
   bool part;
   bool regcg;   // register-resident precise Newton-CG (solve_regs)
+  bool lazy_tab;  // dynamic spacing: build only the crossbridge table rows the heads read
   float Kl, nu_c, dtm;
   double zref;  // precise mode thin reference z
   float dvar;   // lattice spacing unknown (dynamic) / fixed spacing
@@ -1645,8 +1650,71 @@ struct Sim : SimDyn<DY> {
   // ------------------------------------------------------------------
   __device__ void build_tables(float pCa, float d, bool sampling, bool absorbing) {
     build_tables_block(s.P, T.centers, T.n_bins, pCa, d, dtm, A.sq64_from, s.cum_tm,
-                       reinterpret_cast<float*>(ws + L.cum_xb), s.pabs, sampling,
-                       absorbing, tid, NT);
+                       reinterpret_cast<float*>(ws + L.cum_xb), s.pabs, sampling, sampling,
+                       absorbing, nullptr, 0, tid, NT);
+  }
+  // the tropomyosin tables alone (they do not depend on the spacing)
+  __device__ void build_tm_tables(float pCa) {
+    build_tables_block(s.P, T.centers, T.n_bins, pCa, 0.f, dtm, A.sq64_from, s.cum_tm,
+                       reinterpret_cast<float*>(ws + L.cum_xb), s.pabs, true, false, false, nullptr, 0,
+                       tid, NT);
+  }
+
+  // Dynamic spacing rebuilds the crossbridge tables every step.  Only the
+  // rows some head reads are built: the sampling keys of all heads (after
+  // the tropomyosin update, thick_step's keys) or the absorbing keys of the
+  // heads the metrics read (old state 2 or 3).  Flags and the sorted key list
+  // live in the CG vector pv, which is free outside the solve.
+  __device__ bool lazy_tables_fit() const {
+    const int nk = 2 * T.n_bins, nwords = (nk + 31) >> 5;
+    return 4 * (nwords + 1) + 2 * nk <= 4 * T.n_dof;
+  }
+  __device__ void build_needed_tables(float pCa, float d, bool absorbing) {
+    const int nk = 2 * T.n_bins, nwords = (nk + 31) >> 5, X = T.total_xbs;
+    uint32_t* bits = reinterpret_cast<uint32_t*>(s.pv);
+    int* count = reinterpret_cast<int*>(bits + nwords);
+    int16_t* list = reinterpret_cast<int16_t*>(count + 1);
+    __syncthreads();
+    for (int w = tid; w < nwords; w += NT) bits[w] = 0u;
+    __syncthreads();
+    for (int i = tid; i < X; i += NT) {
+      int key = -1;
+      if (!absorbing) {
+        key = sample_key(i);
+      } else {
+        const int so = s.old_xbs[i];
+        if (so == 2 || so == 3) key = s.old_key[i];
+      }
+      if (key >= 0) atomicOr(&bits[key >> 5], 1u << (key & 31));
+    }
+    __syncthreads();
+    if (warp == 0) {
+      int base = 0;
+      for (int c = 0; c < nwords; c += 32) {
+        const int wi = c + lane;
+        uint32_t wb = wi < nwords ? bits[wi] : 0u;
+        const int n = __popc(wb);
+        int incl = n;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += v;
+        }
+        int off = base + incl - n;
+        while (wb) {
+          list[off++] = (int16_t)(wi * 32 + __ffs(wb) - 1);
+          wb &= wb - 1u;
+        }
+        base += __shfl_sync(0xffffffffu, incl, 31);
+      }
+      if (lane == 0) *count = base;
+    }
+    __syncthreads();
+    const int nkeys = *count;
+    build_tables_block(s.P, T.centers, T.n_bins, pCa, d, dtm, A.sq64_from, s.cum_tm,
+                       reinterpret_cast<float*>(ws + L.cum_xb), s.pabs, false, !absorbing, absorbing, list,
+                       nkeys, tid, NT);
+    __syncthreads();
   }
 
   // ------------------------------------------------------------------
@@ -1799,6 +1867,18 @@ struct Sim : SimDyn<DY> {
     if (x != x) dg = nb + 1;                  // NaN: digitize puts it past the last edge
     int bin = dg - 1;
     return bin < 0 ? 0 : (bin > nb - 1 ? nb - 1 : bin);
+  }
+
+  // Table key of head i at the current geometry: permissiveness of its
+  // nearest site (tropomyosin state 3 and a valid head) and the bin of its
+  // axial offset (transitions.py:807-922).
+  __device__ __forceinline__ int sample_key(int i) const {
+    const int nsi = T.n_sites;
+    const int thin = thin_of(i);
+    const int near = s.xb_near[i];
+    const int site = near < 0 ? 0 : (near > nsi - 1 ? nsi - 1 : near);
+    const bool perm = (s.tm[thin * nsi + site] == 3) && T.xb_valid[i];
+    return (perm ? T.n_bins : 0) + bin_of(s.xb_ax[i]);
   }
 
   __device__ void thick_step(const uint32_t* sub, size_t inj_off) {

@@ -233,7 +233,8 @@ class Engine:
         return up
 
     def tune_threads(self, topo, threads: int, precision: Optional[str] = None):
-        """Set the CTA size of a lattice for one precision mode, or both when None."""
+        """Set the CTA size of a lattice for one precision mode, or both when None
+        (0: back to the library's default)."""
         up = self.upload(topo)
         if precision is None:
             self._check(self.lib.mf_tune_threads(self.h, up.topo_id, int(threads)), 'mf_tune_threads')

@@ -13,6 +13,7 @@ results come back shaped ``(sweep_1, ..., replicates, time)``.
 """
 from __future__ import annotations
 
+import time
 import warnings
 from dataclasses import dataclass, field
 from typing import Dict, List, Optional, Tuple, Union
@@ -526,13 +527,27 @@ def run_conditions(conditions: List[dict], *, static_params: Optional[StaticPara
         DT[i] = float(c.get('dt', 1.0))
         KEYS[i] = np.asarray(c['key'], np.uint32) if c.get('key') is not None else default_keys[i]
     topos = [c['topology'] for c in conditions]
-    if autotune:
-        from .autotune import autotune_many
-        autotune_many(topos, precision=precision, device=device, dynamic_ls=all(dyn))
     eng = get_engine(device)
     dev = torch.device('cuda', eng.device)
     flags = (MF_FLAG_DYNAMIC_LS if all(dyn) else 0) | (MF_FLAG_PRECISE if precision == 'mixed' else 0)
     from .engine import upload, to_host
+    if autotune:
+        from .autotune import autotune_many, choose_batch_sizes
+        picks = autotune_many(topos, precision=precision, device=device, dynamic_ls=all(dyn))
+        Ts = min(T, 20)  # the batch itself, a few steps long
+
+        def run_short():
+            with torch.cuda.device(dev):
+                a = upload(dev, P, Z[:, :Ts], PC[:, :Ts], L[:, :Ts], np.minimum(np.asarray(steps, np.int32), Ts),
+                           KEYS.view(np.int32), K, NU, DT)
+                torch.cuda.synchronize(dev)
+                t0 = time.perf_counter()
+                eng.run_batch(topos, *a[:6], K_lat=a[6], nu=a[7], dt=a[8], n_newton=sp.n_newton_steps,
+                              n_cg=sp.n_cg_steps, flags=flags, chunk_steps=chunk_steps,
+                              residual_warn=sp.solver_residual_tol)
+                torch.cuda.synchronize(dev)
+                return time.perf_counter() - t0
+        choose_batch_sizes(topos, picks, run_short, precision=precision, device=device)
     with torch.cuda.device(dev):
         dP, dZ, dPC, dL, dN, dKY, dK, dNU, dDT = upload(dev, P, Z, PC, L, np.asarray(steps, np.int32),
                                                         KEYS.view(np.int32), K, NU, DT)

@@ -224,3 +224,25 @@ def test_run_conditions_matches_run_per_condition():
     assert np.array_equal(ref.metrics['lattice_spacing'].reshape(-1), dyn[0]['lattice_spacing'])
     with pytest.raises(ValueError):
         run_conditions([dict(topology=t22, duration_ms=5, K_lat=5.0), dict(topology=t11, duration_ms=5)])
+
+
+def test_run_conditions_autotune():
+    """run_conditions(autotune=True): per-lattice sizes checked on the batch itself;
+    the results agree with the default sizes' (same draws; reduction orders differ)."""
+    from multifil_jax_b200 import run_conditions
+    from multifil_jax_b200.engine import get_engine
+    s, d = get_skeletal_params()
+    tops = [SarcTopology.create(r, k, s, d) for r, k in ((1, 1), (2, 1), (2, 2))]
+    conds = [dict(topology=t, duration_ms=12, pCa=4.5 + 0.5 * i, K_lat=5.0, nu=0.5)
+             for i, t in enumerate(tops * 3)]
+    ref = run_conditions(conds, precision='mixed')
+    try:
+        got = run_conditions(conds, precision='mixed', autotune=True)
+    finally:
+        eng = get_engine()
+        for t in tops:
+            eng.tune_threads(t, 0, 'mixed')
+    for r, g in zip(ref, got):
+        assert np.all(np.isfinite(g['axial_force']))
+        np.testing.assert_allclose(g['axial_force'], r['axial_force'], rtol=1e-2, atol=5.0)
+        np.testing.assert_allclose(g['lattice_spacing'], r['lattice_spacing'], rtol=1e-3)
