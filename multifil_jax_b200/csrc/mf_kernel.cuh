@@ -500,7 +500,13 @@ __device__ void run_condition(const StepArgs& A, int ci) {
     __syncthreads();
   }
 
-  __shared__ uint32_t sub_thin[2], sub_thick[2];
+  // Sub-keys of step t in slot t & 1.  The keys of step t + 1 are derived
+  // during step t by the CTA's last thread, which has the fewest sites in
+  // the tropomyosin update (keys_ready), so the serial Threefry chain leaves
+  // the start of the step; otherwise thread 0 derives them there.
+  __shared__ uint32_t sub_thin[2][2], sub_thick[2][2];
+  __shared__ int keys_ready;
+  if (m.tid == 0) keys_ready = 0;
   // Drivers (z, pCa, ls) of step t in drv[t & 1].  Thread 0 copies those of
   // step t + 1 with cp.async during step t: their latency overlaps a whole
   // step, and no register holds them (or the driver pointers) across the
@@ -577,13 +583,16 @@ __device__ void run_condition(const StepArgs& A, int ci) {
         m.s.old_xbs[i] = m.s.xb_state[i];
         m.s.old_key[i] = m.s.xb_key[i];
       }
-      __syncthreads();
       if (m.tid == 0) {
-        uint32_t kn[2];
-        step_keys(m.part, key_s[0], key_s[1], sub_thin, sub_thick, kn);
-        key_s[0] = kn[0];
-        key_s[1] = kn[1];
+        if (!keys_ready) {
+          uint32_t kn[2];
+          step_keys(m.part, key_s[0], key_s[1], sub_thin[t & 1], sub_thick[t & 1], kn);
+          key_s[0] = kn[0];
+          key_s[1] = kn[1];
+        }
+        keys_ready = 0;
       }
+      __syncthreads();
       MF_PH(3);
     }
     // 2-4. kinetics
@@ -596,10 +605,18 @@ __device__ void run_condition(const StepArgs& A, int ci) {
     } else {
       const size_t inj_t = ((size_t)b * A.T + t) * (size_t)S;
       const size_t inj_x = ((size_t)b * A.T + t) * (size_t)X;
-      m.thin_step(sub_thin, inj_t);
+      m.thin_step(sub_thin[t & 1], inj_t, [&]() {
+        if (m.tid == NT - 1 && t + 1 < t1) {
+          uint32_t kn[2];
+          step_keys(m.part, key_s[0], key_s[1], sub_thin[(t + 1) & 1], sub_thick[(t + 1) & 1], kn);
+          key_s[0] = kn[0];
+          key_s[1] = kn[1];
+          keys_ready = 1;
+        }
+      });
       if (DY && m.lazy_tab) m.build_needed_tables(pCa, d_kin, false);
       MF_PH(5);
-      m.thick_step(sub_thick, inj_x);
+      m.thick_step(sub_thick[t & 1], inj_x);
       MF_PH(6);
     }
     // 5. mechanics

@@ -1824,7 +1824,10 @@ struct Sim : SimDyn<DY> {
     return bits_to_uniform(bits32(part, key[0], key[1], (uint32_t)n, (uint32_t)i));
   }
 
-  __device__ void thin_step(const uint32_t* sub, size_t inj_off) {
+  // after_loop: run by every thread once its sites are sampled, before the
+  // update is published (work for threads with fewer sites)
+  template <class Fn>
+  __device__ void thin_step(const uint32_t* sub, size_t inj_off, Fn&& after_loop) {
     const int S = T.n_sites_total;
     for (int g = tid; g < S; g += NT) {
       const int t = g / T.n_sites;
@@ -1848,6 +1851,7 @@ struct Sim : SimDyn<DY> {
       }
       s.tm_new[g] = (int8_t)ns;
     }
+    after_loop();
     __syncthreads();
     for (int g = tid; g < S; g += NT) s.tm[g] = s.tm_new[g];
     __syncthreads();
