@@ -1248,7 +1248,7 @@ struct Sim : SimDyn<DY> {
   // ------------------------------------------------------------------
   // RF filaments per warp: one at 384 threads (a 2x2 lattice has 12 filaments
   // for 12 warps), two otherwise
-  static constexpr int RE = 3, RF = NT == 384 ? 1 : 2;
+  static constexpr int RE = 3, RF = NT == 384 ? 1 : (NT == 512 ? 3 : 2);
   using RVec = float[RF][RE];
 
   __device__ __forceinline__ bool slot(int k, int& base, int& n, int& f, bool& thick) const {
