@@ -24,8 +24,12 @@ namespace {
 struct Cfg {
   int threads = 0;          // CTA size
   bool vec_global = false;  // CG vectors and head terms in the workspace
+  bool regs = false;        // register-resident CG layout (x and u only in shared memory)
   size_t smem_local = 0;    // dynamic shared memory at that size
   bool tuned = false;       // set through mf_tune_threads[_mode]
+  // launch grouping key and kernel layout flags
+  int group_key() const { return threads * 4 + (vec_global ? 1 : 0) + (regs ? 2 : 0); }
+  int layout_flags() const { return (vec_global ? FLAG_VEC_GLOBAL : 0) | (regs ? FLAG_REGS : 0); }
 };
 
 struct TopoHost {
@@ -110,22 +114,38 @@ static int default_threads(const TopoDev& t, bool precise) {
   return 1024;
 }
 
+// Configuration of a lattice at nt threads: the register layout where the
+// register-resident CG covers the lattice (precise mode, allow_regs: batches
+// with n_cg > 0), else every CG vector in shared memory, else in the
+// workspace.  false when even that does not fit.
+static bool make_cfg(const TopoDev& t, int nt, bool precise, bool allow_regs, int smem_optin, Cfg& c) {
+  c.threads = nt;
+  if (precise && allow_regs && regcg_fits(t, nt)) {
+    const size_t sm = smem_bytes(t, nt, LAYOUT_REGS, true);
+    if (sm + kStaticSmem <= (size_t)smem_optin) {
+      c.regs = true;
+      c.vec_global = false;
+      c.smem_local = sm;
+      return true;
+    }
+  }
+  c.regs = false;
+  c.vec_global = smem_bytes(t, nt, LAYOUT_SMEM, precise) + kStaticSmem > (size_t)smem_optin;
+  c.smem_local = smem_bytes(t, nt, c.vec_global ? LAYOUT_GLOBAL : LAYOUT_SMEM, precise);
+  return c.smem_local + kStaticSmem <= (size_t)smem_optin;
+}
+
 // The configuration a batch uses.  With the lattice spacing solved as an
 // unknown both transition tables (827 matrix exponentials) are rebuilt every
 // step, one matrix per thread: an untuned default below 512 threads is raised
 // to 512 (measured fastest for every lattice of 1x1 to 4x4 in that mode).
-static Cfg batch_cfg(const TopoHost& t, int pm, bool dyn, int smem_optin) {
+static Cfg batch_cfg(const TopoHost& t, int pm, bool dyn, int n_cg, int smem_optin) {
   Cfg c = t.cfg[pm];
   if (dyn && !c.tuned && c.threads < 512) {
-    size_t sm = smem_bytes(t.dev, 512, false, pm != 0);
-    const bool vg = sm + kStaticSmem > (size_t)smem_optin;
-    const size_t need = smem_bytes(t.dev, 512, vg, pm != 0);
-    if (need + kStaticSmem <= (size_t)smem_optin) {
-      c.threads = 512;
-      c.vec_global = vg;
-      c.smem_local = need;
-    }
+    Cfg c5 = c;
+    if (make_cfg(t.dev, 512, pm != 0, true, smem_optin, c5)) c = c5;
   }
+  if (c.regs && n_cg <= 0) make_cfg(t.dev, c.threads, pm != 0, false, smem_optin, c);  // no CG: no register layout
   return c;
 }
 
@@ -264,11 +284,7 @@ int mf_upload_topology(mf_ctx* ctx, const mf_topo_desc* d, int32_t* topo_id) {
   CK(cudaMemcpy(t->d_struct, &td, sizeof(TopoDev), cudaMemcpyHostToDevice));
   for (int p = 0; p < 2; ++p) {
     Cfg& c = t->cfg[p];
-    c.threads = default_threads(td, p != 0);
-    size_t sm = smem_bytes(td, c.threads, false, p != 0);
-    c.vec_global = sm + kStaticSmem > (size_t)ctx->smem_optin;
-    c.smem_local = smem_bytes(td, c.threads, c.vec_global, p != 0);
-    if (c.smem_local + kStaticSmem > (size_t)ctx->smem_optin)
+    if (!make_cfg(td, default_threads(td, p != 0), p != 0, true, ctx->smem_optin, c))
       return fail(ctx, MF_ERR_INVALID, "lattice needs %zu B shared memory (limit %d)", c.smem_local,
                   ctx->smem_optin);
   }
@@ -286,15 +302,11 @@ int mf_tune_threads_mode(mf_ctx* ctx, int32_t topo_id, int32_t precise, int32_t 
   if (reset) threads = default_threads(t.dev, precise != 0);
   if (threads != 128 && threads != 256 && threads != 384 && threads != 512 && threads != 1024)
     return fail(ctx, MF_ERR_INVALID, "threads must be 0, 128, 256, 384, 512 or 1024");
-  size_t sm = smem_bytes(t.dev, threads, false, precise != 0);
-  bool vg = sm + kStaticSmem > (size_t)ctx->smem_optin;
-  sm = smem_bytes(t.dev, threads, vg, precise != 0);
-  if (sm + kStaticSmem > (size_t)ctx->smem_optin) return fail(ctx, MF_ERR_INVALID, "does not fit");
-  Cfg& c = t.cfg[precise ? 1 : 0];
-  c.threads = threads;
-  c.vec_global = vg;
-  c.smem_local = sm;
+  Cfg c;
+  if (!make_cfg(t.dev, threads, precise != 0, true, ctx->smem_optin, c))
+    return fail(ctx, MF_ERR_INVALID, "does not fit");
   c.tuned = !reset;
+  t.cfg[precise ? 1 : 0] = c;
   return MF_OK;
 }
 
@@ -410,8 +422,8 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
   const bool dynb = (bt->flags & MF_FLAG_DYNAMIC_LS) != 0;
   auto key_of = [&](int i) {
     const TopoHost& t = *ctx->topos[bt->topo_id[i]];
-    const Cfg c = batch_cfg(t, pm, dynb, ctx->smem_optin);
-    return std::make_pair(c.threads * 2 + (c.vec_global ? 1 : 0), -(long)n_steps[i] * t.dev.n_dof);
+    const Cfg c = batch_cfg(t, pm, dynb, bt->n_cg, ctx->smem_optin);
+    return std::make_pair(c.group_key(), -(long)n_steps[i] * t.dev.n_dof);
   };
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key_of(a) < key_of(b); });
   off = 0;
@@ -445,14 +457,14 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
   int T = 0;
   for (int i = 0; i < B; ++i) T = std::max(T, n_steps[i]);
   // groups
-  struct Group { int begin, end, threads; bool vg; size_t smem; };
+  struct Group { int begin, end, threads, key, lflags; size_t smem; };
   std::vector<Group> groups;
   for (int k = 0; k < B;) {
-    const Cfg c0 = batch_cfg(*ctx->topos[bt->topo_id[order[k]]], pm, dynb, ctx->smem_optin);
-    Group g{k, k, c0.threads, c0.vec_global, 0};
+    const Cfg c0 = batch_cfg(*ctx->topos[bt->topo_id[order[k]]], pm, dynb, bt->n_cg, ctx->smem_optin);
+    Group g{k, k, c0.threads, c0.group_key(), c0.layout_flags(), 0};
     while (g.end < B) {
-      const Cfg ck = batch_cfg(*ctx->topos[bt->topo_id[order[g.end]]], pm, dynb, ctx->smem_optin);
-      if (ck.threads != g.threads || ck.vec_global != g.vg) break;
+      const Cfg ck = batch_cfg(*ctx->topos[bt->topo_id[order[g.end]]], pm, dynb, bt->n_cg, ctx->smem_optin);
+      if (ck.group_key() != g.key) break;
       g.smem = std::max(g.smem, ck.smem_local);
       ++g.end;
     }
@@ -483,7 +495,7 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
     CK(cudaMemcpyAsync(ctx->d_cond, rows.data(), sizeof(CondDesc) * rows.size(), cudaMemcpyHostToDevice, st));
     for (auto& lr : launches) {
       const Group& g = groups[lr.second];
-      StepArgs a = make_args(bt, ctx->d_cond, base_flags | (g.vg ? 64 : 0), max_dof, max_x, max_s);
+      StepArgs a = make_args(bt, ctx->d_cond, base_flags | g.lflags, max_dof, max_x, max_s);
       cudaError_t e = launch(g.threads, a, 1, lr.first, g.smem, st);
       if (e != cudaSuccess) return fail(ctx, MF_ERR_CUDA, "plain launch: %s", cudaGetErrorString(e));
     }
@@ -523,7 +535,7 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
   }
   for (int c = 0; c < n_chunks; ++c) {
     for (const Group& g : groups) {
-      StepArgs a = make_args(bt, ctx->d_cond + (size_t)c * B, base_flags | (g.vg ? 64 : 0), max_dof,
+      StepArgs a = make_args(bt, ctx->d_cond + (size_t)c * B, base_flags | g.lflags, max_dof,
                              max_x, max_s);
       cudaError_t e = launch(g.threads, a, g.end - g.begin, g.begin, g.smem, launch_st);
       if (e != cudaSuccess) {
@@ -635,8 +647,8 @@ int mf_run_batch_static(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
   const bool dynb = (bt->flags & MF_FLAG_DYNAMIC_LS) != 0;
   auto key_of = [&](int i) {
     const TopoHost& t = *ctx->topos[bt->topo_id[i]];
-    const Cfg c = batch_cfg(t, pm, dynb, ctx->smem_optin);
-    return std::make_pair(c.threads * 2 + (c.vec_global ? 1 : 0), -(long)n_steps[i] * t.dev.n_dof);
+    const Cfg c = batch_cfg(t, pm, dynb, bt->n_cg, ctx->smem_optin);
+    return std::make_pair(c.group_key(), -(long)n_steps[i] * t.dev.n_dof);
   };
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key_of(a) < key_of(b); });
   CondDesc* d_desc = reinterpret_cast<CondDesc*>(base);
@@ -678,16 +690,16 @@ int mf_run_batch_static(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
   if (bt->flags & MF_FLAG_PRECISE) flags |= FLAG_PRECISE;
   if (bt->flags & MF_FLAG_ORIGINAL_PRNG) flags |= FLAG_ORIG_PRNG;
   for (int k = 0; k < B;) {
-    const Cfg c0 = batch_cfg(*ctx->topos[bt->topo_id[order[k]]], pm, dynb, ctx->smem_optin);
+    const Cfg c0 = batch_cfg(*ctx->topos[bt->topo_id[order[k]]], pm, dynb, bt->n_cg, ctx->smem_optin);
     int e = k;
     size_t smem = 0;
     while (e < B) {
-      const Cfg ck = batch_cfg(*ctx->topos[bt->topo_id[order[e]]], pm, dynb, ctx->smem_optin);
-      if (ck.threads != c0.threads || ck.vec_global != c0.vec_global) break;
+      const Cfg ck = batch_cfg(*ctx->topos[bt->topo_id[order[e]]], pm, dynb, bt->n_cg, ctx->smem_optin);
+      if (ck.group_key() != c0.group_key()) break;
       smem = std::max(smem, ck.smem_local);
       ++e;
     }
-    StepArgs a = make_args(bt, d_desc, flags | (c0.vec_global ? 64 : 0), max_dof, max_x, max_s);
+    StepArgs a = make_args(bt, d_desc, flags | c0.layout_flags(), max_dof, max_x, max_s);
     cudaError_t err = launch(c0.threads, a, e - k, k, smem, st);
     if (err != cudaSuccess) return fail(ctx, MF_ERR_CUDA, "static launch: %s", cudaGetErrorString(err));
     k = e;

@@ -13,6 +13,8 @@ constexpr int kNParams = 44;
 constexpr int kNMetrics = 52;
 // per-warp partials of the metrics' fused block reduction (one per lane)
 constexpr int kRedPartials = 32;
+// filaments per warp of the register-resident precise CG at nt threads
+__host__ __device__ constexpr int regcg_rf(int nt) { return nt == 384 ? 1 : (nt == 512 ? 3 : 2); }
 constexpr int kMaxLevels = 12;
 
 // DynamicParams field indices (reference core/params.py:73-556 order).

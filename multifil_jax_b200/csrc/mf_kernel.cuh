@@ -27,11 +27,26 @@ __host__ __device__ inline size_t site_region_bytes(const TopoDev& t) {
 // force broadcast.
 __host__ __device__ constexpr int red_floats(int nw) { return kRedPartials * nw + 2 * 96 + 1; }
 
+// Where the CG vectors and head terms of a condition live (kernel flag bits
+// 64 and 128).  LAYOUT_SMEM: all in shared memory; LAYOUT_GLOBAL: in the
+// workspace (lattices too large for shared memory); LAYOUT_REGS: the
+// register-resident CG, which keeps only x and u in shared memory.
+enum Layout { LAYOUT_SMEM = 0, LAYOUT_GLOBAL = 1, LAYOUT_REGS = 2 };
+constexpr int FLAG_VEC_GLOBAL = 64, FLAG_REGS = 128;
+
+// Whether the register-resident precise CG covers this lattice at nt threads
+// (regcg_rf filaments per warp, 3 nodes per lane, crowns of 3 heads).
+__host__ __device__ inline bool regcg_fits(const TopoDev& t, int nt) {
+  const int rf = regcg_rf(nt), re = 3;
+  return t.n_thick + t.n_thin <= rf * (nt / 32) && t.n_crowns <= 32 * re && t.n_sites <= 32 * re && t.nxb == 3;
+}
+
 // Shared-memory bytes of one condition of this lattice with nt threads in one
-// precision mode (mirrors carve() below: every array both modes use, plus
-// the float32 scan-reversal buffers or the precise-mode CG vectors w, s and
-// the partner lists).
-__host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, bool vec_global, bool precise) {
+// precision mode and layout (mirrors carve() below: every array both modes
+// use, plus the float32 scan-reversal buffers or the precise-mode CG vectors
+// w, s and the partner lists).
+__host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, int layout, bool precise) {
+  const bool vec_global = layout == LAYOUT_GLOBAL;
   const int N = t.n_dof, X = t.total_xbs, S = t.n_sites_total;
   const int nw = nt / 32;
   const CoefLayout cl = coef_layout(t);
@@ -39,7 +54,8 @@ __host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, bool vec_
   auto add = [&](size_t bytes) { o = align_up(o + bytes, 16); };
   add(sizeof(double) * 64);                // redd
   add(sizeof(float) * red_floats(nw));     // red
-  if (!vec_global) add(sizeof(float) * (precise ? 7 : 5) * N);  // x r dx pv zz (+ wv sv)
+  if (layout == LAYOUT_REGS) add(sizeof(float) * 2 * N);  // x zz
+  else if (!vec_global) add(sizeof(float) * (precise ? 7 : 5) * N);  // x r dx pv zz (+ wv sv)
   if (!vec_global) add(sizeof(float) * 4 * X);  // fxb fdx fdd frdd
   add(sizeof(float) * X);                  // xb_ax
   add(site_region_bytes(t));               // site / win1 | win2, overlaid by face_pos and site_h
@@ -69,19 +85,28 @@ __host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, bool vec_
 }
 
 template <int NT, bool PR, bool DY>
-__device__ void carve(Sim<NT, PR, DY>& m, char* base, bool vec_global) {
+__device__ void carve(Sim<NT, PR, DY>& m, char* base, int layout) {
   const TopoDev& t = m.T;
   const int N = t.n_dof, X = t.total_xbs, S = t.n_sites_total;
+  const bool vec_global = layout == LAYOUT_GLOBAL;
   size_t o = 0;
   auto take = [&](size_t bytes) { char* p = base + o; o = align_up(o + bytes, 16); return p; };
   m.s.redd = (double*)take(sizeof(double) * 64);
   m.s.red = (float*)take(sizeof(float) * red_floats(NT / 32));
   // the workspace keeps room for all seven vectors; shared memory only for
   // the ones this mode uses
-  float* v7 = vec_global ? reinterpret_cast<float*>(m.ws + m.L.vec) : (float*)take(sizeof(float) * (PR ? 7 : 5) * N);
-  m.s.x = v7; m.s.r = v7 + N; m.s.dx = v7 + 2 * N; m.s.pv = v7 + 3 * N; m.s.zz = v7 + 4 * N;
-  m.s.wv = PR ? v7 + 5 * N : nullptr;
-  m.s.sv = PR ? v7 + 6 * N : nullptr;
+  if (layout == LAYOUT_REGS) {
+    float* v2 = (float*)take(sizeof(float) * 2 * N);
+    m.s.x = v2;
+    m.s.zz = v2 + N;
+    m.s.r = m.s.dx = m.s.wv = m.s.sv = nullptr;
+    m.s.pv = m.s.zz;  // only the table-key list uses pv outside a smem CG; u is free then
+  } else {
+    float* v7 = vec_global ? reinterpret_cast<float*>(m.ws + m.L.vec) : (float*)take(sizeof(float) * (PR ? 7 : 5) * N);
+    m.s.x = v7; m.s.r = v7 + N; m.s.dx = v7 + 2 * N; m.s.pv = v7 + 3 * N; m.s.zz = v7 + 4 * N;
+    m.s.wv = PR ? v7 + 5 * N : nullptr;
+    m.s.sv = PR ? v7 + 6 * N : nullptr;
+  }
   float* f4 = vec_global ? reinterpret_cast<float*>(m.ws + m.L.vec) + 7 * N : (float*)take(sizeof(float) * 4 * X);
   m.s.fxb = f4; m.s.fdx = f4 + X; m.s.fdd = f4 + 2 * X; m.s.frdd = f4 + 3 * X;
   m.s.xb_ax = (float*)take(sizeof(float) * X);
@@ -412,14 +437,13 @@ __device__ void run_condition(const StepArgs& A, int ci) {
   m.part = (A.flags & FLAG_ORIG_PRNG) == 0;
   m.status = 0;
   m.Tstride = cd.T;
-  if (m.tid == 0) carve(m, smem_raw, (A.flags & 64) != 0);
+  const int layout = (A.flags & FLAG_VEC_GLOBAL) ? LAYOUT_GLOBAL : ((A.flags & FLAG_REGS) ? LAYOUT_REGS : LAYOUT_SMEM);
+  if (m.tid == 0) carve(m, smem_raw, layout);
   __syncthreads();
   m.lazy_tab = DY && m.lazy_tables_fit();
-  {
-    const int nf = T.n_thick + T.n_thin;
-    m.regcg = PR && A.n_cg > 0 && (A.flags & 64) == 0 && nf <= Sim<NT, PR, DY>::RF * (NT / 32) &&
-              T.n_crowns <= 32 * Sim<NT, PR, DY>::RE && T.n_sites <= 32 * Sim<NT, PR, DY>::RE && T.nxb == 3;
-  }
+  // the host sets FLAG_REGS exactly when regcg_fits, n_cg > 0 and the
+  // precise mode hold (the register layout has no room for the other CG)
+  m.regcg = PR && layout == LAYOUT_REGS;
   const int b = m.b;
   const int N = T.n_dof, X = T.total_xbs, S = T.n_sites_total, NTN = T.n_thick_nodes;
   // Workspace arrays of this condition, formed where they are used (launch

@@ -1246,9 +1246,9 @@ struct Sim : SimDyn<DY> {
   // dependent index chains.  Same Chronopoulos-Gear recurrences as
   // solve_cg_gear.
   // ------------------------------------------------------------------
-  // RF filaments per warp: one at 384 threads (a 2x2 lattice has 12 filaments
-  // for 12 warps), two otherwise
-  static constexpr int RE = 3, RF = NT == 384 ? 1 : (NT == 512 ? 3 : 2);
+  // RF filaments per warp (regcg_rf): one at 384 threads (a 2x2 lattice has
+  // 12 filaments for 12 warps), three at 512 (3x3: 33, 4x4: 48), two otherwise
+  static constexpr int RE = 3, RF = regcg_rf(NT);
   using RVec = float[RF][RE];
 
   __device__ __forceinline__ bool slot(int k, int& base, int& n, int& f, bool& thick) const {
