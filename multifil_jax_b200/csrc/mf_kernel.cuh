@@ -163,7 +163,7 @@ __device__ void carve(Sim<NT, PR, DY>& m, char* base, int layout) {
 // transposed exchange and meet at a single barrier.  After it every warp
 // forms the totals from the per-warp partials and stores its share of the
 // 18 output groups (group q = lane * NW + warp), so no warp carries the
-// whole epilogue.  The axial force is summed in filament order by thread 0
+// whole epilogue.  The axial force is summed in filament order by one thread
 // during the partial pass and handed over through the same barrier.
 template <int NT, bool PR, bool DY>
 __device__ void metrics(Sim<NT, PR, DY>& m, int t, float zl, float pCa, float new_ls, double resid, int iters,
@@ -192,8 +192,10 @@ __device__ void metrics(Sim<NT, PR, DY>& m, int t, float zl, float pCa, float ne
 #else
 #define MF_MT(k) do { } while (0)
 #endif
-  if (tid == 0) {
-    // axial force: sum over thick filaments in filament order
+  if (tid == NT - 1 - T.n_thick) {
+    // axial force: sum over thick filaments in filament order, on a thread
+    // with the lightest share of the loops below (the energies take the
+    // last n_thick threads)
     float force = 0.f;
     for (int th = 0; th < T.n_thick; ++th) {
       const int n0 = th * T.n_crowns;

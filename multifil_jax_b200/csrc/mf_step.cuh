@@ -797,8 +797,12 @@ struct Sim : SimDyn<DY> {
     const int c = s.win2[g];
     float acc = 0.f;
     if (c < 3) {
-      if (c >= 1) acc = acc + (-val((int)s.site_h[2 * g]));
-      if (c >= 2) acc = acc + (-val((int)s.site_h[2 * g + 1]));
+      // two heads in head order: their slots come from an atomic counter, and
+      // a contracted multiply-add of the second term is not symmetric
+      int h0 = s.site_h[2 * g], h1 = s.site_h[2 * g + 1];
+      if (c >= 2 && h1 < h0) { const int tmp = h0; h0 = h1; h1 = tmp; }
+      if (c >= 1) acc = acc + (-val(h0));
+      if (c >= 2) acc = acc + (-val(h1));
       return acc;
     }
     const int nb = *s.nbound;
@@ -836,13 +840,15 @@ struct Sim : SimDyn<DY> {
         jdd_part += frd;
       }
     }
-    if (tid < nthk) {
+    // titin on the last threads: the bound heads above fill the first ones
+    if (NT - 1 - tid < nthk) {
+      const int th = NT - 1 - tid;
       float ax, a_x, a_d, r_d, rad;
-      titin(tid, zl, d, ax, a_x, a_d, r_d, rad);
-      tvec[tid] = ax;
-      tvec[nthk + tid] = a_x;
-      tvec[2 * nthk + tid] = a_d;
-      tvec[3 * nthk + tid] = r_d;
+      titin(th, zl, d, ax, a_x, a_d, r_d, rad);
+      tvec[th] = ax;
+      tvec[nthk + th] = a_x;
+      tvec[2 * nthk + th] = a_d;
+      tvec[3 * nthk + th] = r_d;
       if (dyn) {
         rad_part += rad;
         jdd_part += r_d;
@@ -1289,12 +1295,15 @@ struct Sim : SimDyn<DY> {
         if (c >= 3) {
           p0 = -2;
         } else {
+          // heads in head order (their slots come from an atomic counter)
           if (c >= 1) {
             h0 = s.site_h[2 * g];
             p0 = h0 / nxb;
           }
           if (c >= 2) {
             h1 = s.site_h[2 * g + 1];
+            if (h1 < h0) { const int tmp = h0; h0 = h1; h1 = tmp; }
+            p0 = h0 / nxb;
             p1 = h1 / nxb;
           }
         }
@@ -1334,13 +1343,15 @@ struct Sim : SimDyn<DY> {
         jdd_part += frd;
       }
     }
-    if (tid < nthk) {
+    // titin on the last threads: the bound heads above fill the first ones
+    if (NT - 1 - tid < nthk) {
+      const int th = NT - 1 - tid;
       float ax, a_x, a_d, r_d, rad;
-      titin(tid, zl, d, ax, a_x, a_d, r_d, rad);
-      tvec[tid] = ax;
-      tvec[nthk + tid] = a_x;
-      tvec[2 * nthk + tid] = a_d;
-      tvec[3 * nthk + tid] = r_d;
+      titin(th, zl, d, ax, a_x, a_d, r_d, rad);
+      tvec[th] = ax;
+      tvec[nthk + th] = a_x;
+      tvec[2 * nthk + th] = a_d;
+      tvec[3 * nthk + th] = r_d;
       if (dyn) {
         rad_part += rad;
         jdd_part += r_d;

@@ -246,3 +246,27 @@ def test_run_conditions_autotune():
         assert np.all(np.isfinite(g['axial_force']))
         np.testing.assert_allclose(g['axial_force'], r['axial_force'], rtol=1e-2, atol=5.0)
         np.testing.assert_allclose(g['lattice_spacing'], r['lattice_spacing'], rtol=1e-3)
+
+
+def test_identical_conditions_identical_results():
+    """Copies of one condition in one launch give bit-identical metrics.  Sites
+    holding two heads sum them in head order: their slots come from an atomic
+    counter, and a contracted multiply-add is not symmetric in its terms (a
+    4x4 mixed run split into two result classes at step 19 before)."""
+    from multifil_jax_b200.engine import get_engine
+    from tests.gpu_helpers import run_engine
+    s, d = get_skeletal_params()
+    topo = SarcTopology.create(4, 4, s, d)
+    eng = get_engine()
+    B, T = 48, 60
+    key = prng.split(prng.PRNGKey(1005), 1)[0]
+    for nt in (0, 1024):
+        eng.tune_threads(topo, nt, 'mixed')
+        try:
+            m = run_engine(eng, topo, np.repeat(d.param_row()[None], B, 0), np.full((B, T), 930.0),
+                           np.full((B, T), 5.0), np.full((B, T), 14.0), np.repeat(key[None], B, 0),
+                           flags=MF_FLAG_PRECISE)['metrics']
+        finally:
+            eng.tune_threads(topo, 0, 'mixed')
+        for b in range(1, B):
+            assert np.array_equal(m[b], m[0]), (nt, b)
