@@ -258,13 +258,14 @@ def test_identical_conditions_identical_results():
     s, d = get_skeletal_params()
     topo = SarcTopology.create(4, 4, s, d)
     eng = get_engine()
-    B, T = 48, 60
-    key = prng.split(prng.PRNGKey(1005), 1)[0]
+    # the condition that showed it: pCa 4.0045, z 996.02 nm, key split(PRNGKey(1004), 1)[0]
+    B, T = 48, 57
+    key = prng.split(prng.PRNGKey(1004), 1)[0]
     for nt in (0, 1024):
         eng.tune_threads(topo, nt, 'mixed')
         try:
-            m = run_engine(eng, topo, np.repeat(d.param_row()[None], B, 0), np.full((B, T), 930.0),
-                           np.full((B, T), 5.0), np.full((B, T), 14.0), np.repeat(key[None], B, 0),
+            m = run_engine(eng, topo, np.repeat(d.param_row()[None], B, 0), np.full((B, T), 996.0190412149619),
+                           np.full((B, T), 4.004470250526508), np.full((B, T), 14.0), np.repeat(key[None], B, 0),
                            flags=MF_FLAG_PRECISE)['metrics']
         finally:
             eng.tune_threads(topo, 0, 'mixed')
