@@ -118,10 +118,10 @@ static int default_threads(const TopoDev& t, bool precise) {
 // register-resident CG covers the lattice (precise mode, allow_regs: batches
 // with n_cg > 0), else every CG vector in shared memory, else in the
 // workspace.  false when even that does not fit.
-static bool make_cfg(const TopoDev& t, int nt, bool precise, bool allow_regs, int smem_optin, Cfg& c) {
+static bool make_cfg(const TopoDev& t, int nt, bool precise, bool allow_regs, bool dyn, int smem_optin, Cfg& c) {
   c.threads = nt;
   if (precise && allow_regs && regcg_fits(t, nt)) {
-    const size_t sm = smem_bytes(t, nt, LAYOUT_REGS, true);
+    const size_t sm = smem_bytes(t, nt, LAYOUT_REGS, true, dyn);
     if (sm + kStaticSmem <= (size_t)smem_optin) {
       c.regs = true;
       c.vec_global = false;
@@ -130,8 +130,8 @@ static bool make_cfg(const TopoDev& t, int nt, bool precise, bool allow_regs, in
     }
   }
   c.regs = false;
-  c.vec_global = smem_bytes(t, nt, LAYOUT_SMEM, precise) + kStaticSmem > (size_t)smem_optin;
-  c.smem_local = smem_bytes(t, nt, c.vec_global ? LAYOUT_GLOBAL : LAYOUT_SMEM, precise);
+  c.vec_global = smem_bytes(t, nt, LAYOUT_SMEM, precise, dyn) + kStaticSmem > (size_t)smem_optin;
+  c.smem_local = smem_bytes(t, nt, c.vec_global ? LAYOUT_GLOBAL : LAYOUT_SMEM, precise, dyn);
   return c.smem_local + kStaticSmem <= (size_t)smem_optin;
 }
 
@@ -140,12 +140,18 @@ static bool make_cfg(const TopoDev& t, int nt, bool precise, bool allow_regs, in
 // step, one matrix per thread: an untuned default below 512 threads is raised
 // to 512 (measured fastest for every lattice of 1x1 to 4x4 in that mode).
 static Cfg batch_cfg(const TopoHost& t, int pm, bool dyn, int n_cg, int smem_optin) {
-  Cfg c = t.cfg[pm];
+  Cfg c = t.cfg[pm];  // sized for a dynamic spacing (the larger carve)
   if (dyn && !c.tuned && c.threads < 512) {
     Cfg c5 = c;
-    if (make_cfg(t.dev, 512, pm != 0, true, smem_optin, c5)) c = c5;
+    if (make_cfg(t.dev, 512, pm != 0, true, true, smem_optin, c5)) c = c5;
   }
-  if (c.regs && n_cg <= 0) make_cfg(t.dev, c.threads, pm != 0, false, smem_optin, c);  // no CG: no register layout
+  // the exact carve of this batch: no register layout without CG steps, no
+  // spacing derivatives with a fixed spacing
+  Cfg e = c;
+  if (make_cfg(t.dev, c.threads, pm != 0, n_cg > 0, dyn, smem_optin, e)) {
+    e.tuned = c.tuned;
+    c = e;
+  }
   return c;
 }
 
@@ -284,7 +290,7 @@ int mf_upload_topology(mf_ctx* ctx, const mf_topo_desc* d, int32_t* topo_id) {
   CK(cudaMemcpy(t->d_struct, &td, sizeof(TopoDev), cudaMemcpyHostToDevice));
   for (int p = 0; p < 2; ++p) {
     Cfg& c = t->cfg[p];
-    if (!make_cfg(td, default_threads(td, p != 0), p != 0, true, ctx->smem_optin, c))
+    if (!make_cfg(td, default_threads(td, p != 0), p != 0, true, true, ctx->smem_optin, c))
       return fail(ctx, MF_ERR_INVALID, "lattice needs %zu B shared memory (limit %d)", c.smem_local,
                   ctx->smem_optin);
   }
@@ -303,7 +309,7 @@ int mf_tune_threads_mode(mf_ctx* ctx, int32_t topo_id, int32_t precise, int32_t 
   if (threads != 128 && threads != 256 && threads != 384 && threads != 512 && threads != 1024)
     return fail(ctx, MF_ERR_INVALID, "threads must be 0, 128, 256, 384, 512 or 1024");
   Cfg c;
-  if (!make_cfg(t.dev, threads, precise != 0, true, ctx->smem_optin, c))
+  if (!make_cfg(t.dev, threads, precise != 0, true, true, ctx->smem_optin, c))
     return fail(ctx, MF_ERR_INVALID, "does not fit");
   c.tuned = !reset;
   t.cfg[precise ? 1 : 0] = c;

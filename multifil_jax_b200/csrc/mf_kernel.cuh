@@ -42,10 +42,10 @@ __host__ __device__ inline bool regcg_fits(const TopoDev& t, int nt) {
 }
 
 // Shared-memory bytes of one condition of this lattice with nt threads in one
-// precision mode and layout (mirrors carve() below: every array both modes
-// use, plus the float32 scan-reversal buffers or the precise-mode CG vectors
-// w, s and the partner lists).
-__host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, int layout, bool precise) {
+// precision mode, layout and spacing mode (mirrors carve() below: every array
+// both modes use, plus the float32 scan-reversal buffers or the precise-mode
+// CG vectors w and s, and the per-head spacing derivatives when dyn).
+__host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, int layout, bool precise, bool dyn) {
   const bool vec_global = layout == LAYOUT_GLOBAL;
   const int N = t.n_dof, X = t.total_xbs, S = t.n_sites_total;
   const int nw = nt / 32;
@@ -56,7 +56,7 @@ __host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, int layou
   add(sizeof(float) * red_floats(nw));     // red
   if (layout == LAYOUT_REGS) add(sizeof(float) * 2 * N);  // x zz
   else if (!vec_global) add(sizeof(float) * (precise ? 7 : 5) * N);  // x r dx pv zz (+ wv sv)
-  if (!vec_global) add(sizeof(float) * 4 * X);  // fxb fdx fdd frdd
+  if (!vec_global) add(sizeof(float) * (dyn ? 4 : 2) * X);  // fxb fdx (+ fdd frdd)
   add(sizeof(float) * X);                  // xb_ax
   add(site_region_bytes(t));               // site / win1 | win2, overlaid by face_pos and site_h
   add(sizeof(int16_t) * 2 * X);            // xb_bound xb_near
@@ -73,8 +73,7 @@ __host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, int layou
   add(sizeof(int) * 4);                    // nbound
   add(sizeof(int) * 32);                   // wsum
   add(sizeof(int16_t) * X);                // xb_key
-  add(sizeof(int16_t) * X);                // hsite
-  if (!vec_global && precise) add(sizeof(int32_t) * 3 * N);  // nb
+  add(sizeof(int) * X);                    // hsite
   add(3 * t.n_thin * 3);                   // face_mono face_kl face_kh
   if (!vec_global) {                       // old-state snapshot
     add(sizeof(float) * t.n_thick_nodes);
@@ -107,8 +106,11 @@ __device__ void carve(Sim<NT, PR, DY>& m, char* base, int layout) {
     m.s.wv = PR ? v7 + 5 * N : nullptr;
     m.s.sv = PR ? v7 + 6 * N : nullptr;
   }
-  float* f4 = vec_global ? reinterpret_cast<float*>(m.ws + m.L.vec) + 7 * N : (float*)take(sizeof(float) * 4 * X);
-  m.s.fxb = f4; m.s.fdx = f4 + X; m.s.fdd = f4 + 2 * X; m.s.frdd = f4 + 3 * X;
+  // fxb fdx, and fdd frdd only in dynamic-spacing kernels (the workspace keeps room for all four)
+  float* f4 = vec_global ? reinterpret_cast<float*>(m.ws + m.L.vec) + 7 * N : (float*)take(sizeof(float) * (DY ? 4 : 2) * X);
+  m.s.fxb = f4; m.s.fdx = f4 + X;
+  m.s.fdd = (DY || vec_global) ? f4 + 2 * X : nullptr;
+  m.s.frdd = (DY || vec_global) ? f4 + 3 * X : nullptr;
   m.s.xb_ax = (float*)take(sizeof(float) * X);
   {
     char* reg = take(site_region_bytes(t));
@@ -133,15 +135,10 @@ __device__ void carve(Sim<NT, PR, DY>& m, char* base, int layout) {
   m.s.nbound = (int*)take(sizeof(int) * 4);
   m.s.wsum = (int*)take(sizeof(int) * 32);
   m.s.xb_key = (int16_t*)take(sizeof(int16_t) * X);
-  m.s.hsite = (int16_t*)take(sizeof(int16_t) * X);
+  m.s.hsite = (int*)take(sizeof(int) * X);
   m.s.face_mono = (int8_t*)take(3 * t.n_thin * 3);
   m.s.face_kl = m.s.face_mono + t.n_thin * 3;
   m.s.face_kh = m.s.face_kl + t.n_thin * 3;
-  if (!vec_global && PR) {
-    m.s.nb = (int32_t*)take(sizeof(int32_t) * 3 * N);
-  } else {
-    m.s.nb = nullptr;
-  }
   if (!vec_global) {
     m.s.old_thick = (float*)take(sizeof(float) * t.n_thick_nodes);
     m.s.old_xbs = (int8_t*)take(X);

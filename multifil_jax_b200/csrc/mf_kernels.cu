@@ -15,12 +15,31 @@
 namespace mf {
 
 cudaError_t MF_NAME(prepare_, MF_NT, MF_P, MF_D)(size_t smem) {
+  auto* kernel = step_kernel<MF_NT, (MF_P != 0), (MF_D != 0)>;
   static size_t attr_bytes = 0;
   if (smem > attr_bytes) {
-    cudaError_t e = cudaFuncSetAttribute(step_kernel<MF_NT, (MF_P != 0), (MF_D != 0)>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attr_bytes = smem;
+  }
+  // Shared-memory carve-out: just what the register-limited occupancy needs
+  // (static and driver-reserved bytes included), so the rest of the SM's
+  // 256 KB stays L1, where the spilled registers live.
+  static int sm_bytes = 0, last_pct = -1;
+  if (!sm_bytes) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+        sm_bytes <= 0)
+      sm_bytes = 233472;
+  }
+  const size_t need = (size_t)min_ctas(MF_NT) * (smem + kStaticSmem + 1024);
+  int pct = (int)((need * 100 + sm_bytes - 1) / (size_t)sm_bytes);
+  pct = pct > 100 ? 100 : pct;
+  if (pct != last_pct) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+    if (e != cudaSuccess) return e;
+    last_pct = pct;
   }
   return cudaSuccess;
 }

@@ -55,12 +55,6 @@ struct StepArgs {
 
 constexpr int FLAG_DYN = 1, FLAG_PRECISE = 2, FLAG_ORIG_PRNG = 4;
 
-// Partner-list words: the partner node (int16, -1 none, -2 a site holding
-// three or more heads) in the low half, the head behind it in the high half.
-__device__ __forceinline__ int nb_pack(int node, int head) { return (int)((uint32_t)(uint16_t)node | ((uint32_t)head << 16)); }
-__device__ __forceinline__ int nb_node_of(int w) { return (int)(int16_t)(w & 0xffff); }
-__device__ __forceinline__ int nb_head_of(int w) { return (int)((uint32_t)w >> 16); }
-
 // 4-byte asynchronous global -> shared copy (no register holds the value)
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
@@ -147,10 +141,10 @@ struct Smem {
   float* fdd;     // [X] df/dd per head (dynamic spacing)
   float* frdd;    // [X] d(radial)/dd per head (dynamic spacing)
   int16_t* blist; // [X] heads carrying force this step, increasing index
-  int16_t* hsite; // [X] global site of a force-carrying head, else -1
+  int* hsite;     // [X] global site of a force-carrying head, else -1 (int32: the JVP reads
+                  // three per node with a nine-word lane stride, free of bank conflicts)
   int16_t* site_h;// [2S] first two force-carrying heads of every site (over site)
-  int32_t* nb;      // [N][3] partners of every node (register CG only): low 16 bits the
-                    // partner node, high 16 bits the head behind it
+
   double* face_pos; // [n_thin*3*width] staged candidate positions, NaN = invalid (over site, win2)
   int8_t* face_mono;// [n_thin*3] 0 scan, 1 increasing, 2 decreasing, 3 no candidate
   int8_t* face_kl;  // [n_thin*3] first valid candidate
@@ -770,7 +764,7 @@ struct Sim : SimDyn<DY> {
           const int k = atomicAdd(&cnt[gs], 1);
           if (k < 2) site_h[2 * gs + k] = (int16_t)i;
         }
-        s.hsite[i] = (int16_t)gs;
+        s.hsite[i] = gs;
       }
       const unsigned m = __ballot_sync(0xffffffffu, f);
       if (lane == 0) s.wsum[warp] = __popc(m);
@@ -786,6 +780,16 @@ struct Sim : SimDyn<DY> {
       __syncthreads();
     }
     if (tid == 0) *s.nbound = base;
+    // the two heads of a site in head order (their slots came from the
+    // atomic counter; a contracted multiply-add of the second term is not
+    // symmetric, so the sums over them need one fixed order)
+    uint32_t* pairs = reinterpret_cast<uint32_t*>(site_h);
+    for (int g = tid; g < S; g += NT) {
+      if (cnt[g] == 2) {
+        const uint32_t w = pairs[g];
+        if ((w >> 16) < (w & 0xffffu)) pairs[g] = (w >> 16) | (w << 16);
+      }
+    }
     __syncthreads();
   }
 
@@ -797,10 +801,9 @@ struct Sim : SimDyn<DY> {
     const int c = s.win2[g];
     float acc = 0.f;
     if (c < 3) {
-      // two heads in head order: their slots come from an atomic counter, and
-      // a contracted multiply-add of the second term is not symmetric
-      int h0 = s.site_h[2 * g], h1 = s.site_h[2 * g + 1];
-      if (c >= 2 && h1 < h0) { const int tmp = h0; h0 = h1; h1 = tmp; }
+      // site_h[2g], site_h[2g+1] in one word, in head order (build_bound_list)
+      const uint32_t pair = reinterpret_cast<const uint32_t*>(s.site_h)[g];
+      const int h0 = (int)(pair & 0xffffu), h1 = (int)(pair >> 16);
       if (c >= 1) acc = acc + (-val(h0));
       if (c >= 2) acc = acc + (-val(h1));
       return acc;
@@ -922,7 +925,7 @@ struct Sim : SimDyn<DY> {
     const float* __restrict__ fdx = s.fdx;
     const float* __restrict__ fdd = s.fdd;
     const float* __restrict__ frdd = s.frdd;
-    const int16_t* __restrict__ hsite = s.hsite;
+    const int* __restrict__ hsite = s.hsite;
     const float* __restrict__ tvec = s.tvec;
     const float kth = s.P[THICK_K], ktn = s.P[THIN_K];
     float rad_part = 0.f, dot = 0.f;
@@ -1265,58 +1268,6 @@ struct Sim : SimDyn<DY> {
     return f < T.n_thick + T.n_thin;
   }
 
-  // Partner lists of every node for this step: crown i -> the sites of its
-  // heads, site g -> the crowns of the heads bound to it (partner node -2 on
-  // sites holding 3+ heads, summed in head order by site_sum instead).
-  __device__ __forceinline__ void build_partner_lists() {
-    const int N = T.n_dof, ntn = T.n_thick_nodes;
-    constexpr int nxb = 3;  // the register path's lattices (three heads per crown)
-    int32_t* __restrict__ nb = s.nb;
-    for (int i = tid; i < N; i += NT) {
-      // three scalar slots (a runtime-indexed array would live in local memory)
-      int p0 = -1, p1 = -1, p2 = -1, h0 = 0, h1 = 0, h2 = 0;
-      if (i < ntn) {
-        h0 = i * nxb;
-        h1 = h0 + 1;
-        h2 = h0 + 2;
-        const int g0 = s.hsite[h0];
-        if (g0 >= 0) p0 = ntn + g0;
-        if (nxb > 1) {
-          const int g1 = s.hsite[h1];
-          if (g1 >= 0) p1 = ntn + g1;
-        }
-        if (nxb > 2) {
-          const int g2 = s.hsite[h2];
-          if (g2 >= 0) p2 = ntn + g2;
-        }
-      } else {
-        const int g = i - ntn;
-        const int c = s.win2[g];
-        if (c >= 3) {
-          p0 = -2;
-        } else {
-          // heads in head order (their slots come from an atomic counter)
-          if (c >= 1) {
-            h0 = s.site_h[2 * g];
-            p0 = h0 / nxb;
-          }
-          if (c >= 2) {
-            h1 = s.site_h[2 * g + 1];
-            if (h1 < h0) { const int tmp = h0; h0 = h1; h1 = tmp; }
-            p0 = h0 / nxb;
-            p1 = h1 / nxb;
-          }
-        }
-      }
-      // three words per node: lanes owning three consecutive nodes read with
-      // a stride of nine words, which hits 32 distinct banks
-      nb[3 * i] = nb_pack(p0, h0);
-      nb[3 * i + 1] = nb_pack(p1, h1);
-      nb[3 * i + 2] = nb_pack(p2, h2);
-    }
-    __syncthreads();
-  }
-
   // F(x) of the lane's nodes into r (float64 accumulation, as residual());
   // returns max|F| over the augmented vector.
   __device__ __forceinline__ float residual_regs(float zl, float d, float* frad, float* jdd, int bad_in, int* bad_out, RVec& r) {
@@ -1325,8 +1276,6 @@ struct Sim : SimDyn<DY> {
     const float* __restrict__ x = s.x;
     float* __restrict__ fxb = s.fxb;
     float* __restrict__ tvec = s.tvec;
-    const int32_t* __restrict__ nbl = s.nb;
-    const int N = T.n_dof;
     float rad_part = 0.f, jdd_part = 0.f;
     const int any_bad = __syncthreads_or(bad_in);
     if (bad_out) *bad_out = any_bad;
@@ -1389,14 +1338,7 @@ struct Sim : SimDyn<DY> {
           } else {
             const int g = i - ntn;
             float acc = 0.f;
-            const int w0 = nbl[3 * i], w1 = nbl[3 * i + 1];
-            const int p0 = nb_node_of(w0);
-            if (p0 == -2) {
-              acc = site_sum(g, [&](int h) { return fxb[h]; });
-            } else {
-              if (p0 >= 0) acc = acc + (-fxb[nb_head_of(w0)]);
-              if (nb_node_of(w1) >= 0) acc = acc + (-fxb[nb_head_of(w1)]);
-            }
+            acc = site_sum(g, [&](int h) { return fxb[h]; });
             double e_j = (xn - xi) + (double)tnc[g];
             if (j + 1 == n) e_j += zoff;
             const double e_m = j > 0 ? (xi - xm) + (double)tnc[g - 1] : 0.0;
@@ -1466,8 +1408,8 @@ struct Sim : SimDyn<DY> {
     const float* __restrict__ fdd = s.fdd;
     const float* __restrict__ frdd = s.frdd;
     const float* __restrict__ tvec = s.tvec;
-    const int32_t* __restrict__ nb = s.nb;
-    const int N = T.n_dof;
+    const int* __restrict__ hsite = s.hsite;
+    const int ntn = T.n_thick_nodes;
     const float kth = s.P[THICK_K], ktn = s.P[THIN_K];
     float rad_part = 0.f, dot = 0.f;
     __syncthreads();  // u of every node stored
@@ -1502,10 +1444,11 @@ struct Sim : SimDyn<DY> {
             float xs = 0.f;
 #pragma unroll
             for (int q = 0; q < 3; ++q) {
-              const int pn = nb_node_of(nb[3 * i + q]);
+              const int h = i * nxb + q;
+              const int gq = hsite[h];
               float wq = 0.f;
-              if (pn >= 0) {
-                const int h = i * nxb + q;
+              if (gq >= 0) {
+                const int pn = ntn + gq;
                 const float dxd = us[pn] - vi;
                 wq = fdx[h] * dxd;
                 if (dyn) {
@@ -1524,15 +1467,7 @@ struct Sim : SimDyn<DY> {
               if (dyn) wh = wh + fdd[h] * ud;
               return wh;
             };
-            float acc = 0.f;
-            const int w0 = nb[3 * i], w1 = nb[3 * i + 1];
-            const int p0 = nb_node_of(w0), p1 = nb_node_of(w1);
-            if (p0 == -2) {
-              acc = site_sum(i - T.n_thick_nodes, [&](int h) { return head_w(h, us[h / nxb]); });
-            } else {
-              if (p0 >= 0) acc = acc + (-head_w(nb_head_of(w0), us[p0]));
-              if (p1 >= 0) acc = acc + (-head_w(nb_head_of(w1), us[p1]));
-            }
+            const float acc = site_sum(i - ntn, [&](int h) { return head_w(h, us[h / nxb]); });
             J = (sj - sm) + acc;
           }
           o = -J;
@@ -1560,9 +1495,6 @@ struct Sim : SimDyn<DY> {
 
   __device__ __forceinline__ void solve_regs(float zl, float& d, double& resid, int& iters, bool dyn_jdd) {
     const float tol = fmaxf(s.P[SOLVER_TOL], fmaxf(s.P[THICK_K] * 1e-4f, 0.25f));
-    MF_SUB(-1);
-    build_partner_lists();
-    MF_SUB(5);
     RVec r;
     const int n_cg = A.n_cg, n_newton = A.n_newton;
     float frad = 0.f, jdd = 0.f, J_dd_inv = 0.f, fmx = 0.f;
