@@ -591,10 +591,18 @@ __device__ void run_condition(const StepArgs& A, int ci) {
           __syncthreads();
         }
       } else if (!((double)pCa == tab_key[0] && (double)d_kin == tab_key[1])) {
+        // with a fixed spacing the metrics' absorbing table has the same
+        // (pCa, spacing) key: both are built in one pass over the CTA's
+        // threads (fewer partly filled rounds of one matrix per thread)
+        const bool abs_too = !DY && !((double)pCa == tab_key[2] && (double)d_kin == tab_key[3]);
         __syncthreads();
-        m.build_tables(pCa, d_kin, true, false);
+        m.build_tables(pCa, d_kin, true, abs_too);
         __syncthreads();
-        if (m.tid == 0) { tab_key[0] = pCa; tab_key[1] = d_kin; }
+        if (m.tid == 0) {
+          tab_key[0] = pCa;
+          tab_key[1] = d_kin;
+          if (abs_too) { tab_key[2] = pCa; tab_key[3] = d_kin; }
+        }
         __threadfence_block();
         __syncthreads();
       }
