@@ -134,3 +134,39 @@ def test_params_api():
     assert s.replace(n_cg_steps=3).n_cg_steps == 3
     with pytest.raises(ValueError):
         StaticParams(n_superlattice_classes=2)
+
+
+def test_choose_batch_sizes_keeps_the_faster_set(monkeypatch):
+    """The batch-level check of the autotuner: per-lattice sizes against the
+    largest of them for every lattice, timed by run_short, faster set kept
+    and left set in the engine (host logic only, with a stand-in engine)."""
+    from types import SimpleNamespace
+    from multifil_jax_b200 import autotune
+
+    class FakeEngine:
+        def __init__(self):
+            self.sizes = {}
+
+        def tune_threads(self, topo, threads, precision=None):
+            if threads == 1024 and topo.nrows == 4:
+                raise RuntimeError('does not fit')
+            self.sizes[(topo.nrows, topo.ncols)] = threads
+
+    eng = FakeEngine()
+    monkeypatch.setattr(autotune, 'get_engine', lambda device=None: eng)
+    tops = [SimpleNamespace(nrows=1, ncols=1), SimpleNamespace(nrows=2, ncols=2), SimpleNamespace(nrows=4, ncols=4)]
+    picks = {(1, 1): 256, (2, 2): 384, (4, 4): 512}
+
+    def timer(uniform_faster):
+        def run_short():
+            uniform = len(set(eng.sizes.values())) == 1
+            return 1.0 if uniform == uniform_faster else 2.0
+        return run_short
+
+    kept = autotune.choose_batch_sizes(tops, picks, timer(True), precision='mixed')
+    assert kept == {(1, 1): 512, (2, 2): 512, (4, 4): 512} and eng.sizes == kept
+    eng.sizes = dict(picks)
+    kept = autotune.choose_batch_sizes(tops, picks, timer(False), precision='mixed')
+    assert kept == picks and eng.sizes == picks
+    # one size already: nothing to compare
+    assert autotune.choose_batch_sizes(tops[:1], {(1, 1): 256}, timer(True)) == {(1, 1): 256}
