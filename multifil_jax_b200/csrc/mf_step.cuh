@@ -67,11 +67,6 @@ __device__ __forceinline__ float warp_sum(float v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
-__device__ __forceinline__ double warp_sum_d(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
 // Transposed warp reduction of 32 values per lane: after it lane l holds the
 // warp total of value l (max for l < NMAX, sum otherwise).  Each of the five
 // exchange steps halves the values a lane keeps, so it takes 31 shuffles
@@ -96,16 +91,6 @@ __device__ __forceinline__ float warp_reduce_transposed(float (&v)[32], int lane
 __device__ __forceinline__ float warp_max(float v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-  return v;
-}
-__device__ __forceinline__ float warp_min(float v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
-  return v;
-}
-__device__ __forceinline__ int warp_sum_i(int v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
 
@@ -285,94 +270,6 @@ struct Sim : SimDyn<DY> {
   // ------------------------------------------------------------------
   // reductions
   // ------------------------------------------------------------------
-  __device__ float bsum(float v) {
-    v = warp_sum(v);
-    __syncthreads();
-    if (lane == 0) s.red[warp] = v;
-    __syncthreads();
-    float t = 0.f;
-    for (int w = 0; w < NW; ++w) t += s.red[w];
-    return t;
-  }
-  __device__ double bsum_d(double v) {
-    v = warp_sum_d(v);
-    __syncthreads();
-    if (lane == 0) s.redd[warp] = v;
-    __syncthreads();
-    double t = 0.0;
-    for (int w = 0; w < NW; ++w) t += s.redd[w];
-    return t;
-  }
-  __device__ float bmax(float v) {
-    v = warp_max(v);
-    __syncthreads();
-    if (lane == 0) s.red[warp] = v;
-    __syncthreads();
-    float t = s.red[0];
-    for (int w = 1; w < NW; ++w) t = fmaxf(t, s.red[w]);
-    return t;
-  }
-  __device__ float bmin(float v) {
-    v = warp_min(v);
-    __syncthreads();
-    if (lane == 0) s.red[warp] = v;
-    __syncthreads();
-    float t = s.red[0];
-    for (int w = 1; w < NW; ++w) t = fminf(t, s.red[w]);
-    return t;
-  }
-  // K floats at once: entries k < nmax reduced with max, the rest summed
-  template <int K>
-  __device__ void bred(float (&v)[K], int nmax) {
-#pragma unroll
-    for (int k = 0; k < K; ++k) v[k] = k < nmax ? warp_max(v[k]) : warp_sum(v[k]);
-    __syncthreads();
-    if (lane == 0)
-#pragma unroll
-      for (int k = 0; k < K; ++k) s.red[k * NW + warp] = v[k];
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      float t = s.red[k * NW];
-      for (int w = 1; w < NW; ++w) t = k < nmax ? fmaxf(t, s.red[k * NW + w]) : t + s.red[k * NW + w];
-      v[k] = t;
-    }
-  }
-  // sum of K floats at once
-  template <int K>
-  __device__ void bsum_k(float (&v)[K]) {
-#pragma unroll
-    for (int k = 0; k < K; ++k) v[k] = warp_sum(v[k]);
-    __syncthreads();
-    if (lane == 0)
-#pragma unroll
-      for (int k = 0; k < K; ++k) s.red[k * NW + warp] = v[k];
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      float t = 0.f;
-      for (int w = 0; w < NW; ++w) t += s.red[k * NW + w];
-      v[k] = t;
-    }
-  }
-  template <int K>
-  __device__ void bsum_ki(int (&v)[K]) {
-#pragma unroll
-    for (int k = 0; k < K; ++k) v[k] = warp_sum_i(v[k]);
-    __syncthreads();
-    int* ri = reinterpret_cast<int*>(s.red);
-    if (lane == 0)
-#pragma unroll
-      for (int k = 0; k < K; ++k) ri[k * NW + warp] = v[k];
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      int t = 0;
-      for (int w = 0; w < NW; ++w) t += ri[k * NW + w];
-      v[k] = t;
-    }
-  }
-
   // ------------------------------------------------------------------
   // geometry helpers
   // ------------------------------------------------------------------
