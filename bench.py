@@ -512,6 +512,89 @@ def study_uneven(args):
     print(json.dumps(out), flush=True)
 
 
+def sinusoid_conditions(n_freq=64, n_seeds=8):
+    """Sinusoidal length perturbation on the 2x2 skeletal lattice at pCa 4.5:
+    z(t) = 900 + 2 sin(2 pi f t) nm for f = logspace(0, 2.7, 64) Hz x 8 seeds
+    (keys split(PRNGKey(seed), 1)[0]), dt = min(1, 1000 / (20 f)) ms, five full
+    cycles and at least 200 ms."""
+    from multifil_jax_b200.engine import prng_split, prng_key
+    out = []
+    for k in range(n_freq):
+        f = 10.0 ** (2.7 * k / (n_freq - 1))
+        dt = min(1.0, 1000.0 / (20.0 * f))
+        n = int(max(5000.0 / f, 200.0) / dt)
+        z = (900.0 + 2.0 * np.sin(2.0 * np.pi * f * np.arange(n) * dt / 1000.0)).astype(np.float32)
+        for seed in range(n_seeds):
+            out.append((f, dt, n, z, prng_split(prng_key(seed), 1)[0]))
+    return out
+
+
+def stiffness(force, z, f, dt):
+    """Complex stiffness DFT(F)/DFT(z) at f over the whole cycles after one settling cycle."""
+    period = 1000.0 / f / dt
+    n0 = int(round(period))
+    n1 = n0 + int(round(int((len(force) - n0) // period) * period))
+    ph = np.exp(-2j * np.pi * f * np.arange(n0, n1) * dt / 1000.0)
+    F = np.asarray(force[n0:n1], np.float64)
+    Z = np.asarray(z[n0:n1], np.float64)
+    return np.sum((F - F.mean()) * ph) / np.sum((Z - Z.mean()) * ph)
+
+
+def study_sinusoid(args):
+    """The precision-study workload (512 conditions of uneven length and dt)
+    in one launch per precision mode: throughput, and how far the float32
+    mode's complex stiffness sits from the mixed mode's per frequency.  The
+    FP64-oracle comparison of this workload is tests/test_gpu_precision_study.py."""
+    import torch
+    from multifil_jax_b200 import SarcTopology, get_skeletal_params
+    from multifil_jax_b200.engine import get_engine, upload, MF_FLAG_PRECISE
+    s, d = get_skeletal_params()
+    topo = SarcTopology.create(2, 2, s, d)
+    eng = get_engine(0)
+    dev = torch.device('cuda', 0)
+    conds = sinusoid_conditions()
+    B, T = len(conds), max(c[2] for c in conds)
+    Z = np.zeros((B, T), np.float32)
+    NS = np.zeros(B, np.int32)
+    DT = np.zeros(B, np.float32)
+    KEYS = np.zeros((B, 2), np.uint32)
+    for i, (f, dt, n, z, key) in enumerate(conds):
+        Z[i, :n], Z[i, n:] = z, z[-1]
+        NS[i], DT[i], KEYS[i] = n, dt, key
+    P = np.tile(d.param_row(), (B, 1)).astype(np.float32)
+    PC = np.full((B, T), 4.5, np.float32)
+    L = np.full((B, T), 14.0, np.float32)
+    total = int(NS.sum())
+    out = {'study': 'sinusoid', 'metric': METRIC, 'conditions': B, 'condition_timesteps': total,
+           'workload': '2x2 skeletal, pCa 4.5, z = 900 + 2 sin(2 pi f t) nm, f = logspace(0, 2.7, 64) Hz x 8 '
+                       'seeds, dt = min(1, 1000/(20 f)) ms, 5 cycles (>= 200 ms), one launch per mode'}
+    Y = {}
+    for name, flags in (('mixed', MF_FLAG_PRECISE), ('float32', 0)):
+        a = upload(dev, P, Z, PC, L, NS, KEYS.view(np.int32), np.zeros(B, np.float32), np.zeros(B, np.float32), DT)
+        kw = dict(K_lat=a[6], nu=a[7], dt=a[8], n_newton=s.n_newton_steps, n_cg=s.n_cg_steps, flags=flags)
+        eng.run_batch(topo, *a[:6], **kw)  # warm-up
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res = eng.run_batch(topo, *a[:6], **kw)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        force = res['metrics'][:, 0, :].cpu().numpy()
+        Y[name] = np.array([stiffness(force[i, :c[2]], c[3], c[0], c[1]) for i, c in enumerate(conds)])
+        out[f'{name}_value'] = total / (ms / 1e3)
+        out[f'{name}_ms'] = ms
+    rel = np.abs(Y['float32'] - Y['mixed']) / np.abs(Y['mixed'])
+    fr = np.array([c[0] for c in conds])
+    out['float32_vs_mixed_stiffness'] = {
+        'median_rel': float(np.median(rel)), 'max_rel': float(rel.max()),
+        'median_rel_by_decade': {f'{lo:g}-{hi:g} Hz': float(np.median(rel[(fr >= lo) & (fr < hi)]))
+                                 for lo, hi in ((1, 10), (10, 100), (100, 600))}}
+    out['mean_abs_stiffness_pN_per_nm'] = {f'{fr[i]:.1f} Hz': float(np.mean(np.abs(Y['mixed'][i:i + 8])))
+                                           for i in (0, 8 * 31, 8 * 63)}
+    print(json.dumps(out), flush=True)
+
+
 def study_serving(args):
     """Serving at 50 / 80 / 95 % of the measured capacity of the request mix."""
     import torch
@@ -549,7 +632,7 @@ def main():
     ap.add_argument('--serve-budget-gb', type=int, default=8)
     ap.add_argument('--traffic', type=float, default=None)
     ap.add_argument('--no-cpu-baseline', action='store_true')
-    ap.add_argument('--study', default=None, choices=['uneven', 'serving'],
+    ap.add_argument('--study', default=None, choices=['uneven', 'serving', 'sinusoid'],
                     help='run one workload study instead of the bench line')
     ap.add_argument('--study-capacity-requests', type=int, default=2000)
     ap.add_argument('--profile-case', default=None,
@@ -559,6 +642,8 @@ def main():
         study_uneven(args)
     elif args.study == 'serving':
         study_serving(args)
+    elif args.study == 'sinusoid':
+        study_sinusoid(args)
     elif args.profile_case:
         profile_case(args)
     elif args.impl == 'reference':
