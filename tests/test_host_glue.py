@@ -170,3 +170,15 @@ def test_choose_batch_sizes_keeps_the_faster_set(monkeypatch):
     assert kept == picks and eng.sizes == picks
     # one size already: nothing to compare
     assert autotune.choose_batch_sizes(tops[:1], {(1, 1): 256}, timer(True)) == {(1, 1): 256}
+
+
+def test_scalar_sweep_matches_constant_trace_sweep(topo):
+    """plan_batch broadcasts a sweep of scalars; the driver arrays equal those
+    of the same sweep given as constant traces."""
+    pcas = [4.0, 5.25, 6.5]
+    a = plan_batch(topo, duration_ms=7, pCa=pcas, z_line=[900.0, 950.0])
+    b = plan_batch(topo, duration_ms=7, pCa=[np.full(7, v) for v in pcas],
+                   z_line=[np.full(7, 900.0), np.full(7, 950.0)])
+    for name in ('pCa', 'z', 'ls', 'params', 'keys'):
+        assert np.array_equal(getattr(a, name), getattr(b, name)), name
+    assert a.pCa.flags['C_CONTIGUOUS'] and a.pCa.dtype == np.float32 and a.pCa.shape == (6, 7)
