@@ -41,10 +41,14 @@ extern "C" {
 #define MF_ERR_BUSY (-6)      /* request still running */
 
 /* per-condition status bits written to status_out */
-#define MF_STATUS_NONFINITE 1      /* a Newton update or residual was not finite */
+#define MF_STATUS_NONFINITE 1      /* a Newton update or residual was not finite (the update
+                                      was zeroed, as kernels/solver.py:415 does) */
 #define MF_STATUS_NOT_CONVERGED 2  /* residual above solver_residual_tol at some step */
-#define MF_STATUS_BOUNDS 4         /* an index was out of range (debug checks) */
-#define MF_STATUS_MULTIBIND 8      /* a site carried 3+ bound heads (sum order differs) */
+/* bit 4 is unused: every index the kernel forms is validated on the host when
+ * the lattice is uploaded, and no data-dependent index leaves its range */
+#define MF_STATUS_MULTIBIND 8      /* a site carried 3+ force-carrying heads at some step (the
+                                      reference's double binding, transitions.py:1199-1219;
+                                      their forces are summed in head order) */
 
 /* batch flags */
 #define MF_FLAG_DYNAMIC_LS 1       /* lattice spacing solved as an unknown (K_lat given) */
@@ -142,19 +146,41 @@ int mf_workspace_bytes(mf_ctx* ctx, const mf_batch* batch, uint64_t* bytes);
 /* Allocation-free variant of mf_run_batch (no counterpart in the reference:
  * it exists for callers of this library, not of the reference API).
  * For callers that must not have the library allocate device memory on the
- * call path -- a framework that owns all HBM through its own allocator and
- * budget, or a loop that cannot absorb cudaMalloc's implicit device-wide
- * synchronisation.  All per-call scratch (per-condition workspaces and the
- * launch descriptor table) comes from one 8 MiB array compiled into the
- * library (present on every device that loads it, until process exit); the
- * call never allocates.  A batch whose scratch exceeds 8 MiB is rejected with
+ * call path: a framework that owns all HBM through its own allocator and
+ * budget.  All per-call scratch (per-condition workspaces and the launch
+ * descriptor table) comes from one 8 MiB array compiled into the library
+ * (present on every device that loads it, until process exit); the call
+ * never allocates.  A batch whose scratch exceeds 8 MiB is rejected with
  * MF_ERR_NOMEM and a message naming both sizes (at 2x2 about 70 conditions
  * fit).  Batched single-launch path only: MF_FLAG_PLAIN and chunk_steps > 0
- * are rejected.  The first call on a device resolves the array's device
- * address, so make it before any stream capture.  Every call reuses the same
+ * are rejected, as are negative n_newton / n_cg (MF_ERR_INVALID).
+ * The call blocks the calling host thread: it reads n_steps, K_lat, nu and dt
+ * from the device with synchronous copies before launching (so those four
+ * arrays must hold their values when the call is made, not merely be ordered
+ * on `stream`), and it returns only after `stream` has synchronised.  It can
+ * therefore not be recorded inside a stream capture.  The array's device
+ * address is resolved once per device per process, on the first call with
+ * that device current; a process that resets the device (cudaDeviceReset)
+ * must not call this entry point afterwards.  Every call reuses the same
  * array (the region a call uses is zeroed before its kernels run); calls that
  * overlap on the GPU race on it and must be serialised by the caller. */
 int mf_run_batch_static(mf_ctx* ctx, const mf_batch* batch, void* stream);
+
+/* Test hook: the transition tables a condition's kernel builds for one
+ * DynamicParams row `params` (host, 44 floats) at (pCa, lattice spacing d)
+ * and timestep dt (ms), with the arithmetic of the precision mode in `flags`
+ * (MF_FLAG_PRECISE or 0).  They are the reference's expm_pade6_batch results
+ * (kernels/transitions.py:99-190) on its tropomyosin generators (:434-513),
+ * crossbridge bin grid (:807-922) and absorbing-chain grid (:1029-1078),
+ * in the form the kernel keeps them.  Outputs (host, any may be NULL):
+ *   cum_tm [27*4*4]        cumulative rows (jnp.cumsum order) of the 27
+ *                          tropomyosin tables, configuration-major;
+ *   cum_xb [2*n_bins*6*6]  cumulative rows of the crossbridge tables, row
+ *                          block = permissiveness * n_bins + bin;
+ *   pabs   [2*n_bins*3]    P_abs[3,4], P_abs[2,0], P_abs[3,0] of each block.
+ * Allocates and synchronises the device (a test hook, not a hot path). */
+int mf_transition_tables(mf_ctx* ctx, int32_t topo_id, const float* params, float pCa, float d, float dt,
+                         int32_t flags, float* cum_tm, float* cum_xb, float* pabs);
 
 /* jax.random on the host: key = PRNGKey(seed); keys_out[2*i..] = split(key, n)[i].
  * partitionable=1: JAX >= 0.5 layout; 0: original layout. */

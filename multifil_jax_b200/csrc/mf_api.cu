@@ -9,6 +9,7 @@
 #include <deque>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -58,6 +59,11 @@ struct mf_ctx {
   Server* server = nullptr;
   cudaStream_t cap_stream = nullptr;  // private stream for CUDA-graph capture
   cudaEvent_t cap_event = nullptr;
+  // The executable graph of the last chunked batch and the launch list it was
+  // captured from: a later batch with the same launches (same shapes, buffers
+  // and flags; the descriptor table's contents may differ) replays it.
+  cudaGraphExec_t graph_exec = nullptr;
+  std::vector<char> graph_sig;
 };
 
 static int fail(mf_ctx* c, int code, const char* fmt, ...) {
@@ -187,6 +193,7 @@ int mf_destroy(mf_ctx* ctx) {
   }
   if (ctx->ws) cudaFree(ctx->ws);
   if (ctx->d_cond) cudaFree(ctx->d_cond);
+  if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
   if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
   if (ctx->cap_event) cudaEventDestroy(ctx->cap_event);
   delete ctx;
@@ -522,48 +529,126 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
       tab[(size_t)c * B + k] = d;
     }
   CK(cudaMemcpyAsync(ctx->d_cond, tab.data(), sizeof(CondDesc) * tab.size(), cudaMemcpyHostToDevice, st));
+  // the launches of the whole batch: every chunk, every CTA-size group
+  struct Launch { int threads, grid, base; size_t smem; StepArgs args; };
+  std::vector<Launch> launches;
+  for (int c = 0; c < n_chunks; ++c)
+    for (const Group& g : groups)
+      launches.push_back({g.threads, g.end - g.begin, g.begin, g.smem,
+                          make_args(bt, ctx->d_cond + (size_t)c * B, base_flags | g.lflags, max_dof, max_x, max_s)});
   const bool use_graph = !(bt->flags & MF_FLAG_NO_GRAPH) && n_chunks > 1;
-  cudaGraph_t graph = nullptr;
-  cudaStream_t launch_st = st;
-  if (use_graph) {
+  if (!use_graph) {
+    for (const Launch& l : launches) {
+      cudaError_t e = launch(l.threads, l.args, l.grid, l.base, l.smem, st);
+      if (e != cudaSuccess) return fail(ctx, MF_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
+    }
+    CK(cudaStreamSynchronize(st));  // the host descriptor table dies here
+    return MF_OK;
+  }
+  // Chunked batches replay one CUDA graph of all their launches.  The launch
+  // list, field by field, is the graph's signature.
+  std::vector<char> sig;
+  auto put = [&sig](const void* p, size_t n) {
+    const char* c = static_cast<const char*>(p);
+    sig.insert(sig.end(), c, c + n);
+  };
+  for (const Launch& l : launches) {
+    const StepArgs& a = l.args;
+    put(&l.threads, sizeof l.threads); put(&l.grid, sizeof l.grid); put(&l.base, sizeof l.base);
+    put(&l.smem, sizeof l.smem); put(&a.cond, sizeof a.cond); put(&a.T, sizeof a.T);
+    put(&a.n_newton, sizeof a.n_newton); put(&a.n_cg, sizeof a.n_cg); put(&a.flags, sizeof a.flags);
+    put(&a.resid_warn, sizeof a.resid_warn); put(&a.sq64_from, sizeof a.sq64_from);
+    put(&a.u_thin, sizeof a.u_thin); put(&a.u_xb, sizeof a.u_xb); put(&a.x_trace, sizeof a.x_trace);
+    put(&a.st_trace, sizeof a.st_trace); put(&a.bd_trace, sizeof a.bd_trace); put(&a.max_dof, sizeof a.max_dof);
+    put(&a.max_xbs, sizeof a.max_xbs); put(&a.max_sites, sizeof a.max_sites);
+  }
+  if (!ctx->graph_exec || sig != ctx->graph_sig) {
     // capture on a private non-blocking stream (the caller's may be the legacy
     // default stream, which cannot be captured); the graph replays on st
     if (!ctx->cap_stream) {
       CK(cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
       CK(cudaEventCreateWithFlags(&ctx->cap_event, cudaEventDisableTiming));
     }
-    launch_st = ctx->cap_stream;
+    if (ctx->graph_exec) {
+      cudaGraphExecDestroy(ctx->graph_exec);
+      ctx->graph_exec = nullptr;
+      ctx->graph_sig.clear();
+    }
+    cudaStream_t cs = ctx->cap_stream;
     for (const Group& g : groups)
       CK(prepare(g.threads, (base_flags & FLAG_PRECISE) != 0, (base_flags & FLAG_DYN) != 0, g.smem));
     CK(cudaEventRecord(ctx->cap_event, st));
-    CK(cudaStreamWaitEvent(launch_st, ctx->cap_event, 0));
-    CK(cudaStreamBeginCapture(launch_st, cudaStreamCaptureModeThreadLocal));
-  }
-  for (int c = 0; c < n_chunks; ++c) {
-    for (const Group& g : groups) {
-      StepArgs a = make_args(bt, ctx->d_cond + (size_t)c * B, base_flags | g.lflags, max_dof,
-                             max_x, max_s);
-      cudaError_t e = launch(g.threads, a, g.end - g.begin, g.begin, g.smem, launch_st);
+    CK(cudaStreamWaitEvent(cs, ctx->cap_event, 0));
+    CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    cudaGraph_t graph = nullptr;
+    for (const Launch& l : launches) {
+      cudaError_t e = launch(l.threads, l.args, l.grid, l.base, l.smem, cs);
       if (e != cudaSuccess) {
-        if (use_graph) {
-          cudaStreamEndCapture(launch_st, &graph);
-          if (graph) cudaGraphDestroy(graph);
-        }
+        cudaStreamEndCapture(cs, &graph);
+        if (graph) cudaGraphDestroy(graph);
         return fail(ctx, MF_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
       }
     }
-  }
-  if (use_graph) {
-    CK(cudaStreamEndCapture(launch_st, &graph));
+    CK(cudaStreamEndCapture(cs, &graph));
     cudaGraphExec_t exec = nullptr;
     cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) return fail(ctx, MF_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
-    e = cudaGraphLaunch(exec, st);
-    cudaGraphExecDestroy(exec);
+    ctx->graph_exec = exec;
+    ctx->graph_sig.swap(sig);
+  }
+  {
+    cudaError_t e = cudaGraphLaunch(ctx->graph_exec, st);
     if (e != cudaSuccess) return fail(ctx, MF_ERR_CUDA, "graph launch: %s", cudaGetErrorString(e));
   }
   CK(cudaStreamSynchronize(st));  // the host descriptor table dies here
+  return MF_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Test hook: the transition tables of one (parameter row, pCa, spacing, dt).
+// ---------------------------------------------------------------------------
+namespace {
+
+// One CTA builds every table with the step kernel's own builder.
+__global__ void tables_probe_kernel(const float* params, const float* centers, int nb, float pCa, float d,
+                                    float dt, int sq64, float* cum_tm, float* cum_xb, float* pabs) {
+  __shared__ float P[kNParams];
+  for (int i = threadIdx.x; i < kNParams; i += blockDim.x) P[i] = params[i];
+  __syncthreads();
+  build_tables_block(P, centers, nb, pCa, d, dt, sq64, cum_tm, cum_xb, pabs, true, true, true, nullptr, 0,
+                     (int)threadIdx.x, (int)blockDim.x);
+}
+
+}  // namespace
+
+extern "C" {
+
+int mf_transition_tables(mf_ctx* ctx, int32_t topo_id, const float* params, float pCa, float d, float dt,
+                         int32_t flags, float* cum_tm, float* cum_xb, float* pabs) {
+  if (!ctx || !params) return fail(ctx, MF_ERR_INVALID, "null argument");
+  if (topo_id < 0 || topo_id >= (int)ctx->topos.size()) return fail(ctx, MF_ERR_NOTFOUND, "unknown topology");
+  CK(cudaSetDevice(ctx->device));
+  const TopoDev& td = ctx->topos[topo_id]->dev;
+  const int nb = td.n_bins;
+  const size_t n_tm = 27 * 16, n_xb = (size_t)2 * nb * 36, n_abs = (size_t)2 * nb * 3;
+  float* buf = nullptr;
+  CK(cudaMalloc(&buf, sizeof(float) * (kNParams + n_tm + n_xb + n_abs)));
+  float *dp = buf, *dtm = buf + kNParams, *dxb = dtm + n_tm, *dab = dxb + n_xb;
+  const int sq64 = (flags & MF_FLAG_PRECISE) ? 1 : 1 << 20;  // as make_args
+  cudaError_t e = cudaMemcpy(dp, params, sizeof(float) * kNParams, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    tables_probe_kernel<<<1, 256>>>(dp, td.centers, nb, pCa, d, dt, sq64, dtm, dxb, dab);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess && cum_tm) e = cudaMemcpy(cum_tm, dtm, sizeof(float) * n_tm, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && cum_xb) e = cudaMemcpy(cum_xb, dxb, sizeof(float) * n_xb, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && pabs) e = cudaMemcpy(pabs, dab, sizeof(float) * n_abs, cudaMemcpyDeviceToHost);
+  cudaFree(buf);
+  if (e != cudaSuccess) return fail(ctx, MF_ERR_CUDA, "mf_transition_tables: %s", cudaGetErrorString(e));
   return MF_OK;
 }
 
@@ -591,8 +676,13 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) char g_static_scratch[kStaticScratchBytes];
 
 // Device address of g_static_scratch per device, resolved once with that
-// device current (the host symbol itself is not a device address).
+// device current (the host symbol itself is not a device address).  The
+// once-flag makes two host threads' first calls on one device resolve it
+// once; the result code is kept so that a failed resolution is reported to
+// every later call instead of being retried.
 char* g_static_ptr[kMaxDevices] = {nullptr};
+cudaError_t g_static_err[kMaxDevices] = {};
+std::once_flag g_static_once[kMaxDevices];
 
 }  // namespace
 
@@ -609,17 +699,20 @@ int mf_run_batch_static(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
   if (bt->chunk_steps > 0) return fail(ctx, MF_ERR_INVALID, "mf_run_batch_static: runs all steps in one launch");
   if ((bt->flags & MF_FLAG_DYNAMIC_LS) && (!bt->K_lat || !bt->nu))
     return fail(ctx, MF_ERR_INVALID, "dynamic lattice spacing needs K_lat and nu");
+  if (bt->n_newton < 0 || bt->n_cg < 0) return fail(ctx, MF_ERR_INVALID, "negative solver caps");
   if (ctx->device < 0 || ctx->device >= kMaxDevices) return fail(ctx, MF_ERR_INVALID, "device index out of range");
   CK(cudaSetDevice(ctx->device));
-  // one-time set-up on this device (the first call must not be inside a capture)
-  if (!g_static_ptr[ctx->device]) {
+  // one-time set-up on this device, with the device current
+  const int dev = ctx->device;
+  std::call_once(g_static_once[dev], [dev]() {
     void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
-    if (e != cudaSuccess || !p)
-      return fail(ctx, MF_ERR_CUDA, "cudaGetSymbolAddress(static scratch): %s", cudaGetErrorString(e));
-    g_static_ptr[ctx->device] = static_cast<char*>(p);
-  }
-  char* base = g_static_ptr[ctx->device];
+    g_static_err[dev] = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (g_static_err[dev] == cudaSuccess && !p) g_static_err[dev] = cudaErrorInvalidSymbol;
+    if (g_static_err[dev] == cudaSuccess) g_static_ptr[dev] = static_cast<char*>(p);
+  });
+  if (g_static_err[dev] != cudaSuccess)
+    return fail(ctx, MF_ERR_CUDA, "cudaGetSymbolAddress(static scratch): %s", cudaGetErrorString(g_static_err[dev]));
+  char* base = g_static_ptr[dev];
   cudaStream_t st = (cudaStream_t)stream_v;
   const int B = bt->B;
   std::vector<int> n_steps(B);

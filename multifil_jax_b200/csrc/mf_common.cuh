@@ -9,6 +9,24 @@
 
 namespace mf {
 
+#ifdef __CUDACC__
+// max / min that return NaN when either operand is NaN, as jnp.maximum,
+// jnp.minimum and jnp.clip do (fmaxf / fminf return the other operand), so
+// that a NaN reaches the residual norm and the status bit the way it reaches
+// the reference's while-loop test.  One instruction (PTX max.NaN / min.NaN,
+// sm_80 and later).
+__device__ __forceinline__ float fmax_nan(float a, float b) {
+  float d;
+  asm("max.NaN.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+  return d;
+}
+__device__ __forceinline__ float fmin_nan(float a, float b) {
+  float d;
+  asm("min.NaN.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+  return d;
+}
+#endif
+
 constexpr int kNParams = 44;
 constexpr int kNMetrics = 52;
 // per-warp partials of the metrics' fused block reduction (one per lane)

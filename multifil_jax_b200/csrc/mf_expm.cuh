@@ -231,14 +231,14 @@ static __device__ void xb_generator(const float* P, float pCa, float x, float d,
   const float cap = 10000.0f;
   float r01 = perm * P[XB_R01_COEFF] * expf(-Ew);
   if (isnan(r01)) r01 = 0.f;
-  float r10 = fminf(expf(logf(r01 + 0.005f) - (U_drx - U_loose)), cap);
+  float r10 = fmin_nan(expf(logf(r01 + 0.005f) - (U_drx - U_loose)), cap);
   if (isnan(r10)) r10 = cap;
-  float r12 = P[XB_R12_COEFF] * expf(fminf(Ediff, 30.0f) / 2.0f);
+  float r12 = P[XB_R12_COEFF] * expf(fmin_nan(Ediff, 30.0f) / 2.0f);
   if (isnan(r12)) r12 = 0.f;
-  const float r21 = fminf(expf(logf(r12) - (U_loose - U_t1)), cap);
-  const float r23 = fminf(P[XB_R23_COEFF] * expf(-f_s * P[XB_DELTA_23] / kt), cap);
-  const float r32 = expf(fminf(logf(r23 + 1e-30f) + (U_t2 - U_t1), logf(cap)));
-  const float r34 = fminf(P[XB_R34_COEFF] * expf(f_s * P[XB_DELTA_34] / kt), cap);
+  const float r21 = fmin_nan(expf(logf(r12) - (U_loose - U_t1)), cap);
+  const float r23 = fmin_nan(P[XB_R23_COEFF] * expf(-f_s * P[XB_DELTA_23] / kt), cap);
+  const float r32 = expf(fmin_nan(logf(r23 + 1e-30f) + (U_t2 - U_t1), logf(cap)));
+  const float r34 = fmin_nan(P[XB_R34_COEFF] * expf(f_s * P[XB_DELTA_34] / kt), cap);
   const float r43 = 0.f;
   const float r40 = P[XB_R40], r04 = P[XB_R04], r05 = P[XB_R05];
   const float k0 = P[XB_SRX_K0], kmax = P[XB_SRX_KMAX], b = P[XB_SRX_B], ca50 = P[XB_SRX_CA50];

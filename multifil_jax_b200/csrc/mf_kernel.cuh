@@ -234,8 +234,8 @@ __device__ void metrics(Sim<NT, PR, DY>& m, int t, float zl, float pCa, float ne
     const float c = dsp - t_shift;
     tsum += c;
     tsq = fmaf(c, c, tsq);
-    tmin = fminf(tmin, dsp);
-    tmax = fmaxf(tmax, dsp);
+    tmin = fmin_nan(tmin, dsp);
+    tmax = fmax_nan(tmax, dsp);
     dxs += m.s.x[i] - old_x[i];
   }
   for (int g = tid; g < S; g += NT) {
@@ -258,8 +258,8 @@ __device__ void metrics(Sim<NT, PR, DY>& m, int t, float zl, float pCa, float ne
     const float c = dsp - n_shift;
     nsum += c;
     nsq = fmaf(c, c, nsq);
-    nmin = fminf(nmin, dsp);
-    nmax = fmaxf(nmax, dsp);
+    nmin = fmin_nan(nmin, dsp);
+    nmax = fmax_nan(nmax, dsp);
   }
   // energies of the thick backbone's first spring and of titin
   // (metrics_fn.py:262-288), one filament per thread counted from the last
@@ -307,7 +307,7 @@ __device__ void metrics(Sim<NT, PR, DY>& m, int t, float zl, float pCa, float ne
   // block totals, lane k holding total k (every warp forms them itself)
   float R = red[lane];
 #pragma unroll 4
-  for (int w = 1; w < NW; ++w) R = lane < 4 ? fmaxf(R, red[w * 32 + lane]) : R + red[w * 32 + lane];
+  for (int w = 1; w < NW; ++w) R = lane < 4 ? fmax_nan(R, red[w * 32 + lane]) : R + red[w * 32 + lane];
   const float force = *force_slot;
   auto tot = [&](int k) { return __shfl_sync(0xffffffffu, R, k); };
   MF_MT(3);

@@ -16,30 +16,35 @@ namespace mf {
 
 cudaError_t MF_NAME(prepare_, MF_NT, MF_P, MF_D)(size_t smem) {
   auto* kernel = step_kernel<MF_NT, (MF_P != 0), (MF_D != 0)>;
-  static size_t attr_bytes = 0;
-  if (smem > attr_bytes) {
-    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // Function attributes belong to the device's context, so what has been set
+  // is remembered per device.
+  constexpr int kDevices = 64;
+  static size_t attr_bytes[kDevices] = {};
+  static int sm_bytes[kDevices] = {}, set_pct[kDevices] = {};  // set_pct: carve-out + 1, 0 = never set
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kDevices) return cudaErrorInvalidDevice;
+  if (smem > attr_bytes[dev]) {
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    attr_bytes = smem;
+    attr_bytes[dev] = smem;
   }
   // Shared-memory carve-out: just what the register-limited occupancy needs
   // (static and driver-reserved bytes included), so the rest of the SM's
   // 256 KB stays L1, where the spilled registers live.
-  static int sm_bytes = 0, last_pct = -1;
-  if (!sm_bytes) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (cudaDeviceGetAttribute(&sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
-        sm_bytes <= 0)
-      sm_bytes = 233472;
+  if (!sm_bytes[dev]) {
+    if (cudaDeviceGetAttribute(&sm_bytes[dev], cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+        sm_bytes[dev] <= 0)
+      sm_bytes[dev] = 233472;
   }
   const size_t need = (size_t)min_ctas(MF_NT) * (smem + kStaticSmem + 1024);
-  int pct = (int)((need * 100 + sm_bytes - 1) / (size_t)sm_bytes);
+  int pct = (int)((need * 100 + sm_bytes[dev] - 1) / (size_t)sm_bytes[dev]);
   pct = pct > 100 ? 100 : pct;
-  if (pct != last_pct) {
-    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+  if (pct + 1 != set_pct[dev]) {
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
     if (e != cudaSuccess) return e;
-    last_pct = pct;
+    set_pct[dev] = pct + 1;
   }
   return cudaSuccess;
 }

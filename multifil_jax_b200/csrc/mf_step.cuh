@@ -82,7 +82,7 @@ __device__ __forceinline__ float warp_reduce_transposed(float (&v)[32], int lane
       const float send = up ? v[j] : v[j + o];
       const float keep = up ? v[j + o] : v[j];
       const float recv = __shfl_xor_sync(0xffffffffu, send, o);
-      v[j] = base + j < NMAX ? fmaxf(keep, recv) : keep + recv;
+      v[j] = base + j < NMAX ? fmax_nan(keep, recv) : keep + recv;
     }
   }
   return v[0];
@@ -90,7 +90,7 @@ __device__ __forceinline__ float warp_reduce_transposed(float (&v)[32], int lane
 
 __device__ __forceinline__ float warp_max(float v) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  for (int o = 16; o > 0; o >>= 1) v = fmax_nan(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
 
@@ -530,7 +530,7 @@ struct Sim : SimDyn<DY> {
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       float t = rb[k * NW];
-      for (int w = 1; w < NW; ++w) t = (max0 && k == 0) ? fmaxf(t, rb[k * NW + w]) : t + rb[k * NW + w];
+      for (int w = 1; w < NW; ++w) t = (max0 && k == 0) ? fmax_nan(t, rb[k * NW + w]) : t + rb[k * NW + w];
       v[k] = t;
     }
   }
@@ -618,8 +618,8 @@ struct Sim : SimDyn<DY> {
     const float Lt = sqrtf(ad * ad + d * d);
     float arg = s.P[TITIN_B] * (Lt - s.P[TITIN_REST]);
     const bool clipped = arg < -100.f || arg > 100.f;
-    arg = fminf(fmaxf(arg, -100.f), 100.f);
-    const float Ft = fmaxf(s.P[TITIN_A] * expf(arg), 0.f);
+    arg = fmin_nan(fmax_nan(arg, -100.f), 100.f);
+    const float Ft = fmax_nan(s.P[TITIN_A] * expf(arg), 0.f);
     const float cosang = Lt > 0.f ? ad / Lt : 0.f;
     ax = 6.0f * (Ft * cosang);
     const float bb = clipped ? 0.f : s.P[TITIN_B];
@@ -660,6 +660,7 @@ struct Sim : SimDyn<DY> {
           gs = thin_of(i) * nsi + bnd;
           const int k = atomicAdd(&cnt[gs], 1);
           if (k < 2) site_h[2 * gs + k] = (int16_t)i;
+          else if (k == 2) status |= MF_MULTIBIND_BIT;
         }
         s.hsite[i] = gs;
       }
@@ -796,7 +797,7 @@ struct Sim : SimDyn<DY> {
         }
       }
       r[i] = (float)F;
-      fmax = fmaxf(fmax, (float)fabs(F));
+      fmax = fmax_nan(fmax, (float)fabs(F));
     });
     float v[3] = {fmax, rad_part, jdd_part};
     reduce<3>(v, true);
@@ -804,7 +805,7 @@ struct Sim : SimDyn<DY> {
     if (dyn) {
       const float Fr = -Kl * (d - d_ref) + (-v[1]);
       *frad = Fr;
-      m = fmaxf(m, fabsf(Fr));
+      m = fmax_nan(m, fabsf(Fr));
       if (jdd) *jdd = -Kl - v[2];
     }
     return m;
@@ -907,7 +908,7 @@ struct Sim : SimDyn<DY> {
 
   // float32 mode: the reference's PCG recurrences and association orders.
   __device__ __forceinline__ void solve_std(float zl, float& d, double& resid, int& iters, bool dyn_jdd) {
-    const float tol = fmaxf(s.P[SOLVER_TOL], fmaxf(s.P[THICK_K] * 1e-4f, 0.25f));
+    const float tol = fmax_nan(s.P[SOLVER_TOL], fmax_nan(s.P[THICK_K] * 1e-4f, 0.25f));
     const int n_cg = A.n_cg, n_newton = A.n_newton;
     float* __restrict__ xv = s.x;
     float* __restrict__ rv = s.r;
@@ -977,7 +978,7 @@ struct Sim : SimDyn<DY> {
       if (dyn) {
         float v = dx_d;
         if (!isfinite(v)) v = 0.f;
-        d = fmaxf(d + v, 1.0f);
+        d = fmax_nan(d + v, 1.0f);
       }
     }
     resid = fmx;
@@ -1073,7 +1074,7 @@ struct Sim : SimDyn<DY> {
   // alpha_k = gamma_k / (delta_k - beta_k gamma_k / alpha_{k-1}) uses
   // (p_k, A p_k) = (u_k, A u_k) - beta_k^2 (p_{k-1}, A p_{k-1}).
   __device__ __forceinline__ void solve_cg_gear(float zl, float& d, double& resid, int& iters, bool dyn_jdd) {
-    const float tol = fmaxf(s.P[SOLVER_TOL], fmaxf(s.P[THICK_K] * 1e-4f, 0.25f));
+    const float tol = fmax_nan(s.P[SOLVER_TOL], fmax_nan(s.P[THICK_K] * 1e-4f, 0.25f));
     const int n_cg = A.n_cg, n_newton = A.n_newton;
     float frad = 0.f, jdd = 0.f, J_dd_inv = 0.f, fmx = 0.f;
     int it = 0, bad = 0, bad_local = 0;
@@ -1131,7 +1132,7 @@ struct Sim : SimDyn<DY> {
       if (dyn) {
         float v = dx_d;
         if (!isfinite(v)) v = 0.f;
-        d = fmaxf(d + v, 1.0f);
+        d = fmax_nan(d + v, 1.0f);
       }
       if (tid == 0) MF_COUNT(4);
     }
@@ -1139,7 +1140,7 @@ struct Sim : SimDyn<DY> {
     iters = it;
     if (!isfinite(fmx)) status |= MF_NONFINITE_BIT;
   }
-  static constexpr int MF_NONFINITE_BIT = 1;
+  static constexpr int MF_NONFINITE_BIT = 1, MF_MULTIBIND_BIT = 8;
   // ------------------------------------------------------------------
   // Register-resident precise Newton-CG (lattices with at most RF filaments
   // per warp and filaments of at most 32*RE nodes, crowns of 3 heads).
@@ -1242,7 +1243,7 @@ struct Sim : SimDyn<DY> {
             F = (e_j - e_m) * ktn + (double)acc;
           }
           Fv = (float)F;
-          fmax = fmaxf(fmax, (float)fabs(F));
+          fmax = fmax_nan(fmax, (float)fabs(F));
         }
         r[k][e] = Fv;
       }
@@ -1259,7 +1260,7 @@ struct Sim : SimDyn<DY> {
     if (dyn) {
       const float Fr = -Kl * (d - d_ref) + (-v[1]);
       *frad = Fr;
-      m = fmaxf(m, fabsf(Fr));
+      m = fmax_nan(m, fabsf(Fr));
       if (jdd) *jdd = -Kl - v[2];
     }
     return m;
@@ -1391,7 +1392,7 @@ struct Sim : SimDyn<DY> {
   }
 
   __device__ __forceinline__ void solve_regs(float zl, float& d, double& resid, int& iters, bool dyn_jdd) {
-    const float tol = fmaxf(s.P[SOLVER_TOL], fmaxf(s.P[THICK_K] * 1e-4f, 0.25f));
+    const float tol = fmax_nan(s.P[SOLVER_TOL], fmax_nan(s.P[THICK_K] * 1e-4f, 0.25f));
     RVec r;
     const int n_cg = A.n_cg, n_newton = A.n_newton;
     float frad = 0.f, jdd = 0.f, J_dd_inv = 0.f, fmx = 0.f;
@@ -1476,7 +1477,7 @@ struct Sim : SimDyn<DY> {
       if (dyn) {
         float v = dx_d;
         if (!isfinite(v)) v = 0.f;
-        d = fmaxf(d + v, 1.0f);
+        d = fmax_nan(d + v, 1.0f);
       }
       if (tid == 0) MF_COUNT(4);
     }

@@ -26,7 +26,9 @@ MF_FLAG_NO_GRAPH = 16
 
 MF_STATUS_NONFINITE = 1
 MF_STATUS_NOT_CONVERGED = 2
+MF_STATUS_MULTIBIND = 8
 
+MF_ERR_INVALID = -1
 MF_ERR_BUSY = -6
 MF_ERR_NOMEM = -3
 
@@ -90,6 +92,9 @@ _SIGNATURES = {
     'mf_run_batch_static': (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(mf_batch), ctypes.c_void_p]),
     'mf_workspace_bytes': (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(mf_batch),
                                           ctypes.POINTER(ctypes.c_uint64)]),
+    'mf_transition_tables': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_float,
+                                            ctypes.c_float, ctypes.c_float, ctypes.c_int32, ctypes.c_void_p,
+                                            ctypes.c_void_p, ctypes.c_void_p]),
     'mf_prng_split': (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32,
                                      ctypes.c_void_p]),
     'mf_prng_uniform': (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32,
@@ -242,6 +247,22 @@ class Engine:
             self._check(self.lib.mf_tune_threads_mode(self.h, up.topo_id, int(precision == 'mixed'), int(threads)),
                         'mf_tune_threads_mode')
 
+    def transition_tables(self, topo, params, pCa: float, d: float, dt: float = 1.0, precision: str = 'float32'):
+        """The kernel's transition tables at (pCa, d): cumulative tropomyosin rows
+        [27, 4, 4], cumulative crossbridge rows [2, n_bins, 6, 6] (permissiveness,
+        bin) and the absorbing-chain entries [2, n_bins, 3] (test hook)."""
+        up = self.upload(topo)
+        nb = topo.n_xb_bins
+        row = np.ascontiguousarray(params, dtype=np.float32).reshape(N_PARAMS)
+        tm = np.zeros((27, 4, 4), np.float32)
+        xb = np.zeros((2, nb, 6, 6), np.float32)
+        pa = np.zeros((2, nb, 3), np.float32)
+        self._check(self.lib.mf_transition_tables(self.h, up.topo_id, row.ctypes.data, float(pCa), float(d),
+                                                  float(dt), MF_FLAG_PRECISE if precision == 'mixed' else 0,
+                                                  tm.ctypes.data, xb.ctypes.data, pa.ctypes.data),
+                    'mf_transition_tables')
+        return tm, xb, pa
+
     # ------------------------------------------------------------------
     def run_batch(self, topos, params, z, pCa, ls, n_steps, keys, K_lat=None, nu=None, dt=None,
                   n_newton=4, n_cg=6, flags=0, chunk_steps=0, residual_warn=1.5, stream=None,
@@ -366,10 +387,12 @@ def to_host(t):
 
 
 def execute_plan(topology, plan, static_params, precision: str = 'float32', device: Optional[int] = None,
-                 minibatch_size="auto", chunk_steps: int = 0, stream=None, key_major: bool = False) -> np.ndarray:
+                 minibatch_size="auto", chunk_steps: int = 0, stream=None, key_major: bool = False,
+                 status_out: Optional[np.ndarray] = None) -> np.ndarray:
     """Run every condition of a BatchPlan on the GPU; returns host metrics [B, 52, T]
     (``key_major``: [52, B, T], transposed on the device so that every metric is
-    one contiguous block on the host)."""
+    one contiguous block on the host).  ``status_out`` (int32 [B]) receives
+    every condition's MF_STATUS_* bits."""
     torch = _torch()
     eng = get_engine(device)
     dev = torch.device('cuda', eng.device)
@@ -399,6 +422,8 @@ def execute_plan(topology, plan, static_params, precision: str = 'float32', devi
                                 flags=flags, chunk_steps=chunk_steps,
                                 residual_warn=static_params.solver_residual_tol, stream=stream)
             m = res['metrics'].permute(1, 0, 2).contiguous() if key_major else res['metrics']
+            if status_out is not None:
+                status_out[s:e] = res['status'].cpu().numpy()
             if out is None:
                 return to_host(m)
             if key_major:

@@ -1,9 +1,9 @@
-"""``run()`` and ``SimulationResult``: the reference's public entry point on the CUDA engine.
+"""``run()``: the reference's public entry point on the CUDA engine.
 
 Mirrors ``multifil_jax/simulation.py:754-1165`` (sweep expansion, per-field
 parameter tables, key split, Poisson lattice-spacing pre-computation, result
-data cube, residual warning) and ``:96-420`` (``SimulationResult`` with
-``sel``/``mean``/``std``/``stack``/indexing).  The per-condition time loop --
+data cube, residual warning); the result type is
+:class:`multifil_jax_b200.result.SimulationResult`.  The per-condition time loop --
 the reference's ``jit(vmap(scan(timestep)))`` -- runs in the fused sm_100a
 kernel through :mod:`multifil_jax_b200.engine`; there is no CPU path.
 
@@ -22,6 +22,7 @@ import numpy as np
 
 from .params import DYNAMIC_FIELDS, DynamicParams, StaticParams, N_PARAMS
 from .topology import SarcTopology
+from .result import MetricsDict, SimulationResult
 
 METRIC_KEYS = (
     'axial_force', 'solver_residual', 'z_line', 'pCa', 'lattice_spacing',
@@ -43,16 +44,6 @@ BATCH_BUCKETS = (1, 2, 4, 8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096, 8192, 
 PRECISIONS = ('float32', 'mixed')
 
 
-class MetricsDict(dict):
-    """dict with attribute access (reference ``core/state.py:118-130``)."""
-
-    def __getattr__(self, key):
-        try:
-            return self[key]
-        except KeyError:
-            raise AttributeError(key)
-
-
 def get_bucket_size(actual_size: int) -> int:
     """Next power-of-two bucket (reference ``simulation.py:434-450``).
 
@@ -63,168 +54,6 @@ def get_bucket_size(actual_size: int) -> int:
         if b >= actual_size:
             return b
     return actual_size
-
-
-class SimulationResult:
-    """Result container of :func:`run` (reference ``simulation.py:96-420``).
-
-    ``metrics`` maps each of the 52 metric names to a numpy array shaped
-    ``grid_shape + (replicates, n_steps)`` (``newton_iters`` int32, the rest
-    float32).
-    """
-
-    __slots__ = ('metrics', 'rng_key', 'z_line', 'pCa', 'lattice_spacing', 'final_state', 'metadata',
-                 'dt', 'name', '_grid_shape', '_axis_names', 'coords', 'topology_config')
-
-    def __init__(self, metrics, rng_key, z_line, pCa, lattice_spacing, final_state=None, metadata=None,
-                 dt=1.0, name="", grid_shape=None, axis_names=None, coords=None, topology_config=None):
-        self.metrics = metrics if isinstance(metrics, MetricsDict) else MetricsDict(metrics)
-        self.rng_key = rng_key
-        self.z_line = z_line
-        self.pCa = pCa
-        self.lattice_spacing = lattice_spacing
-        self.final_state = final_state
-        self.metadata = metadata if metadata is not None else {}
-        self.dt = float(dt)
-        self.name = str(name)
-        self._grid_shape = grid_shape
-        self._axis_names = axis_names if axis_names is not None else []
-        self.coords = coords if coords is not None else {}
-        self.topology_config = topology_config if topology_config is not None else {}
-
-    @property
-    def n_steps(self) -> int:
-        return self.metrics['axial_force'].shape[-1]
-
-    @property
-    def replicate_axis(self) -> Optional[int]:
-        return self._axis_names.index('replicates') if 'replicates' in self._axis_names else None
-
-    @property
-    def time(self) -> np.ndarray:
-        return np.arange(self.n_steps) * self.dt
-
-    @property
-    def axial_force(self) -> np.ndarray:
-        return self.metrics['axial_force']
-
-    @property
-    def mean_force(self) -> float:
-        return float(np.mean(self.metrics['axial_force']))
-
-    @property
-    def steady_state_force(self) -> float:
-        n_avg = max(1, self.n_steps // 5)
-        return float(np.mean(self.metrics['axial_force'][..., -n_avg:]))
-
-    def _reduce_replicates(self, fn, suffix: str) -> 'SimulationResult':
-        if self.replicate_axis is None:
-            raise ValueError("No replicate axis to reduce.")
-        m = MetricsDict({k: fn(v, axis=-2) for k, v in self.metrics.items()})
-        coords = {k: v for k, v in self.coords.items() if k != 'replicates'}
-        names = [n for n in self._axis_names if n != 'replicates']
-        f = m['axial_force']
-        return SimulationResult(
-            metrics=m, rng_key=self.rng_key, z_line=np.mean(self.z_line, axis=-2),
-            pCa=np.mean(self.pCa, axis=-2), lattice_spacing=np.mean(self.lattice_spacing, axis=-2),
-            final_state=None, metadata=self.metadata, dt=self.dt, name=self.name + suffix,
-            grid_shape=f.shape[:-1] if f.ndim > 1 else None, axis_names=names, coords=coords)
-
-    def mean(self) -> 'SimulationResult':
-        return self._reduce_replicates(np.mean, "_mean")
-
-    def std(self) -> 'SimulationResult':
-        return self._reduce_replicates(np.std, "_std")
-
-    def __getitem__(self, key) -> 'SimulationResult':
-        m = MetricsDict({k: v[key] for k, v in self.metrics.items()})
-        f = m['axial_force']
-        keys = key if isinstance(key, tuple) else (key,)
-        names = list(self._axis_names)
-        coords = dict(self.coords)
-        pos = 0
-        opaque = False
-        for k in keys:
-            if pos >= len(self._axis_names):
-                break
-            nm = self._axis_names[pos]
-            if isinstance(k, (int, np.integer)):
-                if nm in names:
-                    names.remove(nm)
-                coords.pop(nm, None)
-            elif isinstance(k, slice):
-                if nm in coords:
-                    try:
-                        coords[nm] = list(coords[nm])[k]
-                    except Exception:
-                        opaque = True
-            else:
-                opaque = True
-            pos += 1
-        if opaque:
-            names = list(self._axis_names)
-            coords = dict(self.coords)
-        return SimulationResult(
-            metrics=m, rng_key=self.rng_key, z_line=self.z_line[key], pCa=self.pCa[key],
-            lattice_spacing=self.lattice_spacing[key], final_state=None, metadata=self.metadata,
-            dt=self.dt, name=self.name, grid_shape=f.shape[:-1] if f.ndim > 1 else None,
-            axis_names=names, coords=coords)
-
-    def summary(self) -> str:
-        lines = [
-            f"SimulationResult: {self.name}",
-            f"  Shape: {self.axial_force.shape}",
-            f"  Duration: {self.n_steps * self.dt:.1f} ms ({self.n_steps} steps @ dt={self.dt}ms)",
-            f"  Mean force: {self.mean_force:.2f} pN",
-            f"  Steady-state force: {self.steady_state_force:.2f} pN",
-            f"  Metrics: {list(self.metrics.keys()) if self.metrics else 'none'}",
-            f"  Max solver residual: {float(np.max(self.metrics['solver_residual'])):.4f} pN",
-        ]
-        if self._axis_names:
-            lines.append(f"  Grid axes: {self._axis_names}")
-        if self.coords:
-            lines.append(f"  Coords: {list(self.coords.keys())}")
-        return '\n'.join(lines)
-
-    def sel(self, **kwargs) -> 'SimulationResult':
-        idx = [slice(None)] * self.axial_force.ndim
-        names = list(self._axis_names)
-        coords = dict(self.coords)
-        for name, value in kwargs.items():
-            if name not in self.coords:
-                raise ValueError(f"Unknown axis '{name}'. Available: {list(self.coords.keys())}")
-            cl = self.coords[name]
-            if value not in cl:
-                raise ValueError(f"Value {value} not in {name} coords: {cl}")
-            idx[self._axis_names.index(name)] = cl.index(value)
-        out = self[tuple(idx)]
-        for name in kwargs:
-            if name in names:
-                names.remove(name)
-            coords.pop(name, None)
-        out._axis_names = names
-        out.coords = coords
-        return out
-
-    @classmethod
-    def stack(cls, results: List['SimulationResult'], axis_name: str = 'structural',
-              axis_values: Optional[List] = None) -> 'SimulationResult':
-        if not results:
-            raise ValueError("Cannot stack empty list of results")
-        keys = list(results[0].metrics.keys())
-        m = MetricsDict({k: np.stack([r.metrics[k] for r in results]) for k in keys})
-        coords = dict(results[0].coords)
-        coords[axis_name] = axis_values if axis_values is not None else list(range(len(results)))
-        return cls(metrics=m, rng_key=results[-1].rng_key,
-                   z_line=np.stack([r.z_line for r in results]), pCa=np.stack([r.pCa for r in results]),
-                   lattice_spacing=np.stack([r.lattice_spacing for r in results]), final_state=None,
-                   metadata=results[0].metadata, dt=results[0].dt, name=results[0].name + "_stacked",
-                   grid_shape=m['axial_force'].shape[:-1], axis_names=[axis_name] + results[0]._axis_names,
-                   coords=coords)
-
-    def __repr__(self) -> str:
-        f = self.metrics.get('axial_force')
-        return f"SimulationResult(name='{self.name}', shape={getattr(f, 'shape', '?')}, dt={self.dt})"
 
 
 # ---------------------------------------------------------------------------
@@ -457,9 +286,15 @@ def run(topology: SarcTopology, duration_ms: float = 1000.0, dt: float = 1.0,
                       sp, replicates, rng_seed, subpopulation)
     if verbose:
         print(f"Grid shape: {plan.grid_shape}, axes: {plan.axis_names}, total: {plan.total}")
-    from .engine import execute_plan
+    from .engine import execute_plan, MF_STATUS_NONFINITE
+    status = np.zeros(plan.total, np.int32)
     metrics = execute_plan(topology, plan, sp, precision=precision, device=device,
-                           minibatch_size=minibatch_size, chunk_steps=chunk_steps, key_major=True)
+                           minibatch_size=minibatch_size, chunk_steps=chunk_steps, key_major=True,
+                           status_out=status)
+    bad = np.flatnonzero(status & MF_STATUS_NONFINITE)
+    if bad.size:
+        warnings.warn(f"{bad.size} of {plan.total} conditions produced a non-finite Newton update or residual "
+                      f"(first: condition {int(bad[0])}); the update was zeroed, as the reference does")
     return assemble_result(plan, metrics, sp, rng_seed, verbose, key_major=True)
 
 

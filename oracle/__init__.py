@@ -16,9 +16,10 @@ Modules, each citing the reference file:line it follows:
 Pinning: the topology and the whole timestep are checked against fixtures
 produced by running the reference's own Python source under a NumPy-backed
 JAX stand-in (``tests/golden/make_golden.py``).  The Threefry hash is checked
-against the published Random123 known-answer vectors; the jax.random key
-split / uniform layering has no golden vector in this environment (JAX is not
-installed), so that layer is "parity unpinned" and follows the documented
-behaviour of JAX >= 0.5 (``jax_threefry_partitionable=True``), with the older
-layout selectable.
+against the published Random123 known-answer vectors, and the jax.random key
+split / uniform layering against outputs of JAX itself for key 0 in both
+counter layouts (``tests/test_prng.py``): the partitionable layout of
+JAX >= 0.5 (the default here) and the original one.  What stays unpinned is
+JAX's own arithmetic under the stand-in (``jvp``/``grad``, the reassociation
+of ``associative_scan``): the fixtures were made without JAX.
 """

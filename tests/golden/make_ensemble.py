@@ -1,7 +1,7 @@
 """Generate the 64-seed ensemble fixture by running the reference's own ``run()``.
 
 TEST INFRASTRUCTURE.  Runs ``multifil_jax.simulation.run`` (the reference
-checkout, default ``/root/reference``) under the NumPy JAX stand-in in
+checkout named by ``MULTIFIL_REF``) under the NumPy JAX stand-in in
 ``jaxshim/`` for the 2x2 skeletal lattice at pCa 4.5, z_line 900 nm, 100 ms,
 ``replicates=64``, ``rng_seed=0`` (keys ``split(PRNGKey(0), 64)``), and writes
 ``ensemble.npz`` next to this file: the 64 axial-force traces.  The GPU test

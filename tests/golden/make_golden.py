@@ -1,7 +1,7 @@
 """Generate golden fixtures by running the reference's own Python source.
 
-TEST INFRASTRUCTURE.  Runs ``multifil_jax`` (the reference checkout, default
-``/root/reference``) under the NumPy JAX stand-in in ``jaxshim/`` and writes
+TEST INFRASTRUCTURE.  Runs ``multifil_jax`` (the reference checkout named by
+``MULTIFIL_REF``) under the NumPy JAX stand-in in ``jaxshim/`` and writes
 ``golden.npz`` next to this file:
 
 * ``topo_RxC__<field>``   every SarcTopology array for a few lattice sizes

@@ -1,8 +1,9 @@
 """Import the reference's Python source under the NumPy JAX stand-in.
 
-TEST INFRASTRUCTURE for ``make_golden.py`` only: needs the reference checkout
-(default ``/root/reference``, override with ``MULTIFIL_REF``), which exists in
-the build container but not on GPU machines.  Package ``__init__`` files of the
+TEST INFRASTRUCTURE for the fixture generators only: needs a checkout of the
+reference project, named by the ``MULTIFIL_REF`` environment variable (the
+directory that holds its ``multifil_jax`` package).  GPU machines have none;
+the fixtures they test against are committed.  Package ``__init__`` files of the
 reference are bypassed (they configure XLA), submodules are imported directly.
 """
 import importlib
@@ -12,10 +13,18 @@ import types
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get('MULTIFIL_REF', '/root/reference')
+
+
+def reference_root() -> str:
+    ref = os.environ.get('MULTIFIL_REF')
+    if not ref or not os.path.isdir(os.path.join(ref, 'multifil_jax')):
+        raise RuntimeError('set MULTIFIL_REF to a checkout of the reference project (the directory '
+                           'holding its multifil_jax package) to regenerate the fixtures')
+    return ref
 
 
 def load():
+    REF = reference_root()
     shim = os.path.join(HERE, 'jaxshim')
     if shim not in sys.path:
         sys.path.insert(0, shim)

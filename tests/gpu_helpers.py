@@ -54,3 +54,53 @@ def state_divergence(res, b, info, topo, T):
 
 def oracle_positions(info, topo):
     return np.stack([np.concatenate([s.thick_x.reshape(-1), s.thin_x.reshape(-1)]) for s in info['states']])
+
+
+def oracle_tables(topo, row, pCa, d, dtype):
+    """The oracle's sampling tables at (pCa, d): (P_tm [27,4,4], P_xb [2*n_bins,6,6])."""
+    from oracle import physics as ph
+    p = ph.param_dict(row, dtype)
+    tab = OS.tables(topo, p, pCa, d, 1.0, dtype)
+    return tab.P_tm, tab.P_xb
+
+
+def divergence_cause(topo, row, pCa, d, dtype, info, res, b, t):
+    """Why the engine's step t differs from the oracle's (fixed spacing, constant pCa).
+
+    Returns (cause, margin): 'draw' with the smallest distance between a
+    uniform and a threshold of the oracle's cumulative row, over the heads and
+    sites whose new state differs; 'bin' with the smallest distance of such a
+    head's axial offset to a bin edge (nm); 'newton' when no integer state
+    differs (the accept-or-iterate decision of the Newton loop, the residual
+    being at its floor).
+    """
+    from oracle import physics as ph
+    X, S = topo.total_xbs, topo.n_sites_total
+    st = res['state_trace'][b, t]
+    o = info['states'][t]
+    u_thin, u_xb = info['uniforms'][t]
+    prev = info['states'][t - 1] if t > 0 else None
+    old_xb = prev.xb_state.astype(np.int32) if prev is not None else np.zeros(X, np.int32)
+    old_tm = prev.tm if prev is not None else np.zeros((topo.n_thin, topo.n_sites), np.int8)
+    P_tm, P_xb = oracle_tables(topo, row, pCa, d, dtype)
+    heads = np.flatnonzero(st[:X] != o.xb_state)
+    sites = np.flatnonzero(st[X:X + S] != o.tm.reshape(-1))
+    if heads.size == 0 and sites.size == 0:
+        return 'newton', None
+    margins, bins = [], []
+    if heads.size:
+        perm = ph.permissiveness(o.tm, o.xb_nearest, topo)
+        key = ph.xb_bin_key(o.xb_dist[:, 0], perm, topo)
+        cum = np.cumsum(P_xb[key[heads], old_xb[heads]].astype(np.float64), axis=1)
+        margins.append(np.min(np.abs(cum - np.asarray(u_xb, np.float64)[heads, None]), axis=1))
+        bins.append(np.min(np.abs(o.xb_dist[heads, 0][:, None].astype(np.float64)
+                                  - topo.xb_bin_edges[None, :].astype(np.float64)), axis=1))
+    if sites.size:
+        cfg = ph.tm_config(old_tm, topo.tm_prev_neighbor, topo.tm_next_neighbor)
+        s_old = old_tm.reshape(-1).astype(np.int32)
+        cum = np.cumsum(P_tm[cfg[sites], s_old[sites]].astype(np.float64), axis=1)
+        margins.append(np.min(np.abs(cum - np.asarray(u_thin, np.float64)[sites, None]), axis=1))
+    m = float(np.min(np.concatenate(margins)))
+    if bins and float(np.min(np.concatenate(bins))) < 1e-4:
+        return 'bin', float(np.min(np.concatenate(bins)))
+    return 'draw', m

@@ -6,7 +6,7 @@ from multifil_jax_b200 import SarcTopology, get_skeletal_params, get_cardiac_par
 from multifil_jax_b200.engine import MF_FLAG_DYNAMIC_LS, MF_FLAG_PRECISE, MF_FLAG_PLAIN, MF_FLAG_ORIGINAL_PRNG
 from multifil_jax_b200.simulation import plan_batch, METRIC_KEYS
 from oracle import prng, step as OS
-from tests.gpu_helpers import run_engine, oracle_with_states, state_divergence, oracle_positions
+from tests.gpu_helpers import run_engine, oracle_with_states, state_divergence, oracle_positions, divergence_cause
 from tests.oracle_helpers import first_divergence, compare_metrics
 
 pytestmark = pytest.mark.gpu
@@ -29,7 +29,9 @@ def test_kernel_matches_oracle_per_step(engine, nr, nc, T, pCa, z):
     div = state_divergence(res, 0, info, topo, T)
     mdiv = first_divergence(res['metrics'], m_o[None], KEYS)
     win = min(v for v in (div, mdiv, T) if v is not None)
-    assert win >= min(T, 10), (div, mdiv)
+    if win < T:  # only a near tie that float32 rounding can split
+        cause, margin = divergence_cause(topo, d.param_row(), pCa, 14.0, np.float32, info, res, 0, win)
+        assert cause in ('newton', 'bin') or margin < 1e-3, (win, cause, margin)
     xo = oracle_positions(info, topo)[:win]
     xg = res['x_trace'][0, :win, :topo.n_dof]
     # relative to the coordinate scale: a node near the M-line inherits the
@@ -42,18 +44,24 @@ def test_kernel_matches_oracle_per_step(engine, nr, nc, T, pCa, z):
 
 
 def test_device_threefry_matches_jax_layout(engine):
-    """No injection: the kernel's own Threefry stream reproduces the oracle's draws."""
+    """No injection: the kernel's own Threefry stream draws exactly the
+    oracle's uniforms (jax.random layout), in both counter layouts, so the
+    run equals the one with the oracle's draws injected, at every step."""
     s, d = get_skeletal_params()
     topo = SarcTopology.create(2, 2, s, d)
-    T = 30
+    T = 60
     for part, flags in ((None, 0), (False, MF_FLAG_ORIGINAL_PRNG)):
         key = prng.split(prng.PRNGKey(3), 1, partitionable=part)[0]
         m_o, info = OS.run_condition(topo, d.param_row(), np.full(T, 900.0), np.full(T, 4.5), np.full(T, 14.0),
                                      key, record_states=True, partitionable=part)
-        res = run_engine(engine, topo, d.param_row()[None], np.full((1, T), 900.0), np.full((1, T), 4.5),
-                         np.full((1, T), 14.0), key[None], traces=True, flags=flags)
-        div = state_divergence(res, 0, info, topo, T)
-        assert div is None or div >= 20, div
+        args = (engine, topo, d.param_row()[None], np.full((1, T), 900.0), np.full((1, T), 4.5),
+                np.full((1, T), 14.0), key[None])
+        own = run_engine(*args, traces=True, flags=flags)
+        inj = run_engine(*args, traces=True, flags=flags,
+                         u_thin=np.stack([u[0] for u in info['uniforms']])[None],
+                         u_xb=np.stack([u[1] for u in info['uniforms']])[None])
+        for k in ('state_trace', 'bound_trace', 'metrics', 'x_trace'):
+            assert np.array_equal(own[k], inj[k]), (part, k)
 
 
 def _golden_case(name):
@@ -81,6 +89,7 @@ def test_run_api_matches_reference_fixture(golden, name):
     ref = np.stack([golden[f'run_{name}__{k}'].reshape(B, T) for k in KEYS], axis=1)
     div = first_divergence(mine, ref, KEYS)
     upto = div if div is not None else T
+    print(f'\n{name}: window {upto} of {T}')
     assert upto >= min(T, 5), div
     bad = compare_metrics(mine, ref, KEYS, rtol=1e-4, upto=upto)
     assert not bad, bad
@@ -98,6 +107,13 @@ def test_plain_chunked_and_batched_are_identical(engine):
     c = run_engine(engine, topo, P, Z, PC, L, keys, chunk_steps=5)
     assert np.array_equal(a['metrics'], b['metrics'])
     assert np.array_equal(a['metrics'], c['metrics'])
+    # a second chunked batch of the same shape replays the cached graph with
+    # the new descriptor table: other inputs, the same results as unchunked
+    PC2 = PC[::-1].copy()
+    a2 = run_engine(engine, topo, P, Z, PC2, L, keys[::-1].copy())
+    c2 = run_engine(engine, topo, P, Z, PC2, L, keys[::-1].copy(), chunk_steps=5)
+    assert np.array_equal(a2['metrics'], c2['metrics'])
+    assert not np.array_equal(a2['metrics'], a['metrics'])
 
 
 def test_condition_alone_equals_in_mixed_batch(engine):
@@ -134,6 +150,7 @@ def test_dynamic_lattice_spacing_matches_oracle(engine, nr, nc):
     div = state_divergence(res, 0, info, topo, T)
     mdiv = first_divergence(res['metrics'], m_o[None], KEYS)
     win = min(v for v in (div, mdiv, T) if v is not None)
+    print(f'\ndynamic spacing {nr}x{nc}: window {win} of {T}')
     assert win >= 5
     ls_o, ls_g = m_o[4, :win], res['metrics'][0, 4, :win]
     assert np.max(np.abs(ls_g - ls_o) / ls_o) < 1e-5
@@ -141,13 +158,16 @@ def test_dynamic_lattice_spacing_matches_oracle(engine, nr, nc):
     assert not bad, bad
 
 
-def test_mixed_precision_force_error_vs_fp64_oracle(engine):
-    """'mixed' precision: <= 1e-5 relative force error against the FP64 oracle (same uniforms)."""
+@pytest.mark.parametrize('pCa', [4.5, 5.5, 6.5])
+def test_mixed_precision_force_error_vs_fp64_oracle(engine, pCa):
+    """'mixed' precision: <= 1e-5 relative force error against the FP64 oracle
+    (same uniforms) over 200 steps; the states follow the oracle's throughout
+    unless a draw falls within 1e-5 of a table threshold."""
     s, d = get_skeletal_params()
     topo = SarcTopology.create(2, 2, s, d)
-    T = 30
+    T = 200
     key = prng.split(prng.PRNGKey(0), 1)[0]
-    zt, pt, lt = np.full(T, 900.0), np.full(T, 4.5), np.full(T, 14.0)
+    zt, pt, lt = np.full(T, 900.0), np.full(T, pCa), np.full(T, 14.0)
     m32, info32 = OS.run_condition(topo, d.param_row(), zt, pt, lt, key)
     m64, info64 = OS.run_condition(topo, d.param_row(), zt, pt, lt, key, dt=np.float64,
                                    uniforms=info32['uniforms'], record_states=True)
@@ -158,7 +178,9 @@ def test_mixed_precision_force_error_vs_fp64_oracle(engine):
     div = state_divergence(res, 0, info64, topo, T)
     mdiv = first_divergence(res['metrics'], m64[None], KEYS)
     win = min(v for v in (div, mdiv, T) if v is not None)
-    assert win >= 3
+    if win < T:
+        cause, margin = divergence_cause(topo, d.param_row(), pCa, 14.0, np.float64, info64, res, 0, win)
+        assert cause == 'bin' or (cause == 'draw' and margin < 1e-5), (win, cause, margin)
     f64, fg = m64[0, :win], res['metrics'][0, 0, :win]
     err_mixed = np.max(np.abs(fg - f64) / np.abs(f64))
     assert err_mixed <= 1e-5, err_mixed
@@ -184,6 +206,7 @@ def test_mixed_precision_dynamic_ls_vs_fp64_oracle(engine, nr, nc, pCa):
     div = state_divergence(res, 0, info64, topo, T)
     mdiv = first_divergence(res['metrics'], m64[None], KEYS)
     win = min(v for v in (div, mdiv, T) if v is not None)
+    print(f'\nmixed dynamic spacing {nr}x{nc} pCa {pCa}: window {win} of {T}')
     assert win >= 3
     for row in (0, 4):  # axial_force, lattice_spacing
         ref, got = m64[row, :win], res['metrics'][0, row, :win]

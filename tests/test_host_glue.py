@@ -112,6 +112,36 @@ def test_result_cube_sel_mean_std_stack(topo):
     assert 'Mean force' in r.summary() and np.isclose(r.time[-1], 4.0)
     with pytest.raises(ValueError):
         r.sel(pCa=9.9)
+    with pytest.raises(ValueError):
+        r.sel(thick_k=1.0)
+
+
+def test_result_axis_bookkeeping(topo):
+    """Integers drop their axis, slices cut coordinates, other keys keep the
+    bookkeeping; reductions average the drivers; trace-sweep coordinates
+    select by value."""
+    p, r = _fake_result(topo, duration_ms=4, pCa=[4.0, 5.0], z_line=[900.0, 950.0, 1000.0], replicates=2)
+    assert r._axis_names == ['z_line', 'pCa', 'replicates', 'time']
+    a = r[1]
+    assert a._axis_names == ['pCa', 'replicates', 'time'] and 'z_line' not in a.coords
+    assert a.axial_force.shape == (2, 2, 4) and np.array_equal(a.z_line, r.z_line[1])
+    b = r[:, 0]
+    assert b._axis_names == ['z_line', 'replicates', 'time'] and b.coords['z_line'] == [900.0, 950.0, 1000.0]
+    c = r[np.array([0, 2])]
+    assert c._axis_names == r._axis_names and c.coords == r.coords and c.axial_force.shape[0] == 2
+    d = r[::2]
+    assert d.coords['z_line'] == [900.0, 1000.0]
+    sd = r.std()
+    assert sd.name == 'run_std' and sd._axis_names == ['z_line', 'pCa', 'time']
+    assert np.array_equal(sd.pCa, r.pCa.mean(axis=-2)) and 'replicates' not in sd.coords
+    one = SimulationResult.stack([r.mean()], axis_name='size')
+    assert one.coords['size'] == [0] and one.name == 'run_mean_stacked'
+    tr = np.linspace(900.0, 905.0, 4)
+    _, t = _fake_result(topo, duration_ms=4, z_line=[tr, tr + 1.0])
+    picked = t.sel(z_line=t.coords['z_line'][1])
+    assert np.array_equal(picked.z_line[0], (tr + 1.0).astype(np.float32))
+    with pytest.raises(ValueError):
+        r.mean().mean()
 
 
 def test_residual_warning(topo):

@@ -44,3 +44,34 @@ def test_uniform_range_and_layering():
     assert ut.shape == (720,) and ux.shape == (624,) and k.shape == (2,)
     k1, tk = prng.split(prng.PRNGKey(3))
     assert np.array_equal(ut, prng.uniform(prng.split(tk)[1], 720))
+
+
+# Outputs of jax.random itself for key 0, as JAX prints them (public JAX
+# documentation and examples): split(PRNGKey(0)) and uniform(PRNGKey(0)) in
+# the original counter layout (jax_threefry_partitionable=False, the default
+# before JAX 0.5; the "Sharp Bits" notebook prints this split), and the same
+# calls in the partitionable layout (the default from JAX 0.5 on).  The first
+# partitionable pair is also H(key=(0,0), counter=(0,0)), the first Random123
+# answer above, which is what the partitionable split hashes.
+JAX_SPLIT0 = {False: [[4146024105, 967050713], [2718843009, 1272950319]],
+              True: [[1797259609, 2579123966], [928981903, 3453687069]]}
+JAX_UNIFORM0 = {False: 0.41845703, True: 0.947667}
+
+
+@pytest.mark.parametrize('part', [False, True])
+def test_jax_known_answers_oracle(part):
+    assert prng.split(prng.PRNGKey(0), 2, partitionable=part).tolist() == JAX_SPLIT0[part]
+    u = prng.uniform(prng.PRNGKey(0), 1, partitionable=part)
+    assert u.dtype == np.float32 and abs(float(u[0]) - JAX_UNIFORM0[part]) < 5e-7
+
+
+@pytest.mark.parametrize('part', [False, True])
+def test_jax_known_answers_library(part):
+    """The library's own jax.random layer (the code the kernel runs, compiled
+    for the host) gives the same answers."""
+    from multifil_jax_b200.engine import load_library, prng_split, prng_key
+    lib = load_library()
+    assert prng_split(prng_key(0), 2, partitionable=part).tolist() == JAX_SPLIT0[part]
+    u = np.zeros(1, np.float32)
+    assert lib.mf_prng_uniform(0, 0, 1, 1 if part else 0, u.ctypes.data) == 0
+    assert abs(float(u[0]) - JAX_UNIFORM0[part]) < 5e-7

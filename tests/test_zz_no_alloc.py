@@ -2,9 +2,9 @@
 
 Who needs it: callers that must not let this library allocate device memory
 while they run -- a host framework that owns every byte of HBM through its own
-allocator and budget, or a loop that cannot take the device-wide stall an
-implicit cudaMalloc synchronisation causes.  mf_run_batch_static takes its
-scratch from a fixed 8 MiB array compiled into the library instead.
+allocator and budget.  mf_run_batch_static takes its scratch from a fixed
+8 MiB array compiled into the library instead.  (It still blocks the calling
+thread until the stream has finished, like mf_run_batch.)
 
 The test drives the new entry point through the C ABI twice in a row (the
 second call reuses the array the first one left behind) and compares both
@@ -115,3 +115,20 @@ def test_static_scratch_rejects_oversized_batch():
     assert rc == MF_ERR_NOMEM
     msg = eng.lib.mf_last_error(eng.h).decode()
     assert 'static array holds' in msg and str(8 << 20) in msg
+
+
+def test_static_scratch_rejects_negative_solver_caps():
+    import torch
+    from multifil_jax_b200.engine import get_engine, mf_batch, MF_ERR_INVALID
+    eng = get_engine(0)
+    topos, inp, B, T = _inputs()
+    tid = np.array([eng.upload(t).topo_id for t in topos], dtype=np.int32)
+    out = torch.zeros((B, 52, T), device=inp['z'].device)
+    for n_newton, n_cg in ((-1, 6), (4, -2)):
+        b = mf_batch()
+        b.B, b.T_max, b.topo_id = B, T, tid.ctypes.data
+        for k in ('params', 'z', 'pCa', 'ls', 'n_steps', 'keys', 'K_lat', 'nu', 'dt'):
+            setattr(b, k, inp[k].data_ptr())
+        b.n_newton, b.n_cg, b.metrics_out = n_newton, n_cg, out.data_ptr()
+        assert eng.lib.mf_run_batch_static(eng.h, ctypes.byref(b), None) == MF_ERR_INVALID
+        assert 'negative solver caps' in eng.lib.mf_last_error(eng.h).decode()
