@@ -104,3 +104,10 @@ def divergence_cause(topo, row, pCa, d, dtype, info, res, b, t):
     if bins and float(np.min(np.concatenate(bins))) < 1e-4:
         return 'bin', float(np.min(np.concatenate(bins)))
     return 'draw', m
+
+
+def float32_force_floor(topo, d):
+    """Force change of two float32 roundings of every thick filament's M-line
+    node (pN): the force reads absolute float32 positions (~58 nm there)."""
+    x0 = np.float32(np.max(np.abs(topo.crown_offsets[:, 0])))
+    return topo.n_thick * float(d.thick_k) * 2.0 * float(np.spacing(x0))

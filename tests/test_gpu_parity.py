@@ -6,7 +6,8 @@ from multifil_jax_b200 import SarcTopology, get_skeletal_params, get_cardiac_par
 from multifil_jax_b200.engine import MF_FLAG_DYNAMIC_LS, MF_FLAG_PRECISE, MF_FLAG_PLAIN, MF_FLAG_ORIGINAL_PRNG
 from multifil_jax_b200.simulation import plan_batch, METRIC_KEYS
 from oracle import prng, step as OS
-from tests.gpu_helpers import run_engine, oracle_with_states, state_divergence, oracle_positions, divergence_cause
+from tests.gpu_helpers import (run_engine, oracle_with_states, state_divergence, oracle_positions,
+                               divergence_cause, float32_force_floor)
 from tests.oracle_helpers import first_divergence, compare_metrics
 
 pytestmark = pytest.mark.gpu
@@ -37,8 +38,10 @@ def test_kernel_matches_oracle_per_step(engine, nr, nc, T, pCa, z):
     # relative to the coordinate scale: a node near the M-line inherits the
     # float32 spacing of positions ~1000 nm away through the coupled solve
     assert np.max(np.abs(xg - xo) / np.maximum(np.abs(xo), 10.0)) < 1e-5
+    # the force reads float32 absolute positions: within two roundings of
+    # every M-line node (the float32 floor), bit-identical in most steps
     f_o, f_g = m_o[0, :win], res['metrics'][0, 0, :win]
-    assert np.max(np.abs(f_g - f_o) / np.maximum(np.abs(f_o), 1.0)) < 1e-5
+    assert np.max(np.abs(f_g - f_o)) <= float32_force_floor(topo, d)
     bad = compare_metrics(res['metrics'], m_o[None], KEYS, rtol=1e-4, upto=win)
     assert not bad, bad
 
