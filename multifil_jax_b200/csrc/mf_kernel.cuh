@@ -744,7 +744,10 @@ __device__ void run_condition(const StepArgs& A, int ci) {
   }
   for (int i = m.tid; i < 27 * 16; i += NT) MF_WS(float, cum_tm)[i] = m.s.cum_tm[i];
   for (int i = m.tid; i < 6 * T.n_bins; i += NT) MF_WS(float, pabs)[i] = m.s.pabs[i];
-  const int st_all = __syncthreads_or(m.status);
+  // block-wide OR of the status bits (__syncthreads_or returns 0 or 1, not
+  // the OR of its operands, so each bit is reduced on its own)
+  int st_all = 0;
+  for (int bit = 1; bit <= 8; bit <<= 1) st_all |= __syncthreads_or(m.status & bit) ? bit : 0;
   if (m.tid == 0) {
     uint32_t* kk = reinterpret_cast<uint32_t*>(MF_WS(double, misc) + MS_KEY);
     kk[0] = key_s[0];

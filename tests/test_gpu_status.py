@@ -57,26 +57,26 @@ def test_starved_newton_sets_not_converged(engine, precision):
     topo = SarcTopology.create(2, 2, s, d)
     B, T = 2, 15
     keys = prng.split(prng.PRNGKey(2), B)
-    args = (topo, np.tile(d.param_row(), (B, 1)), np.full((B, T), 950.0), np.full((B, T), 4.5),
+    args = (topo, np.tile(d.param_row(), (B, 1)), np.full((B, T), 900.0), np.full((B, T), 4.5),
             np.full((B, T), 14.0), keys)
     flags = MF_FLAG_PRECISE if precision == 'mixed' else 0
     loose = run_engine(engine, *args, flags=flags)
-    assert not np.any(loose['status'] & MF_STATUS_NOT_CONVERGED)
-    # one Newton iteration and a 1e-3 pN tolerance: the first step after the
-    # 50 nm z offset cannot meet it
+    assert np.all(loose['status'] == 0)
+    # one Newton iteration and a 1e-4 pN tolerance: float32 cannot go below
+    # its ~0.75 pN floor, and mixed precision stops near 1e-3 pN
     import torch
     from tests.gpu_helpers import tt, keys_tensor
     res = engine.run_batch(topo, tt(args[1], torch.float32), tt(args[2], torch.float32), tt(args[3], torch.float32),
                            tt(args[4], torch.float32), tt(np.full(B, T, np.int32)), keys_tensor(keys),
                            K_lat=tt(np.zeros(B), torch.float32), nu=tt(np.zeros(B), torch.float32),
-                           dt=tt(np.ones(B), torch.float32), n_newton=1, flags=flags, residual_warn=1e-3)
+                           dt=tt(np.ones(B), torch.float32), n_newton=1, flags=flags, residual_warn=1e-4)
     torch.cuda.synchronize()
     st = res['status'].cpu().numpy()
     m = res['metrics'].cpu().numpy()
     assert np.all(st & MF_STATUS_NOT_CONVERGED) and not np.any(st & MF_STATUS_NONFINITE)
-    assert m[:, 1].max() > 1e-3 and m[:, 51].max() <= 1
+    assert m[:, 1].max() > 1e-4 and m[:, 51].max() <= 1
     with warnings.catch_warnings(record=True) as w:
         warnings.simplefilter('always')
-        run(topo, duration_ms=T, z_line=950.0, static_params=StaticParams().replace(
-            n_newton_steps=1, solver_residual_tol=1e-3), precision=precision)
+        run(topo, duration_ms=T, z_line=900.0, static_params=StaticParams().replace(
+            n_newton_steps=1, solver_residual_tol=1e-4), precision=precision)
     assert any('exceeds threshold' in str(x.message) for x in w)
