@@ -165,42 +165,53 @@ __host__ __device__ inline CoefLayout coef_layout(const TopoDev& t) {
 // the 27 tropomyosin row sums (shared) and, per crossbridge bin and
 // permissiveness, the cumulative rows of expm(Q dt) ("sampling", global) or
 // the three absorbing-chain entries the metrics read ("absorbing", global).
-// Out of line: it runs only when pCa or the spacing changes, and its
-// unrolled Pade arithmetic would otherwise sit in the step loop's code.
-// tm: the 27 tropomyosin tables; sampling / absorbing: the crossbridge
-// tables of every key, or with `keys` only the nkeys listed ones (of the one
-// kind selected).
+// Each matrix is one 8-lane group's work (expm_rows): lane r builds, keeps
+// and stores row r.  Out of line: it runs only when pCa or the spacing
+// changes, and its Pade arithmetic would otherwise sit in the step loop's
+// code.  tm: the 27 tropomyosin tables; sampling / absorbing: the
+// crossbridge tables of every key, or with `keys` only the nkeys listed ones
+// (of the one kind selected).
 static __device__ __noinline__ void build_tables_block(const float* P, const float* centers, int nb, float pCa, float d,
                                                 float dtm, int sq64, float* cum_tm, float* cum_xb, float* pabs,
                                                 bool tm, bool sampling, bool absorbing, const int16_t* keys,
                                                 int nkeys, int tid, int nt) {
+  const int r = tid & (kGroup - 1);                      // row of this lane
+  const int group = tid / kGroup, ngroups = nt / kGroup;
+  const unsigned gmask = 0xFFu << (tid & 31 & ~(kGroup - 1));
   if (tm) {
-    for (int m = tid; m < 27; m += nt) {
-      float Q[16];
-      tm_generator(P, pCa, m, Q);
-      for (int i = 0; i < 16; ++i) Q[i] = Q[i] * dtm;
-      expm_pade6<4>(Q, sq64);
-      for (int r = 0; r < 4; ++r) cum4(Q + 4 * r, cum_tm + m * 16 + 4 * r);
+    for (int m = group; m < 27; m += ngroups) {
+      float q[4];
+      tm_generator_row(P, pCa, m, r < 4 ? r : 3, q);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) q[j] = q[j] * dtm;
+      expm_rows<4>(gmask, r, q, sq64);
+      if (r < 4) cum4(q, cum_tm + m * 16 + 4 * r);
     }
   }
   const int nwork = keys ? nkeys : (sampling ? 2 * nb : 0) + (absorbing ? 2 * nb : 0);
-  for (int w = tid; w < nwork; w += nt) {
+  for (int w = group; w < nwork; w += ngroups) {
     const bool is_abs = keys ? absorbing : (!sampling || w >= 2 * nb);
     const int key = keys ? (int)keys[w] : (is_abs && sampling ? w - 2 * nb : w);
     const int bin = key % nb;
     const float perm = key >= nb ? 1.0f : 0.0f;
-    float Q[36];
-    xb_generator(P, pCa, centers[bin], d, perm, Q);
-    if (is_abs)
-      for (int j = 0; j < 6; ++j) { Q[24 + j] = 0.f; Q[j] = 0.f; }
-    for (int i = 0; i < 36; ++i) Q[i] = Q[i] * dtm;
-    expm_pade6<6>(Q, sq64);
+    float q[6];
+    xb_generator_row(P, pCa, centers[bin], d, perm, r < 6 ? r : 5, q);
+    if (is_abs && (r == 0 || r == 4)) {  // the absorbing chain: rows 0 and 4 zeroed
+#pragma unroll
+      for (int j = 0; j < 6; ++j) q[j] = 0.f;
+    }
+#pragma unroll
+    for (int j = 0; j < 6; ++j) q[j] = q[j] * dtm;
+    expm_rows<6>(gmask, r, q, sq64);
     if (is_abs) {
-      pabs[key * 3 + 0] = Q[3 * 6 + 4];  // P_abs[3,4]
-      pabs[key * 3 + 1] = Q[2 * 6 + 0];  // P_abs[2,0]
-      pabs[key * 3 + 2] = Q[3 * 6 + 0];  // P_abs[3,0]
-    } else {
-      for (int r = 0; r < 6; ++r) cum6(Q + 6 * r, cum_xb + key * 36 + 6 * r);
+      if (r == 3) {
+        pabs[key * 3 + 0] = q[4];  // P_abs[3,4]
+        pabs[key * 3 + 2] = q[0];  // P_abs[3,0]
+      } else if (r == 2) {
+        pabs[key * 3 + 1] = q[0];  // P_abs[2,0]
+      }
+    } else if (r < 6) {
+      cum6(q, cum_xb + key * 36 + 6 * r);
     }
   }
 }
