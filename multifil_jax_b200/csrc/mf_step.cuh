@@ -165,53 +165,59 @@ __host__ __device__ inline CoefLayout coef_layout(const TopoDev& t) {
 // the 27 tropomyosin row sums (shared) and, per crossbridge bin and
 // permissiveness, the cumulative rows of expm(Q dt) ("sampling", global) or
 // the three absorbing-chain entries the metrics read ("absorbing", global).
-// Each matrix is one 8-lane group's work (expm_rows): lane r builds, keeps
-// and stores row r.  Out of line: it runs only when pCa or the spacing
-// changes, and its Pade arithmetic would otherwise sit in the step loop's
-// code.  tm: the 27 tropomyosin tables; sampling / absorbing: the
+// Each matrix is one lane pair's work (expm_pair): lane h builds, keeps and
+// stores rows h*N/2 ... of it.  Out of line: it runs only when pCa or the
+// spacing changes, and its Pade arithmetic would otherwise sit in the step
+// loop's code.  tm: the 27 tropomyosin tables; sampling / absorbing: the
 // crossbridge tables of every key, or with `keys` only the nkeys listed ones
 // (of the one kind selected).
 static __device__ __noinline__ void build_tables_block(const float* P, const float* centers, int nb, float pCa, float d,
                                                 float dtm, int sq64, float* cum_tm, float* cum_xb, float* pabs,
                                                 bool tm, bool sampling, bool absorbing, const int16_t* keys,
                                                 int nkeys, int tid, int nt) {
-  const int r = tid & (kGroup - 1);                      // row of this lane
-  const int group = tid / kGroup, ngroups = nt / kGroup;
-  const unsigned gmask = 0xFFu << (tid & 31 & ~(kGroup - 1));
+  const int h = tid & 1;                                  // which half of the rows
+  const int pair = tid >> 1, npairs = nt >> 1;
+  const unsigned pmask = 3u << (tid & 30);
   if (tm) {
-    for (int m = group; m < 27; m += ngroups) {
-      float q[4];
-      tm_generator_row(P, pCa, m, r < 4 ? r : 3, q);
+    for (int m = pair; m < 27; m += npairs) {
+      float q[2][4];
+      tm_generator_rows(P, pCa, m, h, q);
 #pragma unroll
-      for (int j = 0; j < 4; ++j) q[j] = q[j] * dtm;
-      expm_rows<4>(gmask, r, q, sq64);
-      if (r < 4) cum4(q, cum_tm + m * 16 + 4 * r);
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) q[i][j] = q[i][j] * dtm;
+      expm_pair<4>(pmask, h, q, sq64);
+#pragma unroll
+      for (int i = 0; i < 2; ++i) cum4(q[i], cum_tm + m * 16 + 4 * (2 * h + i));
     }
   }
   const int nwork = keys ? nkeys : (sampling ? 2 * nb : 0) + (absorbing ? 2 * nb : 0);
-  for (int w = group; w < nwork; w += ngroups) {
+  for (int w = pair; w < nwork; w += npairs) {
     const bool is_abs = keys ? absorbing : (!sampling || w >= 2 * nb);
     const int key = keys ? (int)keys[w] : (is_abs && sampling ? w - 2 * nb : w);
     const int bin = key % nb;
     const float perm = key >= nb ? 1.0f : 0.0f;
-    float q[6];
-    xb_generator_row(P, pCa, centers[bin], d, perm, r < 6 ? r : 5, q);
-    if (is_abs && (r == 0 || r == 4)) {  // the absorbing chain: rows 0 and 4 zeroed
+    float q[3][6];
+    xb_generator_rows(P, pCa, centers[bin], d, perm, h, q);
+    if (is_abs) {  // the absorbing chain: rows 0 and 4 zeroed
 #pragma unroll
-      for (int j = 0; j < 6; ++j) q[j] = 0.f;
+      for (int j = 0; j < 6; ++j) q[h == 0 ? 0 : 1][j] = 0.f;
     }
 #pragma unroll
-    for (int j = 0; j < 6; ++j) q[j] = q[j] * dtm;
-    expm_rows<6>(gmask, r, q, sq64);
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 6; ++j) q[i][j] = q[i][j] * dtm;
+    expm_pair<6>(pmask, h, q, sq64);
     if (is_abs) {
-      if (r == 3) {
-        pabs[key * 3 + 0] = q[4];  // P_abs[3,4]
-        pabs[key * 3 + 2] = q[0];  // P_abs[3,0]
-      } else if (r == 2) {
-        pabs[key * 3 + 1] = q[0];  // P_abs[2,0]
+      if (h == 1) {
+        pabs[key * 3 + 0] = q[0][4];  // P_abs[3,4]
+        pabs[key * 3 + 2] = q[0][0];  // P_abs[3,0]
+      } else {
+        pabs[key * 3 + 1] = q[2][0];  // P_abs[2,0]
       }
-    } else if (r < 6) {
-      cum6(q, cum_xb + key * 36 + 6 * r);
+    } else {
+#pragma unroll
+      for (int i = 0; i < 3; ++i) cum6(q[i], cum_xb + key * 36 + 6 * (3 * h + i));
     }
   }
 }
