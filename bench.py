@@ -126,29 +126,29 @@ def sweep_inputs():
 # ---------------------------------------------------------------------------
 # algorithmic work of one condition-timestep
 # ---------------------------------------------------------------------------
-def flops_per_condition_step(topo, iters, n_bound, tables_rebuilt=0.0):
-    """FP32 flops the fused step performs, counted from the kernel's arithmetic.
+# Floating-point operations of the reference algorithm on the 2x2 lattice,
+# per unit of work, from an op-counting run of the oracle (`python -m
+# oracle.opcount`, which counts every element operation of the oracle's
+# timestep by phase; tests/test_opcount.py checks these values against a
+# fresh count).  A step costs per_step + Newton iterations x per_newton; each
+# condition of a fixed-spacing, fixed-pCa launch builds its sampling and
+# absorbing tables once (per_table_build each, the squarings at each
+# matrix's own s).
+OPCOUNT_2X2 = {'per_step_flops': 68740.1, 'per_newton_flops': 269191.35294117645, 'per_step_sfu': 1272.0,
+               'per_newton_sfu': 8792.0, 'table_build_flops': 2617894, 'absorbing_build_flops': 2521696}
 
-    Per step: nearest-site search 3 flops x 30 candidates per head; sampling
-    ~6 compares per head/site; residual: 12 per node + 40 per bound head
-    (sqrt, atan2 counted as 1 flop each, SFU separately); per CG iteration:
-    JVP 8 per node + 6 per bound head, Thomas scans 2 x 2 flops per scan node
-    (2n nodes per filament) + 1 per node, dots/axpys 10 per node; CG iterations
-    per Newton iteration = 6, plus one residual per Newton iteration and the
-    initial one; metrics 12 per node.
-    """
-    N, X, S = topo.n_dof, topo.total_xbs, topo.n_sites_total
-    scan_nodes = topo.n_thick * 2 * topo.n_crowns + topo.n_thin * 2 * topo.n_sites
-    kin = X * 30 * 3 + (X + S) * 6
-    resid = N * 12 + n_bound * 40
-    cg = N * 8 + n_bound * 6 + 2 * 2 * scan_nodes + N + N * 10
-    newton = resid + 6 * cg
-    metrics = N * 12 + X * 4
-    per_step = kin + resid + iters * newton + metrics
-    return per_step
+
+def flops_per_condition_step(iters, steps_per_build):
+    """Op-counted flops (and SFU calls) per condition-timestep of the sweep."""
+    c = OPCOUNT_2X2
+    f = c['per_step_flops'] + iters * c['per_newton_flops'] + \
+        (c['table_build_flops'] + c['absorbing_build_flops']) / steps_per_build
+    sfu = c['per_step_sfu'] + iters * c['per_newton_sfu']
+    return f, sfu
 
 
 def fp32_peak_tflops(sm_mhz, n_sm=148):
+    """FP32 CUDA-core peak: SMs x 128 lanes x 2 (fused multiply-add) x clock."""
     return n_sm * 128 * 2 * sm_mhz * 1e6 / 1e12
 
 
@@ -254,18 +254,17 @@ def bench_gpu(args):
     torch.cuda.synchronize()
     other_value = B * T * args.steps / (sum(a.elapsed_time(b) for a, b in oe) / 1e3)
 
-    flops = flops_per_condition_step(topo, iters_mean, nbound_mean)
+    flops, sfu = flops_per_condition_step(iters_mean, T)
     sm_mhz = clocks.get('sm_mhz') or 1965.0
     fp32_peak = fp32_peak_tflops(sm_mhz)
-    achieved_tf = flops * (B * T) / (t_dev / args.steps / world * 1.0) / 1e12 if world == 1 else \
-        flops * (B * T) / (t_dev / args.steps) / 1e12
+    launch_s = t_dev / args.steps / world if world == 1 else t_dev / args.steps
+    achieved_tf = flops * (B * T) / launch_s / 1e12
     peaks_path = os.path.join(REPO, 'MEASURED_PEAKS.json')
     if os.path.exists(peaks_path):
         peaks, peak_source = json.load(open(peaks_path)), 'measured (copy bandwidth of this pool)'
     else:
         peaks, peak_source = {'hbm_gbs': 6650.0}, 'fallback (earlier measurement on this pool)'
     hbm_bytes_step = B * T * (52 * 4 + 3 * 4)  # metrics written + drivers read (algorithmic)
-    launch_s = t_dev / args.steps / world if world == 1 else t_dev / args.steps
     hbm_gbs = hbm_bytes_step / launch_s / 1e9
     line = {
         'metric': METRIC, 'value': value, 'unit': METRIC, 'n_gpus': world, 'steps': args.steps,
@@ -286,22 +285,31 @@ def bench_gpu(args):
         'e2e': {'value': e2e_value, 'unit': METRIC, 'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': int(d2h),
                 'warmup_calls': E2E_WARMUP},
         'gpu_launches': args.steps,
-        'roofline': {'bound': 'hbm', 'achieved': hbm_gbs, 'peak': peaks['hbm_gbs'], 'unit': 'GB/s',
-                     'frac': hbm_gbs / peaks['hbm_gbs'], 'peak_source': peak_source,
+        'roofline': {'bound': 'fp32', 'achieved': achieved_tf, 'peak': fp32_peak, 'unit': 'TFLOP/s',
+                     'frac': achieved_tf / fp32_peak,
+                     'peak_source': f'148 SMs x 128 FP32 lanes x 2 x median SM clock under load ({sm_mhz:.0f} MHz); '
+                                    'no measured FP32 figure exists for this pool',
+                     'flops_per_condition_step': flops, 'sfu_calls_per_condition_step': sfu,
+                     'flops_source': 'op-counting run of the oracle (python -m oracle.opcount): per step '
+                                     f"{OPCOUNT_2X2['per_step_flops']:.0f} + {iters_mean:.3f} Newton iterations x "
+                                     f"{OPCOUNT_2X2['per_newton_flops']:.0f} + one sampling and one absorbing "
+                                     f'table build per condition over {T} steps',
                      'traffic': args.traffic if args.traffic is not None else (
                          TRAFFIC_PER_LAUNCH if (B, T, args.precision) == (256, 500, 'mixed') else None),
-                     'traffic_unit': 'bytes per launch',
-                     'note': 'state stays in shared memory; algorithmic HBM bytes = 220 B per condition-step '
-                             '(28.16 MB per launch); traffic = dram__bytes_read.sum + dram__bytes_write.sum of '
-                             'one full launch of this workload (ncu, one pass)'},
-        'roofline_fp32': {'bound': 'fp32 cuda-core issue', 'achieved': achieved_tf, 'peak': fp32_peak,
-                          'unit': 'TFLOP/s', 'frac': achieved_tf / fp32_peak,
-                          'flops_per_condition_step': flops,
-                          'peak_basis': f'148 SMs x 128 lanes x 2 x median SM clock {sm_mhz:.0f} MHz'},
+                     'traffic_unit': 'DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum, ncu)',
+                     'note': 'not a tensor-core contraction and not HBM-bound: state stays on chip, the step is a '
+                             'chain of dependent CUDA-core and shared-memory operations per condition'},
+        'roofline_hbm': {'bound': 'hbm', 'achieved': hbm_gbs, 'peak': peaks['hbm_gbs'], 'unit': 'GB/s',
+                         'frac': hbm_gbs / peaks['hbm_gbs'], 'peak_source': peak_source,
+                         'algorithmic_bytes_per_condition_step': 220},
         'clocks': clocks,
     }
-    if args.serve_requests > 0 and rank == 0:
-        line['serving'] = bench_serving(args, local)
+    if rank == 0 and not args.no_workloads:
+        line['uneven'] = measure_uneven(args)
+        sin, _, _ = measure_sinusoid(args)
+        line['sinusoid'] = sin
+        if args.serve_requests > 0:
+            line['serving'] = measure_serving(args)
     if rank == 0 and not args.no_cpu_baseline:
         line['cpu_baseline'] = cpu_baseline(args)
     if rank == 0:
@@ -380,10 +388,12 @@ def _oracle_sample(args_tuple):
     return time.perf_counter() - t0
 
 
-def cpu_baseline(args, cores=1, n_cond=2, T=20):
-    """The oracle (NumPy restatement of the reference timestep) on host cores."""
+def cpu_baseline(args, cores=1, n_cond=8, T=150):
+    """The oracle (NumPy restatement of the reference timestep) on host cores:
+    n_cond conditions spread over the sweep's pCa range (its keys), T steps each."""
     os.environ.setdefault('OMP_NUM_THREADS', '1')
-    jobs = [(2, 2, T, float(p), i) for i, p in enumerate(np.linspace(4.0, 7.0, n_cond))]
+    idx = np.linspace(0, 255, n_cond).round().astype(int)
+    jobs = [(2, 2, T, float(np.linspace(4.0, 7.0, 256)[i]), int(i)) for i in idx]
     t0 = time.perf_counter()
     if cores > 1:
         import multiprocessing as mp
@@ -394,7 +404,8 @@ def cpu_baseline(args, cores=1, n_cond=2, T=20):
             _oracle_sample(j)
     dt = time.perf_counter() - t0
     return {'value': n_cond * T / dt, 'unit': METRIC, 'cores': cores, 'kind': 'port',
-            'sample': f'{n_cond} conditions x {T} timesteps of the 2x2 pCa sweep (oracle, NumPy float32)'}
+            'sample': f'{n_cond} conditions of the 2x2 pCa sweep (pCa spread over 4..7, their sweep keys) x '
+                      f'{T} timesteps (oracle, NumPy float32)'}
 
 
 def bench_reference(args):
@@ -468,6 +479,128 @@ def uneven_conditions(n=512, seed=0):
                           pCa=float(rng.uniform(4, 7)), duration_ms=float(int(rng.uniform(200, 1000))),
                           K_lat=5.0, nu=0.5, dynamic_params=d, key=keys[i]))
     return conds, topos
+
+
+def measure_uneven(args):
+    """Uneven-batch workload (one run_conditions call, host arrays in and
+    host metrics out): 512 conditions of lattices 1-4 x 1-4, lattice spacing
+    solved as an unknown, default CTA sizes."""
+    import torch
+    from multifil_jax_b200 import run_conditions
+    conds, topos = uneven_conditions()
+    total = sum(int(c['duration_ms']) for c in conds)
+    run_conditions(conds, precision=args.precision)  # warm-up: every kernel variant loaded
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    run_conditions(conds, precision=args.precision)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    return {'workload': '512 conditions, nrows/ncols ~ U{1..4}, z ~ U[850,1000] nm, pCa ~ U[4,7], '
+                        '200-1000 ms at dt 1 ms, dynamic lattice spacing (K_lat 5, nu 0.5), skeletal, '
+                        'keys split(PRNGKey(0),512), one launch through run_conditions',
+            'conditions': len(conds), 'condition_timesteps': total, 'value': total / wall, 'unit': METRIC,
+            'wall_s': wall, 'precision': args.precision}
+
+
+def measure_sinusoid(args, modes=('mixed',)):
+    """Sinusoid workload: 512 conditions of uneven length and dt in one launch
+    per precision mode (device-timed); returns throughput and the forces."""
+    import torch
+    from multifil_jax_b200 import SarcTopology, get_skeletal_params
+    from multifil_jax_b200.engine import get_engine, upload, MF_FLAG_PRECISE
+    s, d = get_skeletal_params()
+    topo = SarcTopology.create(2, 2, s, d)
+    eng = get_engine(0)
+    dev = torch.device('cuda', 0)
+    conds = sinusoid_conditions()
+    B, T = len(conds), max(c[2] for c in conds)
+    Z = np.zeros((B, T), np.float32)
+    NS = np.zeros(B, np.int32)
+    DT = np.zeros(B, np.float32)
+    KEYS = np.zeros((B, 2), np.uint32)
+    for i, (f, dt, n, z, key) in enumerate(conds):
+        Z[i, :n], Z[i, n:] = z, z[-1]
+        NS[i], DT[i], KEYS[i] = n, dt, key
+    P = np.tile(d.param_row(), (B, 1)).astype(np.float32)
+    PC = np.full((B, T), 4.5, np.float32)
+    L = np.full((B, T), 14.0, np.float32)
+    total = int(NS.sum())
+    out = {'workload': '2x2 skeletal, pCa 4.5, z = 900 + 2 sin(2 pi f t) nm, f = logspace(0, 2.7, 64) Hz x 8 '
+                       'seeds, dt = min(1, 1000/(20 f)) ms, 5 cycles (>= 200 ms), one launch per mode',
+           'conditions': B, 'condition_timesteps': total, 'unit': METRIC}
+    forces = {}
+    for name in modes:
+        flags = MF_FLAG_PRECISE if name == 'mixed' else 0
+        a = upload(dev, P, Z, PC, L, NS, KEYS.view(np.int32), np.zeros(B, np.float32), np.zeros(B, np.float32), DT)
+        kw = dict(K_lat=a[6], nu=a[7], dt=a[8], n_newton=s.n_newton_steps, n_cg=s.n_cg_steps, flags=flags)
+        eng.run_batch(topo, *a[:6], **kw)  # warm-up
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res = eng.run_batch(topo, *a[:6], **kw)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        forces[name] = res['metrics'][:, 0, :].cpu().numpy()
+        out[f'{name}_value'] = total / (ms / 1e3)
+        out[f'{name}_ms'] = ms
+    return out, conds, forces
+
+
+def measure_serving(args):
+    """Serving workload: capacity of the request mix (every request at t = 0),
+    then a Poisson stream at a fraction of that capacity, and the plain path on
+    a sample of the same mix for the served-over-plain ratio."""
+    cap_args = argparse.Namespace(**vars(args))
+    cap_args.serve_requests = args.serve_capacity_requests
+    cap_args.serve_rate = 1e9
+    cap = bench_serving(cap_args, 0)
+    cap_req = cap['requests'] / cap['wall_s']
+    run_args = argparse.Namespace(**vars(args))
+    run_args.serve_rate = args.serve_load * cap_req
+    res = bench_serving(run_args, 0)
+    plain = plain_on_request_mix(args)
+    res.update({'capacity_requests_per_s': cap_req,
+                'capacity_condition_timesteps_per_s': cap['condition_timesteps_per_s'],
+                'load_fraction_of_capacity': args.serve_load,
+                'plain_condition_timesteps_per_s': plain['value'],
+                'served_over_plain': res['condition_timesteps_per_s'] / plain['value'],
+                'capacity_over_plain': cap['condition_timesteps_per_s'] / plain['value'],
+                'plain_sample': plain['sample']})
+    return res
+
+
+def plain_on_request_mix(args, n=32, steps=40):
+    """The plain form (one condition per launch, one launch per timestep) on
+    the first n requests of the serving mix, each cut to `steps` steps."""
+    import torch
+    from multifil_jax_b200 import SarcTopology, get_skeletal_params, get_cardiac_params
+    from multifil_jax_b200.engine import get_engine, upload, prng_split, prng_key, MF_FLAG_PLAIN, MF_FLAG_PRECISE
+    rng = np.random.default_rng(1)
+    eng = get_engine(0)
+    dev = torch.device('cuda', 0)
+    flags = MF_FLAG_PLAIN | (MF_FLAG_PRECISE if args.precision == 'mixed' else 0)
+    total_t = 0.0
+    for i in range(n):
+        r, c = (int(v) for v in rng.integers(1, args.serve_max_lattice + 1, 2))
+        sp = get_skeletal_params() if rng.random() < 0.5 else get_cardiac_params()
+        rng.uniform(args.serve_min_ms, args.serve_max_ms)
+        pca, z = float(rng.uniform(4, 7)), float(rng.uniform(850, 1000))
+        topo = SarcTopology.create(r, c, *sp)
+        key = prng_split(prng_key(1000 + i), 1)[0]
+        a = upload(dev, sp[1].param_row()[None].astype(np.float32), np.full((1, steps), z, np.float32),
+                   np.full((1, steps), pca, np.float32), np.full((1, steps), 14.0, np.float32),
+                   np.array([steps], np.int32), key[None].view(np.int32), np.zeros(1, np.float32),
+                   np.zeros(1, np.float32), np.ones(1, np.float32))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        eng.run_batch(topo, *a[:6], K_lat=a[6], nu=a[7], dt=a[8], flags=flags)
+        e1.record()
+        torch.cuda.synchronize()
+        total_t += e0.elapsed_time(e1) / 1e3
+    return {'value': n * steps / total_t,
+            'sample': f'the first {n} requests of the mix, {steps} steps each, one launch per step'}
 
 
 def study_uneven(args):
@@ -545,45 +678,11 @@ def study_sinusoid(args):
     in one launch per precision mode: throughput, and how far the float32
     mode's complex stiffness sits from the mixed mode's per frequency.  The
     FP64-oracle comparison of this workload is tests/test_gpu_precision_study.py."""
-    import torch
-    from multifil_jax_b200 import SarcTopology, get_skeletal_params
-    from multifil_jax_b200.engine import get_engine, upload, MF_FLAG_PRECISE
-    s, d = get_skeletal_params()
-    topo = SarcTopology.create(2, 2, s, d)
-    eng = get_engine(0)
-    dev = torch.device('cuda', 0)
-    conds = sinusoid_conditions()
-    B, T = len(conds), max(c[2] for c in conds)
-    Z = np.zeros((B, T), np.float32)
-    NS = np.zeros(B, np.int32)
-    DT = np.zeros(B, np.float32)
-    KEYS = np.zeros((B, 2), np.uint32)
-    for i, (f, dt, n, z, key) in enumerate(conds):
-        Z[i, :n], Z[i, n:] = z, z[-1]
-        NS[i], DT[i], KEYS[i] = n, dt, key
-    P = np.tile(d.param_row(), (B, 1)).astype(np.float32)
-    PC = np.full((B, T), 4.5, np.float32)
-    L = np.full((B, T), 14.0, np.float32)
-    total = int(NS.sum())
-    out = {'study': 'sinusoid', 'metric': METRIC, 'conditions': B, 'condition_timesteps': total,
-           'workload': '2x2 skeletal, pCa 4.5, z = 900 + 2 sin(2 pi f t) nm, f = logspace(0, 2.7, 64) Hz x 8 '
-                       'seeds, dt = min(1, 1000/(20 f)) ms, 5 cycles (>= 200 ms), one launch per mode'}
-    Y = {}
-    for name, flags in (('mixed', MF_FLAG_PRECISE), ('float32', 0)):
-        a = upload(dev, P, Z, PC, L, NS, KEYS.view(np.int32), np.zeros(B, np.float32), np.zeros(B, np.float32), DT)
-        kw = dict(K_lat=a[6], nu=a[7], dt=a[8], n_newton=s.n_newton_steps, n_cg=s.n_cg_steps, flags=flags)
-        eng.run_batch(topo, *a[:6], **kw)  # warm-up
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        res = eng.run_batch(topo, *a[:6], **kw)
-        e1.record()
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
-        force = res['metrics'][:, 0, :].cpu().numpy()
-        Y[name] = np.array([stiffness(force[i, :c[2]], c[3], c[0], c[1]) for i, c in enumerate(conds)])
-        out[f'{name}_value'] = total / (ms / 1e3)
-        out[f'{name}_ms'] = ms
+    out, conds, forces = measure_sinusoid(args, modes=('mixed', 'float32'))
+    out['study'] = 'sinusoid'
+    out['metric'] = METRIC
+    Y = {name: np.array([stiffness(f[i, :c[2]], c[3], c[0], c[1]) for i, c in enumerate(conds)])
+         for name, f in forces.items()}
     rel = np.abs(Y['float32'] - Y['mixed']) / np.abs(Y['mixed'])
     fr = np.array([c[0] for c in conds])
     out['float32_vs_mixed_stiffness'] = {
@@ -622,16 +721,21 @@ def main():
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--precision', default='mixed', choices=['float32', 'mixed'])
-    ap.add_argument('--plain-conditions', type=int, default=8)
-    ap.add_argument('--serve-requests', type=int, default=300)
+    ap.add_argument('--plain-conditions', type=int, default=256)
+    ap.add_argument('--serve-requests', type=int, default=10000)
     ap.add_argument('--serve-rate', type=float, default=200.0)
+    ap.add_argument('--serve-load', type=float, default=0.5,
+                    help='arrival rate of the bench line\'s serving run, as a fraction of the measured capacity')
+    ap.add_argument('--serve-capacity-requests', type=int, default=2000)
     ap.add_argument('--serve-max-lattice', type=int, default=6)
     ap.add_argument('--serve-min-ms', type=float, default=100.0)
-    ap.add_argument('--serve-max-ms', type=float, default=400.0)
+    ap.add_argument('--serve-max-ms', type=float, default=2000.0)
     ap.add_argument('--serve-chunk', type=int, default=25)
     ap.add_argument('--serve-budget-gb', type=int, default=8)
     ap.add_argument('--traffic', type=float, default=None)
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-workloads', action='store_true',
+                    help='leave the uneven, sinusoid and serving workloads out of the bench line')
     ap.add_argument('--study', default=None, choices=['uneven', 'serving', 'sinusoid'],
                     help='run one workload study instead of the bench line')
     ap.add_argument('--study-capacity-requests', type=int, default=2000)

@@ -1,7 +1,9 @@
 """Operation counts of one timestep of the reference algorithm, by phase.
 
-TEST INFRASTRUCTURE (oracle), used by ``bench.py`` for the roofline numerator
-and by ``tests/test_opcount.py``.  The oracle's own timestep
+TEST INFRASTRUCTURE (oracle).  ``python -m oracle.opcount`` prints the
+counts; the 2x2 figures are the roofline numerator ``bench.py`` uses (as
+constants, checked against a fresh count by ``tests/test_opcount.py``).  The
+oracle's own timestep
 (``oracle.step.timestep``, which restates timestep.py:65-199 and
 solver.py:329-771) is run once on arrays of :class:`Counted`, an ndarray
 subclass that counts every floating-point element operation NumPy performs
@@ -95,14 +97,9 @@ class Counted(np.ndarray):
         return _wrap(result)
 
     def __array_function__(self, func, types, args, kwargs):
-        def unwrap(v):
-            if isinstance(v, Counted):
-                return _plain(v)
-            if isinstance(v, (list, tuple)):
-                return type(v)(unwrap(x) for x in v)
-            return v
-        result = func(*unwrap(args), **{k: unwrap(v) for k, v in kwargs.items()})
-        return _wrap(result)
+        # NumPy's own implementation on the counted arrays, so that the ufuncs
+        # it applies inside (np.sum, np.diff, np.cumsum, np.mean, ...) are counted
+        return _wrap(super().__array_function__(func, types, args, kwargs))
 
 
 @contextlib.contextmanager
@@ -134,15 +131,18 @@ def expm_flops(n: int, s: np.ndarray) -> int:
 
 
 class _Tracer:
-    """Runs the oracle's functions under the phase each belongs to."""
+    """Runs the oracle's functions under the phase each belongs to, counting calls."""
 
     def __init__(self):
         self.saved = []
+        self.calls = defaultdict(int)
 
     def patch(self, owner, name, label):
         fn = getattr(owner, name)
+        calls = self.calls
 
         def traced(*a, **k):
+            calls[label] += 1
             with phase(label):
                 return fn(*a, **k)
         self.saved.append((owner, name, fn))
@@ -197,33 +197,65 @@ def count_timestep(topo, row, c: OS.Condition, z: float, pCa: float, ls: float, 
         tr.restore()
         _state['counts'] = None
     out = {k: dict(v) for k, v in counts.items()}
+    out['calls'] = dict(tr.calls)
+    tr.calls.clear()
     for f in ('thick_x', 'thin_x', 'xb_dist'):
         setattr(nc, f, np.asarray(_plain(getattr(nc, f))))
     return out, nc, ex
 
 
-def per_step_counts(topo, row, pCa=4.5, z=900.0, ls=14.0, T=20, key=None, n_newton=4, n_cg=6):
-    """Mean counts per timestep over T steps of a fixed-spacing isometric run
-    (the first step's table builds reported apart, as a per-build figure)."""
+def unit_counts(topo, row, pCa=4.5, z=900.0, ls=14.0, T=20, key=None, n_newton=4, n_cg=6):
+    """Counts per unit of work over T steps of a fixed-spacing isometric run:
+    per step (nearest sites, both kinetics, the metrics, the first residual),
+    per Newton iteration (one residual, n_cg JVPs, n_cg + 1 preconditioner
+    applications, the CG vector updates), per table build and per absorbing
+    table build.  A step then costs per_step + iterations x per_newton flops,
+    and a launch adds one build of each table per (pCa, spacing) it meets."""
     from . import prng
     dt = np.float32
     p = ph.param_dict(row, dt)
     pre = ph.Preconditioner(topo, p, dt)
     c = OS.initial_condition(topo, p, z, n_newton, n_cg, dt, pre)
     key = prng.split(prng.PRNGKey(0), 1)[0] if key is None else np.asarray(key, np.uint32)
-    total = defaultdict(lambda: defaultdict(float))
-    iters = []
+    tot = defaultdict(lambda: defaultdict(float))
+    calls = defaultdict(int)
+    iters = 0
     build = None
     for t in range(T):
         ut, ux, key = prng.step_uniforms(key, topo.n_sites_total, topo.total_xbs)
         cnt, c, ex = count_timestep(topo, row, c, z, pCa, ls, ut, ux, n_newton, n_cg)
-        iters.append(ex['iters'])
+        iters += ex['iters']
+        for k, v in cnt.pop('calls').items():
+            calls[k] += v
         if build is None:
-            build = {k: cnt.get(k, {}) for k in ('tables', 'absorbing')}
+            build = {k: int(cnt[k]['flops']) for k in ('tables', 'absorbing')}
         for ph_name, kinds in cnt.items():
-            if ph_name in ('tables', 'absorbing'):
-                continue
             for kind, v in kinds.items():
-                total[ph_name][kind] += v / T
-    return {'per_step': {k: dict(v) for k, v in total.items()}, 'per_table_build': build,
-            'mean_newton_iters': float(np.mean(iters)), 'steps': T}
+                tot[ph_name][kind] += v
+    per_call = {k: {kind: v / max(calls[k], 1) for kind, v in tot[k].items()}
+                for k in ('residual', 'jvp', 'precond')}
+    fixed_phases = ('nearest', 'tm_kinetics', 'xb_kinetics', 'metrics')
+
+    def f(kind):
+        step = sum(tot[k][kind] for k in fixed_phases) / T + per_call['residual'].get(kind, 0.0)
+        newton = (per_call['residual'].get(kind, 0.0) + n_cg * per_call['jvp'].get(kind, 0.0)
+                  + (n_cg + 1) * per_call['precond'].get(kind, 0.0)
+                  + (tot['cg_vector'][kind] / iters if iters else 0.0))
+        return step, newton
+    step_f, newton_f = f('flops')
+    step_s, newton_s = f('sfu')
+    return {'per_step_flops': step_f, 'per_newton_flops': newton_f, 'per_step_sfu': step_s,
+            'per_newton_sfu': newton_s, 'table_build_flops': build['tables'],
+            'absorbing_build_flops': build['absorbing'], 'mean_newton_iters': iters / T, 'steps': T,
+            'phases_per_step': {k: {kind: v / T for kind, v in kinds.items()} for k, kinds in tot.items()
+                                if k not in ('tables', 'absorbing')},
+            'calls': dict(calls)}
+
+
+if __name__ == '__main__':
+    import json
+    from multifil_jax_b200 import SarcTopology, get_skeletal_params
+    s_, d_ = get_skeletal_params()
+    for n in (1, 2, 3, 4):
+        t_ = SarcTopology.create(n, n, s_, d_)
+        print(json.dumps({'lattice': f'{n}x{n}', **unit_counts(t_, d_.param_row())}))
