@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define MF_ABI_VERSION 1
+#define MF_ABI_VERSION 2
 
 /* error codes */
 #define MF_OK 0
@@ -59,6 +59,14 @@ extern "C" {
 
 #define MF_N_PARAMS 44
 #define MF_N_METRICS 52
+
+/* subpopulations (mf_batch.pop_*): reference core/subpopulation.py */
+#define MF_MAX_POPS 4              /* populations per condition */
+#define MF_POP_EXPLICIT 1          /* per-unit labels select a population's tables ('random',
+                                      'c_zone'); without it the K generators are blended
+                                      with the fractions ('mean_field') */
+#define MF_POP_XB 2                /* the populations change crossbridge rates (xb_* fields) */
+#define MF_POP_TM 4                /* the populations change tropomyosin rates (tm_* fields) */
 
 typedef struct mf_ctx mf_ctx;
 
@@ -111,6 +119,19 @@ typedef struct {
     float* x_trace;         /* [B*T_max*max_dof] node positions after each step or NULL */
     int8_t* state_trace;    /* [B*T_max*(max_xbs + max_sites)] xb then tm states or NULL */
     int32_t* bound_trace;   /* [B*T_max*(max_xbs + max_sites)] xb then thin bound_to or NULL */
+    /* Subpopulations (simulation.py:485-577 and the per-population branches of
+     * kernels/transitions.py:580-596, 925-994); n_pops <= 1: one population and
+     * the pop_* fields are ignored.  Mechanics always use `params`. */
+    int32_t n_pops;           /* K populations, 2..MF_MAX_POPS (population 0 = wild type) */
+    int32_t pop_flags;        /* MF_POP_EXPLICIT | MF_POP_XB | MF_POP_TM */
+    int32_t label_stride;     /* row stride of xb_label / tm_label (>= every condition's
+                                 total_xbs and n_sites_total) */
+    const float* pop_params;  /* [B*n_pops*44] device: each population's DynamicParams row */
+    const float* pop_frac;    /* [B*n_pops] device: blend weights (mean field) */
+    const int8_t* xb_label;   /* [B*label_stride] device: population of each head
+                                 (MF_POP_EXPLICIT with MF_POP_XB; values are clamped to [0, K)) */
+    const int8_t* tm_label;   /* [B*label_stride] device: population of each binding site
+                                 (MF_POP_EXPLICIT with MF_POP_TM) */
 } mf_batch;
 
 int mf_abi_version(void);
@@ -165,6 +186,68 @@ int mf_workspace_bytes(mf_ctx* ctx, const mf_batch* batch, uint64_t* bytes);
  * array (the region a call uses is zeroed before its kernels run); calls that
  * overlap on the GPU race on it and must be serialised by the caller. */
 int mf_run_batch_static(mf_ctx* ctx, const mf_batch* batch, void* stream);
+
+/* ---- one step of caller-owned states (the public timestep split) ------- */
+/* Phases of mf_step_states (reference timestep.py:65-199 and the functions it
+ * calls).  MF_PHASE_KINETICS is kinetics_step (nearest sites, tropomyosin and
+ * crossbridge transitions); MF_PHASE_TIMESTEP is timestep (kinetics, then the
+ * equilibrium solve); MF_PHASE_EQUILIBRIUM alone is solve_equilibrium
+ * (kernels/solver.py:663-771); MF_PHASE_NEAREST alone is
+ * update_nearest_neighbors (kernels/geometry.py:186-262). */
+#define MF_PHASE_NEAREST 1
+#define MF_PHASE_TRANSITIONS 2
+#define MF_PHASE_EQUILIBRIUM 4
+#define MF_PHASE_KINETICS (MF_PHASE_NEAREST | MF_PHASE_TRANSITIONS)
+#define MF_PHASE_TIMESTEP (MF_PHASE_KINETICS | MF_PHASE_EQUILIBRIUM)
+
+/* B states of one lattice held by the caller in the reference's State layout
+ * (core/state.py:69-113), row-major [B, ...] device arrays, updated in place.
+ * Float32 arithmetic (the reference's).  Drivers follow resolve_value
+ * (core/state.py:331-343): NULL or NaN entries take the constant from the
+ * parameter row. */
+typedef struct {
+    int32_t B;
+    int32_t topo_id;
+    int32_t phases;            /* MF_PHASE_* bits */
+    int32_t flags;             /* 0 or MF_FLAG_ORIGINAL_PRNG */
+    float dt;                  /* timestep (ms) of the transition tables */
+    int32_t n_newton;          /* Newton cap (solve_equilibrium's n_newton_steps) */
+    int32_t n_cg;              /* CG iterations per Newton step */
+    float* thick_axial;        /* [B*n_thick*n_crowns] thick.axial */
+    int8_t* xb_states;         /* [B*X] thick.xb_states */
+    int32_t* xb_bound_to;      /* [B*X] thick.xb_bound_to (-1 unbound) */
+    int32_t* xb_nearest_bs;    /* [B*X] thick.xb_nearest_bs */
+    float* xb_distances;       /* [B*X*2] thick.xb_distances (axial, radial) */
+    float* thin_axial;         /* [B*S] thin.axial */
+    int8_t* tm_states;         /* [B*S] thin.tm_states */
+    int32_t* thin_bound_to;    /* [B*S] thin.bound_to (-1 unbound) */
+    uint32_t* keys;            /* [B*2] jax.random key; advanced by the transitions phase */
+    const float* params;       /* [B*44] DynamicParams rows (the constants) */
+    const float* pCa;          /* [B] drivers or NULL */
+    const float* z_line;       /* [B] or NULL */
+    const float* lattice_spacing; /* [B] or NULL */
+    const float* K_lat;        /* [B] effective lattice stiffness (x n_thick) or NULL: fixed spacing */
+    const float* d_ref;        /* [B] reference spacing (with K_lat) */
+    float* residual_out;       /* [B] or NULL: max |F| after the solve (pN) */
+    float* ls_out;             /* [B] or NULL: lattice spacing after the solve */
+    int32_t* iters_out;        /* [B] or NULL: Newton iterations */
+    int32_t* status_out;       /* [B] or NULL: MF_STATUS_* bits */
+    int32_t n_pops, pop_flags, label_stride; /* subpopulations, as in mf_batch */
+    const float* pop_params;
+    const float* pop_frac;
+    const int8_t* xb_label;
+    const int8_t* tm_label;
+    const float* u_thin;       /* test hook: [B*S] injected uniforms or NULL */
+    const float* u_xb;         /* test hook: [B*X] injected uniforms or NULL */
+} mf_state_batch;
+
+/* Run the selected phases on every state of the batch (one CTA per state).
+ * Replaces the reference's kinetics_step / timestep / solve_equilibrium /
+ * update_nearest_neighbors (timestep.py:65-199, kernels/solver.py:663-771,
+ * kernels/geometry.py:186-262) for B states at once.  The transition
+ * tables are built on every call that samples.  Returns after `stream` has
+ * synchronised. */
+int mf_step_states(mf_ctx* ctx, const mf_state_batch* sb, void* stream);
 
 /* Test hook: the transition tables a condition's kernel builds for one
  * DynamicParams row `params` (host, 44 floats) at (pCa, lattice spacing d)

@@ -18,6 +18,8 @@ from .params import (StaticParams, DynamicParams, DYNAMIC_FIELDS, get_skeletal_p
                      get_cardiac_params)
 from .topology import SarcTopology  # noqa: F401
 from .simulation import run, run_conditions, SimulationResult, MetricsDict, METRIC_KEYS  # noqa: F401
+from .subpopulation import Subpopulation  # noqa: F401
+from . import timestep  # noqa: F401
 
 
 def get_ca_concentration(pCa: float) -> float:
@@ -25,6 +27,6 @@ def get_ca_concentration(pCa: float) -> float:
     return 10.0 ** (-pCa)
 
 
-__all__ = ['run', 'run_conditions', 'SimulationResult', 'SarcTopology', 'StaticParams', 'DynamicParams', 'DYNAMIC_FIELDS',
+__all__ = ['run', 'run_conditions', 'SimulationResult', 'SarcTopology', 'Subpopulation', 'timestep', 'StaticParams', 'DynamicParams', 'DYNAMIC_FIELDS',
            'get_skeletal_params', 'get_cardiac_params', 'get_ca_concentration', 'MetricsDict',
            'METRIC_KEYS']

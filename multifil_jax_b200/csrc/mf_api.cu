@@ -16,6 +16,7 @@
 #include "../../include/multifil_b200.h"
 #include "mf_kernel.cuh"
 #include "mf_launch.cuh"
+#include "mf_state.cuh"
 
 using namespace mf;
 
@@ -124,10 +125,11 @@ static int default_threads(const TopoDev& t, bool precise) {
 // register-resident CG covers the lattice (precise mode, allow_regs: batches
 // with n_cg > 0), else every CG vector in shared memory, else in the
 // workspace.  false when even that does not fit.
-static bool make_cfg(const TopoDev& t, int nt, bool precise, bool allow_regs, bool dyn, int smem_optin, Cfg& c) {
+static bool make_cfg(const TopoDev& t, int nt, bool precise, bool allow_regs, bool dyn, int smem_optin, Cfg& c,
+                     PopShape ps = PopShape()) {
   c.threads = nt;
   if (precise && allow_regs && regcg_fits(t, nt)) {
-    const size_t sm = smem_bytes(t, nt, LAYOUT_REGS, true, dyn);
+    const size_t sm = smem_bytes(t, nt, LAYOUT_REGS, true, dyn, ps);
     if (sm + kStaticSmem <= (size_t)smem_optin) {
       c.regs = true;
       c.vec_global = false;
@@ -136,29 +138,29 @@ static bool make_cfg(const TopoDev& t, int nt, bool precise, bool allow_regs, bo
     }
   }
   c.regs = false;
-  c.vec_global = smem_bytes(t, nt, LAYOUT_SMEM, precise, dyn) + kStaticSmem > (size_t)smem_optin;
-  c.smem_local = smem_bytes(t, nt, c.vec_global ? LAYOUT_GLOBAL : LAYOUT_SMEM, precise, dyn);
+  c.vec_global = smem_bytes(t, nt, LAYOUT_SMEM, precise, dyn, ps) + kStaticSmem > (size_t)smem_optin;
+  c.smem_local = smem_bytes(t, nt, c.vec_global ? LAYOUT_GLOBAL : LAYOUT_SMEM, precise, dyn, ps);
   return c.smem_local + kStaticSmem <= (size_t)smem_optin;
 }
 
 // The configuration a batch uses.  With the lattice spacing solved as an
 // unknown both transition tables (827 matrix exponentials) are rebuilt every
-// step, one matrix per thread: an untuned default below 512 threads is raised
-// to 512 (measured fastest for every lattice of 1x1 to 4x4 in that mode).
-static Cfg batch_cfg(const TopoHost& t, int pm, bool dyn, int n_cg, int smem_optin) {
+// step: an untuned default below 512 threads is raised to 512 (measured
+// fastest for every lattice of 1x1 to 4x4 in that mode).  false when the
+// batch's exact carve (its populations included) fits no layout.
+static bool batch_cfg(const TopoHost& t, int pm, bool dyn, int n_cg, PopShape ps, int smem_optin, Cfg& out) {
   Cfg c = t.cfg[pm];  // sized for a dynamic spacing (the larger carve)
   if (dyn && !c.tuned && c.threads < 512) {
     Cfg c5 = c;
-    if (make_cfg(t.dev, 512, pm != 0, true, true, smem_optin, c5)) c = c5;
+    if (make_cfg(t.dev, 512, pm != 0, true, true, smem_optin, c5, ps)) c = c5;
   }
   // the exact carve of this batch: no register layout without CG steps, no
-  // spacing derivatives with a fixed spacing
+  // spacing derivatives with a fixed spacing, the populations' tables
   Cfg e = c;
-  if (make_cfg(t.dev, c.threads, pm != 0, n_cg > 0, dyn, smem_optin, e)) {
-    e.tuned = c.tuned;
-    c = e;
-  }
-  return c;
+  if (!make_cfg(t.dev, c.threads, pm != 0, n_cg > 0, dyn, smem_optin, e, ps)) return false;
+  e.tuned = c.tuned;
+  out = e;
+  return true;
 }
 
 extern "C" {
@@ -328,18 +330,77 @@ int mf_tune_threads(mf_ctx* ctx, int32_t topo_id, int32_t threads) {
   return rc ? rc : mf_tune_threads_mode(ctx, topo_id, 1, threads);
 }
 
-static size_t slot_bytes(const TopoDev& t) {
+static size_t slot_bytes(const TopoDev& t, PopShape ps = PopShape()) {
   const CoefLayout cl = coef_layout(t);
-  return slot_layout(t.n_dof, t.total_xbs, t.n_sites_total, t.n_bins, cl.total).total;
+  return slot_layout(t.n_dof, t.total_xbs, t.n_sites_total, t.n_bins, cl.total, ps.kx(), ps.kt()).total;
+}
+
+// Subpopulation inputs of a call (mf_batch / mf_state_batch pop_* fields).
+struct PopArgs {
+  int n_pops, pop_flags, label_stride;
+  const float* pop_params;
+  const float* pop_frac;
+  const int8_t* xb_label;
+  const int8_t* tm_label;
+};
+
+// Subpopulation shape of a call, checked against every lattice it runs.
+static int check_pops(mf_ctx* ctx, const PopArgs& pa, const std::vector<const TopoDev*>& lattices, PopShape& ps) {
+  ps = PopShape();
+  if (pa.n_pops <= 1) return MF_OK;
+  if (pa.n_pops > MF_MAX_POPS) return fail(ctx, MF_ERR_INVALID, "n_pops %d above %d", pa.n_pops, MF_MAX_POPS);
+  if (pa.pop_flags & ~(MF_POP_EXPLICIT | MF_POP_XB | MF_POP_TM))
+    return fail(ctx, MF_ERR_INVALID, "unknown pop_flags bits");
+  ps.K = pa.n_pops;
+  ps.flags = pa.pop_flags;
+  if (!ps.active()) return MF_OK;
+  if (!pa.pop_params) return fail(ctx, MF_ERR_INVALID, "subpopulations need pop_params");
+  if ((ps.blend_xb() || ps.blend_tm()) && !pa.pop_frac)
+    return fail(ctx, MF_ERR_INVALID, "mean-field subpopulations need pop_frac");
+  if (ps.kx() > 1 && !pa.xb_label) return fail(ctx, MF_ERR_INVALID, "explicit crossbridge populations need xb_label");
+  if (ps.kt() > 1 && !pa.tm_label) return fail(ctx, MF_ERR_INVALID, "explicit tropomyosin populations need tm_label");
+  for (const TopoDev* td : lattices) {
+    if ((ps.kx() > 1 && pa.label_stride < td->total_xbs) || (ps.kt() > 1 && pa.label_stride < td->n_sites_total))
+      return fail(ctx, MF_ERR_INVALID, "label_stride %d below a condition's head or site count", pa.label_stride);
+    if ((long)ps.kx() * 2 * td->n_bins > 32767) return fail(ctx, MF_ERR_INVALID, "too many population table keys");
+  }
+  return MF_OK;
+}
+
+static int batch_pops(mf_ctx* ctx, const mf_batch* bt, PopShape& ps) {
+  std::vector<const TopoDev*> lat;
+  if (bt->n_pops > 1)
+    for (int i = 0; i < bt->B; ++i) {
+      const int id = bt->topo_id[i];
+      if (id < 0 || id >= (int)ctx->topos.size()) return fail(ctx, MF_ERR_NOTFOUND, "unknown topology %d", id);
+      lat.push_back(&ctx->topos[id]->dev);
+    }
+  const PopArgs pa{bt->n_pops, bt->pop_flags, bt->label_stride, bt->pop_params, bt->pop_frac, bt->xb_label,
+                   bt->tm_label};
+  return check_pops(ctx, pa, lat, ps);
+}
+
+// Population inputs of condition i in its descriptor.
+static void fill_pops(CondDesc& c, const mf_batch* bt, const PopShape& ps, int i) {
+  c.pop_params = c.pop_frac = nullptr;
+  c.xb_label = c.tm_label = nullptr;
+  if (!ps.active()) return;
+  c.pop_params = bt->pop_params + (size_t)i * ps.K * MF_N_PARAMS;
+  if (bt->pop_frac) c.pop_frac = bt->pop_frac + (size_t)i * ps.K;
+  if (ps.kx() > 1) c.xb_label = bt->xb_label + (size_t)i * bt->label_stride;
+  if (ps.kt() > 1) c.tm_label = bt->tm_label + (size_t)i * bt->label_stride;
 }
 
 int mf_workspace_bytes(mf_ctx* ctx, const mf_batch* bt, uint64_t* bytes) {
   if (!ctx || !bt || !bytes) return fail(ctx, MF_ERR_INVALID, "null argument");
+  PopShape ps;
+  const int prc = batch_pops(ctx, bt, ps);
+  if (prc) return prc;
   uint64_t tot = 0;
   for (int i = 0; i < bt->B; ++i) {
     const int id = bt->topo_id[i];
     if (id < 0 || id >= (int)ctx->topos.size()) return fail(ctx, MF_ERR_NOTFOUND, "unknown topology %d", id);
-    tot += slot_bytes(ctx->topos[id]->dev);
+    tot += slot_bytes(ctx->topos[id]->dev, ps);
   }
   *bytes = tot + sizeof(CondDesc) * (uint64_t)bt->B;
   return MF_OK;
@@ -373,8 +434,9 @@ static int ensure_cond(mf_ctx* ctx, size_t n) {
 }
 
 static StepArgs make_args(const mf_batch* bt, const CondDesc* dc, int flags, int max_dof, int max_x,
-                          int max_s) {
+                          int max_s, PopShape ps) {
   StepArgs a{};
+  a.pop = ps;
   a.cond = dc;
   a.T = bt->T_max;
   a.n_newton = bt->n_newton;
@@ -403,6 +465,9 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
   if (bt->n_newton < 0 || bt->n_cg < 0) return fail(ctx, MF_ERR_INVALID, "negative solver caps");
   if ((bt->flags & MF_FLAG_DYNAMIC_LS) && (!bt->K_lat || !bt->nu))
     return fail(ctx, MF_ERR_INVALID, "dynamic lattice spacing needs K_lat and nu");
+  PopShape ps;
+  int rc = batch_pops(ctx, bt, ps);
+  if (rc) return rc;
   CK(cudaSetDevice(ctx->device));
   cudaStream_t st = (cudaStream_t)stream_v;
   const int B = bt->B;
@@ -424,19 +489,23 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
     max_dof = std::max(max_dof, td.n_dof);
     max_x = std::max(max_x, td.total_xbs);
     max_s = std::max(max_s, td.n_sites_total);
-    off += slot_bytes(td);
+    off += slot_bytes(td, ps);
   }
-  int rc = ensure_ws(ctx, off);
+  // CTA configuration of every condition
+  const int pm = (bt->flags & MF_FLAG_PRECISE) ? 1 : 0;
+  const bool dynb = (bt->flags & MF_FLAG_DYNAMIC_LS) != 0;
+  std::vector<Cfg> cfgs(B);
+  for (int i = 0; i < B; ++i)
+    if (!batch_cfg(*ctx->topos[bt->topo_id[i]], pm, dynb, bt->n_cg, ps, ctx->smem_optin, cfgs[i]))
+      return fail(ctx, MF_ERR_INVALID, "condition %d: its lattice and populations exceed shared memory", i);
+  rc = ensure_ws(ctx, off);
   if (rc) return rc;
   // order: group by (threads, vec_global), longest work first inside a group
   std::vector<int> order(B);
   for (int i = 0; i < B; ++i) order[i] = i;
-  const int pm = (bt->flags & MF_FLAG_PRECISE) ? 1 : 0;
-  const bool dynb = (bt->flags & MF_FLAG_DYNAMIC_LS) != 0;
   auto key_of = [&](int i) {
     const TopoHost& t = *ctx->topos[bt->topo_id[i]];
-    const Cfg c = batch_cfg(t, pm, dynb, bt->n_cg, ctx->smem_optin);
-    return std::make_pair(c.group_key(), -(long)n_steps[i] * t.dev.n_dof);
+    return std::make_pair(cfgs[i].group_key(), -(long)n_steps[i] * t.dev.n_dof);
   };
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key_of(a) < key_of(b); });
   off = 0;
@@ -461,7 +530,8 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
     hc[k].K_lat = h_K[i];
     hc[k].nu = h_nu[i];
     hc[k].dt = h_dt[i];
-    off += slot_bytes(t.dev);
+    fill_pops(hc[k], bt, ps, i);
+    off += slot_bytes(t.dev, ps);
   }
   int base_flags = 0;
   if (bt->flags & MF_FLAG_DYNAMIC_LS) base_flags |= FLAG_DYN;
@@ -473,10 +543,10 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
   struct Group { int begin, end, threads, key, lflags; size_t smem; };
   std::vector<Group> groups;
   for (int k = 0; k < B;) {
-    const Cfg c0 = batch_cfg(*ctx->topos[bt->topo_id[order[k]]], pm, dynb, bt->n_cg, ctx->smem_optin);
+    const Cfg& c0 = cfgs[order[k]];
     Group g{k, k, c0.threads, c0.group_key(), c0.layout_flags(), 0};
     while (g.end < B) {
-      const Cfg ck = batch_cfg(*ctx->topos[bt->topo_id[order[g.end]]], pm, dynb, bt->n_cg, ctx->smem_optin);
+      const Cfg& ck = cfgs[order[g.end]];
       if (ck.group_key() != g.key) break;
       g.smem = std::max(g.smem, ck.smem_local);
       ++g.end;
@@ -508,7 +578,7 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
     CK(cudaMemcpyAsync(ctx->d_cond, rows.data(), sizeof(CondDesc) * rows.size(), cudaMemcpyHostToDevice, st));
     for (auto& lr : launches) {
       const Group& g = groups[lr.second];
-      StepArgs a = make_args(bt, ctx->d_cond, base_flags | g.lflags, max_dof, max_x, max_s);
+      StepArgs a = make_args(bt, ctx->d_cond, base_flags | g.lflags, max_dof, max_x, max_s, ps);
       cudaError_t e = launch(g.threads, a, 1, lr.first, g.smem, st);
       if (e != cudaSuccess) return fail(ctx, MF_ERR_CUDA, "plain launch: %s", cudaGetErrorString(e));
     }
@@ -535,7 +605,8 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
   for (int c = 0; c < n_chunks; ++c)
     for (const Group& g : groups)
       launches.push_back({g.threads, g.end - g.begin, g.begin, g.smem,
-                          make_args(bt, ctx->d_cond + (size_t)c * B, base_flags | g.lflags, max_dof, max_x, max_s)});
+                          make_args(bt, ctx->d_cond + (size_t)c * B, base_flags | g.lflags, max_dof, max_x, max_s,
+                                    ps)});
   const bool use_graph = !(bt->flags & MF_FLAG_NO_GRAPH) && n_chunks > 1;
   if (!use_graph) {
     for (const Launch& l : launches) {
@@ -561,6 +632,7 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
     put(&a.u_thin, sizeof a.u_thin); put(&a.u_xb, sizeof a.u_xb); put(&a.x_trace, sizeof a.x_trace);
     put(&a.st_trace, sizeof a.st_trace); put(&a.bd_trace, sizeof a.bd_trace); put(&a.max_dof, sizeof a.max_dof);
     put(&a.max_xbs, sizeof a.max_xbs); put(&a.max_sites, sizeof a.max_sites);
+    put(&a.pop.K, sizeof a.pop.K); put(&a.pop.flags, sizeof a.pop.flags);
   }
   if (!ctx->graph_exec || sig != ctx->graph_sig) {
     // capture on a private non-blocking stream (the caller's may be the legacy
@@ -619,7 +691,7 @@ __global__ void tables_probe_kernel(const float* params, const float* centers, i
   for (int i = threadIdx.x; i < kNParams; i += blockDim.x) P[i] = params[i];
   __syncthreads();
   build_tables_block(P, centers, nb, pCa, d, dt, sq64, cum_tm, cum_xb, pabs, true, true, true, nullptr, 0,
-                     (int)threadIdx.x, (int)blockDim.x);
+                     (int)threadIdx.x, (int)blockDim.x, PopShape(), nullptr, nullptr);
 }
 
 }  // namespace
@@ -701,6 +773,11 @@ int mf_run_batch_static(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
     return fail(ctx, MF_ERR_INVALID, "dynamic lattice spacing needs K_lat and nu");
   if (bt->n_newton < 0 || bt->n_cg < 0) return fail(ctx, MF_ERR_INVALID, "negative solver caps");
   if (ctx->device < 0 || ctx->device >= kMaxDevices) return fail(ctx, MF_ERR_INVALID, "device index out of range");
+  PopShape ps;
+  {
+    const int prc = batch_pops(ctx, bt, ps);
+    if (prc) return prc;
+  }
   CK(cudaSetDevice(ctx->device));
   // one-time set-up on this device, with the device current
   const int dev = ctx->device;
@@ -733,21 +810,24 @@ int mf_run_batch_static(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
     max_dof = std::max(max_dof, td.n_dof);
     max_x = std::max(max_x, td.total_xbs);
     max_s = std::max(max_s, td.n_sites_total);
-    need += slot_bytes(td);
+    need += slot_bytes(td, ps);
   }
   if (need > kStaticScratchBytes)
     return fail(ctx, MF_ERR_NOMEM,
                 "mf_run_batch_static: batch needs %zu B of scratch, the static array holds %zu B "
                 "(split the batch or use mf_run_batch)", need, kStaticScratchBytes);
   // group by CTA configuration exactly as mf_run_batch does
-  std::vector<int> order(B);
-  for (int i = 0; i < B; ++i) order[i] = i;
   const int pm = (bt->flags & MF_FLAG_PRECISE) ? 1 : 0;
   const bool dynb = (bt->flags & MF_FLAG_DYNAMIC_LS) != 0;
+  std::vector<Cfg> cfgs(B);
+  for (int i = 0; i < B; ++i)
+    if (!batch_cfg(*ctx->topos[bt->topo_id[i]], pm, dynb, bt->n_cg, ps, ctx->smem_optin, cfgs[i]))
+      return fail(ctx, MF_ERR_INVALID, "condition %d: its lattice and populations exceed shared memory", i);
+  std::vector<int> order(B);
+  for (int i = 0; i < B; ++i) order[i] = i;
   auto key_of = [&](int i) {
     const TopoHost& t = *ctx->topos[bt->topo_id[i]];
-    const Cfg c = batch_cfg(t, pm, dynb, bt->n_cg, ctx->smem_optin);
-    return std::make_pair(c.group_key(), -(long)n_steps[i] * t.dev.n_dof);
+    return std::make_pair(cfgs[i].group_key(), -(long)n_steps[i] * t.dev.n_dof);
   };
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key_of(a) < key_of(b); });
   CondDesc* d_desc = reinterpret_cast<CondDesc*>(base);
@@ -775,7 +855,8 @@ int mf_run_batch_static(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
     c.K_lat = h_K[i];
     c.nu = h_nu[i];
     c.dt = h_dt[i];
-    off += slot_bytes(t.dev);
+    fill_pops(c, bt, ps, i);
+    off += slot_bytes(t.dev, ps);
   }
   // The array keeps whatever the previous call left.  The kernel rebuilds
   // every workspace field at step 0, but the region this call uses is zeroed
@@ -789,21 +870,123 @@ int mf_run_batch_static(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
   if (bt->flags & MF_FLAG_PRECISE) flags |= FLAG_PRECISE;
   if (bt->flags & MF_FLAG_ORIGINAL_PRNG) flags |= FLAG_ORIG_PRNG;
   for (int k = 0; k < B;) {
-    const Cfg c0 = batch_cfg(*ctx->topos[bt->topo_id[order[k]]], pm, dynb, bt->n_cg, ctx->smem_optin);
+    const Cfg& c0 = cfgs[order[k]];
     int e = k;
     size_t smem = 0;
     while (e < B) {
-      const Cfg ck = batch_cfg(*ctx->topos[bt->topo_id[order[e]]], pm, dynb, bt->n_cg, ctx->smem_optin);
+      const Cfg& ck = cfgs[order[e]];
       if (ck.group_key() != c0.group_key()) break;
       smem = std::max(smem, ck.smem_local);
       ++e;
     }
-    StepArgs a = make_args(bt, d_desc, flags | c0.layout_flags(), max_dof, max_x, max_s);
+    StepArgs a = make_args(bt, d_desc, flags | c0.layout_flags(), max_dof, max_x, max_s, ps);
     cudaError_t err = launch(c0.threads, a, e - k, k, smem, st);
     if (err != cudaSuccess) return fail(ctx, MF_ERR_CUDA, "static launch: %s", cudaGetErrorString(err));
     k = e;
   }
   CK(cudaStreamSynchronize(st));  // the host descriptor staging vector dies here
+  return MF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// One step of caller-owned states (state_kernel, mf_state.cuh).
+// ---------------------------------------------------------------------------
+static cudaError_t prepare_state(int nt, bool dyn, size_t smem) {
+#define MF_PREP_STATE_CASE(NT, D) \
+  if (nt == NT && dyn == (D != 0)) return prepare_state_##NT##_##D(smem);
+  MF_FOR_EACH_STATE_INSTANCE(MF_PREP_STATE_CASE)
+#undef MF_PREP_STATE_CASE
+  return cudaErrorInvalidValue;
+}
+
+static cudaError_t launch_state(int nt, bool dyn, const StepArgs& a, const StateIO& io, int grid, size_t smem,
+                                cudaStream_t st) {
+  cudaError_t e = prepare_state(nt, dyn, smem);
+  if (e != cudaSuccess) return e;
+  cudaGetLastError();
+#define MF_LAUNCH_STATE_CASE(NT, D) \
+  if (nt == NT && dyn == (D != 0)) return launch_state_##NT##_##D(a, io, grid, smem, st);
+  MF_FOR_EACH_STATE_INSTANCE(MF_LAUNCH_STATE_CASE)
+#undef MF_LAUNCH_STATE_CASE
+  return cudaErrorInvalidValue;
+}
+
+int mf_step_states(mf_ctx* ctx, const mf_state_batch* sb, void* stream_v) {
+  if (!ctx || !sb) return fail(ctx, MF_ERR_INVALID, "null argument");
+  if (sb->B < 0) return fail(ctx, MF_ERR_INVALID, "negative batch size");
+  if (sb->B == 0) return MF_OK;
+  if (sb->topo_id < 0 || sb->topo_id >= (int)ctx->topos.size()) return fail(ctx, MF_ERR_NOTFOUND, "unknown topology");
+  if (sb->phases & ~(MF_PHASE_NEAREST | MF_PHASE_TRANSITIONS | MF_PHASE_EQUILIBRIUM) || !sb->phases)
+    return fail(ctx, MF_ERR_INVALID, "phases must be a non-empty set of MF_PHASE_* bits");
+  if (sb->flags & ~MF_FLAG_ORIGINAL_PRNG) return fail(ctx, MF_ERR_INVALID, "only MF_FLAG_ORIGINAL_PRNG is accepted");
+  if (sb->n_newton < 0 || sb->n_cg < 0) return fail(ctx, MF_ERR_INVALID, "negative solver caps");
+  if (!sb->thick_axial || !sb->xb_states || !sb->xb_bound_to || !sb->xb_nearest_bs || !sb->xb_distances ||
+      !sb->thin_axial || !sb->tm_states || !sb->thin_bound_to || !sb->keys || !sb->params)
+    return fail(ctx, MF_ERR_INVALID, "missing state array");
+  const bool dyn = sb->K_lat != nullptr;
+  if (dyn && !sb->d_ref) return fail(ctx, MF_ERR_INVALID, "a dynamic lattice spacing needs d_ref with K_lat");
+  if ((sb->phases & MF_PHASE_TRANSITIONS) && !(sb->dt > 0.f)) return fail(ctx, MF_ERR_INVALID, "dt must be positive");
+  const TopoHost& th = *ctx->topos[sb->topo_id];
+  const TopoDev& td = th.dev;
+  PopShape ps;
+  const PopArgs pa{sb->n_pops, sb->pop_flags, sb->label_stride, sb->pop_params, sb->pop_frac, sb->xb_label,
+                   sb->tm_label};
+  int rc = check_pops(ctx, pa, {&td}, ps);
+  if (rc) return rc;
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t st = (cudaStream_t)stream_v;
+  // the float32 mode's CTA size (tuned or default), its exact carve
+  Cfg c;
+  if (!make_cfg(td, th.cfg[0].threads, false, false, dyn, ctx->smem_optin, c, ps))
+    return fail(ctx, MF_ERR_INVALID, "lattice and populations exceed shared memory");
+  const size_t stride = slot_bytes(td, ps);
+  rc = ensure_ws(ctx, stride * (size_t)sb->B);
+  if (rc) return rc;
+  StepArgs a{};
+  a.T = 1;
+  a.n_newton = sb->n_newton;
+  a.n_cg = sb->n_cg;
+  a.flags = (dyn ? FLAG_DYN : 0) | ((sb->flags & MF_FLAG_ORIGINAL_PRNG) ? FLAG_ORIG_PRNG : 0) | c.layout_flags();
+  a.resid_warn = INFINITY;
+  a.sq64_from = 1 << 20;
+  a.u_thin = sb->u_thin;
+  a.u_xb = sb->u_xb;
+  a.pop = ps;
+  StateIO io{};
+  io.topo = th.d_struct;
+  io.ws = ctx->ws;
+  io.ws_stride = stride;
+  io.thick_axial = sb->thick_axial;
+  io.xb_states = sb->xb_states;
+  io.xb_bound = sb->xb_bound_to;
+  io.xb_nearest = sb->xb_nearest_bs;
+  io.xb_dist = sb->xb_distances;
+  io.thin_axial = sb->thin_axial;
+  io.tm_states = sb->tm_states;
+  io.thin_bound = sb->thin_bound_to;
+  io.keys = sb->keys;
+  io.params = sb->params;
+  io.pCa = sb->pCa;
+  io.z = sb->z_line;
+  io.ls = sb->lattice_spacing;
+  io.K_lat = sb->K_lat;
+  io.d_ref = sb->d_ref;
+  io.resid_out = sb->residual_out;
+  io.ls_out = sb->ls_out;
+  io.iters_out = sb->iters_out;
+  io.status_out = sb->status_out;
+  if (ps.active()) {
+    io.pop_params = sb->pop_params;
+    io.pop_frac = sb->pop_frac;
+    io.xb_label = ps.kx() > 1 ? sb->xb_label : nullptr;
+    io.tm_label = ps.kt() > 1 ? sb->tm_label : nullptr;
+    io.label_stride = sb->label_stride;
+  }
+  io.phases = sb->phases;
+  io.dt = sb->dt;
+  cudaError_t e = launch_state(c.threads, dyn, a, io, sb->B, c.smem_local, st);
+  if (e != cudaSuccess) return fail(ctx, MF_ERR_CUDA, "state launch: %s", cudaGetErrorString(e));
+  CK(cudaStreamSynchronize(st));
   return MF_OK;
 }
 

@@ -116,7 +116,25 @@ struct SlotLayout {
 
 MF_HD size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
-MF_HD SlotLayout slot_layout(int n_dof, int X, int S, int n_bins, int coef_floats) {
+// Subpopulations of a batch (reference core/subpopulation.py): K populations,
+// flag bits POP_EXPLICIT (labels select a population's tables; else the K
+// generators are blended), POP_XB / POP_TM (the rate families they change).
+// K <= 1 is a single population.
+constexpr int POP_EXPLICIT = 1, POP_XB = 2, POP_TM = 4, kMaxPops = 4;
+struct PopShape {
+  int K = 1;
+  int flags = 0;
+  // crossbridge / tropomyosin table sets kept per condition
+  MF_HD int kx() const { return (K > 1 && (flags & (POP_EXPLICIT | POP_XB)) == (POP_EXPLICIT | POP_XB)) ? K : 1; }
+  MF_HD int kt() const { return (K > 1 && (flags & (POP_EXPLICIT | POP_TM)) == (POP_EXPLICIT | POP_TM)) ? K : 1; }
+  // blended (mean-field) generators of a family
+  MF_HD bool blend_xb() const { return K > 1 && (flags & (POP_EXPLICIT | POP_XB)) == POP_XB; }
+  MF_HD bool blend_tm() const { return K > 1 && (flags & (POP_EXPLICIT | POP_TM)) == POP_TM; }
+  // the population rows are read at all
+  MF_HD bool active() const { return K > 1 && (flags & (POP_XB | POP_TM)) != 0; }
+};
+
+MF_HD SlotLayout slot_layout(int n_dof, int X, int S, int n_bins, int coef_floats, int kx = 1, int kt = 1) {
   SlotLayout L{};
   size_t o = 0;
   L.x = o; o = align_up(o + sizeof(float) * n_dof, 16);
@@ -128,9 +146,9 @@ MF_HD SlotLayout slot_layout(int n_dof, int X, int S, int n_bins, int coef_float
   L.tm = o; o = align_up(o + S, 16);
   L.thin_bound = o; o = align_up(o + 2 * S, 16);
   L.misc = o; o = align_up(o + 64 * sizeof(double), 16);
-  L.cum_xb = o; o = align_up(o + sizeof(float) * 2 * n_bins * 36, 16);
-  L.pabs = o; o = align_up(o + sizeof(float) * 2 * n_bins * 3, 16);
-  L.cum_tm = o; o = align_up(o + sizeof(float) * 27 * 16, 16);
+  L.cum_xb = o; o = align_up(o + sizeof(float) * kx * 2 * n_bins * 36, 16);
+  L.pabs = o; o = align_up(o + sizeof(float) * kx * 2 * n_bins * 3, 16);
+  L.cum_tm = o; o = align_up(o + sizeof(float) * kt * 27 * 16, 16);
   L.coef = o; o = align_up(o + sizeof(float) * coef_floats, 16);
   L.vec = o; o = align_up(o + sizeof(float) * (7 * n_dof + 4 * X), 16);  // CG vectors + head terms when not in smem
   L.total = align_up(o, 256);

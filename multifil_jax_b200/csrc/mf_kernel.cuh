@@ -45,7 +45,8 @@ __host__ __device__ inline bool regcg_fits(const TopoDev& t, int nt) {
 // precision mode, layout and spacing mode (mirrors carve() below: every array
 // both modes use, plus the float32 scan-reversal buffers or the precise-mode
 // CG vectors w and s, and the per-head spacing derivatives when dyn).
-__host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, int layout, bool precise, bool dyn) {
+__host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, int layout, bool precise, bool dyn,
+                                             PopShape pop = PopShape()) {
   const bool vec_global = layout == LAYOUT_GLOBAL;
   const int N = t.n_dof, X = t.total_xbs, S = t.n_sites_total;
   const int nw = nt / 32;
@@ -63,8 +64,8 @@ __host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, int layou
   add(sizeof(int16_t) * S);                // thin_bound
   add(X);                                  // xb_state
   add(2 * S);                              // tm tm_new
-  add(sizeof(float) * 27 * 16);            // cum_tm
-  add(sizeof(float) * 6 * t.n_bins);       // pabs
+  add(sizeof(float) * pop.kt() * 27 * 16);  // cum_tm
+  add(sizeof(float) * pop.kx() * 6 * t.n_bins);  // pabs
   add(sizeof(float) * cl.total);           // coef
   if (!precise) add(sizeof(float) * nw * 128);  // scan reversal buffer per warp (filaments <= 128)
   add(sizeof(float) * kNParams);           // P
@@ -79,6 +80,12 @@ __host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, int layou
     add(sizeof(float) * t.n_thick_nodes);
     add(X);
     add(sizeof(int16_t) * X);
+  }
+  if (pop.active()) {                      // population rows, fractions, labels
+    add(sizeof(float) * pop.K * kNParams);
+    add(sizeof(float) * pop.K);
+    if (pop.kx() > 1) add(X);
+    if (pop.kt() > 1) add(S);
   }
   return o;
 }
@@ -125,8 +132,9 @@ __device__ void carve(Sim<NT, PR, DY>& m, char* base, int layout) {
   m.s.xb_state = (int8_t*)take(X);
   int8_t* t2 = (int8_t*)take(2 * S);
   m.s.tm = t2; m.s.tm_new = t2 + S;
-  m.s.cum_tm = (float*)take(sizeof(float) * 27 * 16);
-  m.s.pabs = (float*)take(sizeof(float) * 6 * t.n_bins);
+  const PopShape& pop = m.A.pop;
+  m.s.cum_tm = (float*)take(sizeof(float) * pop.kt() * 27 * 16);
+  m.s.pabs = (float*)take(sizeof(float) * pop.kx() * 6 * t.n_bins);
   m.s.coef = (float*)take(sizeof(float) * m.cl.total);
   m.s.scan = PR ? nullptr : (float*)take(sizeof(float) * NT / 32 * 128);
   m.s.P = (float*)take(sizeof(float) * kNParams);
@@ -149,6 +157,14 @@ __device__ void carve(Sim<NT, PR, DY>& m, char* base, int layout) {
     m.s.old_thick = reinterpret_cast<float*>(m.ws + m.L.x);
     m.s.old_xbs = reinterpret_cast<int8_t*>(m.ws + m.L.xb_state);
     m.s.old_key = reinterpret_cast<int16_t*>(m.ws + m.L.xb_near);
+  }
+  m.s.Pk = m.s.fk = nullptr;
+  m.s.xlab = m.s.tlab = nullptr;
+  if (pop.active()) {
+    m.s.Pk = (float*)take(sizeof(float) * pop.K * kNParams);
+    m.s.fk = (float*)take(sizeof(float) * pop.K);
+    if (pop.kx() > 1) m.s.xlab = (int8_t*)take(X);
+    if (pop.kt() > 1) m.s.tlab = (int8_t*)take(S);
   }
 }
 
@@ -418,7 +434,8 @@ __device__ void run_condition(const StepArgs& A, int ci) {
     sh_cd = A.cond[ci];
     sh_T = *sh_cd.topo;
     sh_cl = coef_layout(sh_T);
-    sh_L = slot_layout(sh_T.n_dof, sh_T.total_xbs, sh_T.n_sites_total, sh_T.n_bins, sh_cl.total);
+    sh_L = slot_layout(sh_T.n_dof, sh_T.total_xbs, sh_T.n_sites_total, sh_T.n_bins, sh_cl.total, A.pop.kx(),
+                       A.pop.kt());
   }
   __syncthreads();
   const CondDesc& cd = sh_cd;
@@ -451,6 +468,16 @@ __device__ void run_condition(const StepArgs& A, int ci) {
 #define MF_WS(type, field) reinterpret_cast<type*>(m.ws + m.L.field)
 
   for (int i = m.tid; i < kNParams; i += NT) m.s.P[i] = cd.params[i];
+  if (A.pop.active()) {
+    // population rows and fractions; labels clamped to [0, K)
+    const int K = A.pop.K;
+    for (int i = m.tid; i < K * kNParams; i += NT) m.s.Pk[i] = cd.pop_params[i];
+    for (int i = m.tid; i < K; i += NT) m.s.fk[i] = cd.pop_frac ? cd.pop_frac[i] : 0.f;
+    if (A.pop.kx() > 1)
+      for (int i = m.tid; i < X; i += NT) m.s.xlab[i] = (int8_t)min(max((int)cd.xb_label[i], 0), K - 1);
+    if (A.pop.kt() > 1)
+      for (int g = m.tid; g < S; g += NT) m.s.tlab[g] = (int8_t)min(max((int)cd.tm_label[g], 0), K - 1);
+  }
   m.Kl = cd.K_lat;
   m.nu_c = cd.nu;
   m.dtm = cd.dt;
@@ -506,8 +533,8 @@ __device__ void run_condition(const StepArgs& A, int ci) {
       m.s.thin_bound[g] = MF_WS(int16_t, thin_bound)[g];
     }
     for (int i = m.tid; i < m.cl.total; i += NT) m.s.coef[i] = MF_WS(float, coef)[i];
-    for (int i = m.tid; i < 27 * 16; i += NT) m.s.cum_tm[i] = MF_WS(float, cum_tm)[i];
-    for (int i = m.tid; i < 6 * T.n_bins; i += NT) m.s.pabs[i] = MF_WS(float, pabs)[i];
+    for (int i = m.tid; i < A.pop.kt() * 27 * 16; i += NT) m.s.cum_tm[i] = MF_WS(float, cum_tm)[i];
+    for (int i = m.tid; i < A.pop.kx() * 6 * T.n_bins; i += NT) m.s.pabs[i] = MF_WS(float, pabs)[i];
     if (m.tid == 0) {
       const uint32_t* kk = reinterpret_cast<const uint32_t*>(MF_WS(double, misc) + MS_KEY);
       key_s[0] = kk[0];
@@ -632,7 +659,7 @@ __device__ void run_condition(const StepArgs& A, int ci) {
     MF_PH(4);
     if (init) {
       // table rows of the initial geometry (every site starts in state 0: block 0)
-      for (int i = m.tid; i < X; i += NT) m.s.xb_key[i] = (int16_t)m.bin_of(m.s.xb_ax[i]);
+      for (int i = m.tid; i < X; i += NT) m.s.xb_key[i] = (int16_t)(m.pop_key(i) + m.bin_of(m.s.xb_ax[i]));
     } else {
       const size_t inj_t = ((size_t)b * A.T + t) * (size_t)S;
       const size_t inj_x = ((size_t)b * A.T + t) * (size_t)X;
@@ -742,8 +769,8 @@ __device__ void run_condition(const StepArgs& A, int ci) {
     MF_WS(int8_t, tm)[g] = m.s.tm[g];
     MF_WS(int16_t, thin_bound)[g] = m.s.thin_bound[g];
   }
-  for (int i = m.tid; i < 27 * 16; i += NT) MF_WS(float, cum_tm)[i] = m.s.cum_tm[i];
-  for (int i = m.tid; i < 6 * T.n_bins; i += NT) MF_WS(float, pabs)[i] = m.s.pabs[i];
+  for (int i = m.tid; i < A.pop.kt() * 27 * 16; i += NT) MF_WS(float, cum_tm)[i] = m.s.cum_tm[i];
+  for (int i = m.tid; i < A.pop.kx() * 6 * T.n_bins; i += NT) MF_WS(float, pabs)[i] = m.s.pabs[i];
   // block-wide OR of the status bits (__syncthreads_or returns 0 or 1, not
   // the OR of its operands, so each bit is reduced on its own)
   int st_all = 0;

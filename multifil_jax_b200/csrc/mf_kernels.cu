@@ -4,6 +4,7 @@
 //   nvcc ... -DMF_NT=256 -DMF_P=1 -DMF_D=0 -c mf_kernels.cu
 #include "mf_kernel.cuh"
 #include "mf_launch.cuh"
+#include "mf_state.cuh"
 
 #if !defined(MF_NT) || !defined(MF_P) || !defined(MF_D)
 #error "compile with -DMF_NT=<CTA size> -DMF_P=<0|1> -DMF_D=<0|1>"
@@ -53,5 +54,32 @@ cudaError_t MF_NAME(launch_, MF_NT, MF_P, MF_D)(const StepArgs& a, int grid, int
   step_kernel<MF_NT, (MF_P != 0), (MF_D != 0)><<<grid, MF_NT, smem, st>>>(a, base);
   return cudaPeekAtLastError();
 }
+
+#if MF_P == 0
+#define MF_SNAME(a, b, c) MF_SPASTE(a, b, c)
+#define MF_SPASTE(a, b, c) a##b##_##c
+// The caller-owned-state kernel of this CTA size and spacing mode: its shared
+// memory limit is raised on first use per device.
+cudaError_t MF_SNAME(prepare_state_, MF_NT, MF_D)(size_t smem) {
+  constexpr int kDevices = 64;
+  static size_t attr_bytes[kDevices] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kDevices) return cudaErrorInvalidDevice;
+  if (smem > attr_bytes[dev]) {
+    e = cudaFuncSetAttribute(state_kernel<MF_NT, (MF_D != 0)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr_bytes[dev] = smem;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t MF_SNAME(launch_state_, MF_NT, MF_D)(const StepArgs& a, const StateIO& io, int grid, size_t smem,
+                                                  cudaStream_t st) {
+  state_kernel<MF_NT, (MF_D != 0)><<<grid, MF_NT, smem, st>>>(a, io);
+  return cudaPeekAtLastError();
+}
+#endif
 
 }  // namespace mf

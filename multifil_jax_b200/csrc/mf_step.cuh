@@ -37,6 +37,12 @@ struct CondDesc {
   int* status;            // or NULL
   uint32_t* key_out;      // [2] or NULL
   float K_lat, nu, dt;
+  // subpopulations (StepArgs::pop): K parameter rows, K fractions, per-head
+  // and per-site population labels (NULL when unused)
+  const float* pop_params;
+  const float* pop_frac;
+  const int8_t* xb_label;
+  const int8_t* tm_label;
 };
 
 struct StepArgs {
@@ -51,6 +57,7 @@ struct StepArgs {
   int8_t* st_trace;
   int* bd_trace;
   int max_dof, max_xbs, max_sites;
+  PopShape pop;          // subpopulations of the batch (K <= 1: none)
 };
 
 constexpr int FLAG_DYN = 1, FLAG_PRECISE = 2, FLAG_ORIG_PRNG = 4;
@@ -142,6 +149,12 @@ struct Smem {
   int8_t* old_xbs;   // [X]
   int16_t* old_key;  // [X] table row (permissiveness, bin) of the pre-step geometry
   int16_t* xb_key;   // [X] table row used by the latest crossbridge sampling
+  // subpopulations: K parameter rows and fractions, per-head / per-site
+  // population labels (only when the batch has populations)
+  float* Pk;         // [K*44]
+  float* fk;         // [K]
+  int8_t* xlab;      // [X] when the crossbridge tables are per population
+  int8_t* tlab;      // [S] when the tropomyosin tables are per population
 };
 
 // Thomas coefficient block layout inside coef (floats).
@@ -171,17 +184,49 @@ __host__ __device__ inline CoefLayout coef_layout(const TopoDev& t) {
 // loop's code.  tm: the 27 tropomyosin tables; sampling / absorbing: the
 // crossbridge tables of every key, or with `keys` only the nkeys listed ones
 // (of the one kind selected).
+//
+// Subpopulations (pop, with the K population rows Pk and fractions fk):
+// a blended family uses sum_k f_k Q_k, products and sums rounded one by one
+// in population order from 0 (the reference's Python sum,
+// transitions.py:580-585, 967-971); an explicit family keeps one table set
+// per population, population-major (table key = population * (2 n_bins) +
+// permissiveness * n_bins + bin; tropomyosin row = population * 27 + cfg).
+// Population rows differ from P only in xb_* / tm_* rate fields.
+template <int R, int C>
+static __device__ __forceinline__ void blend_acc(float (&acc)[R][C], const float (&q)[R][C], float f) {
+#pragma unroll
+  for (int i = 0; i < R; ++i)
+#pragma unroll
+    for (int j = 0; j < C; ++j) acc[i][j] = __fadd_rn(acc[i][j], __fmul_rn(f, q[i][j]));
+}
+
 static __device__ __noinline__ void build_tables_block(const float* P, const float* centers, int nb, float pCa, float d,
                                                 float dtm, int sq64, float* cum_tm, float* cum_xb, float* pabs,
                                                 bool tm, bool sampling, bool absorbing, const int16_t* keys,
-                                                int nkeys, int tid, int nt) {
+                                                int nkeys, int tid, int nt, PopShape pop, const float* Pk,
+                                                const float* fk) {
   const int h = tid & 1;                                  // which half of the rows
   const int pair = tid >> 1, npairs = nt >> 1;
   const unsigned pmask = 3u << (tid & 30);
   if (tm) {
-    for (int m = pair; m < 27; m += npairs) {
+    const int kt = pop.kt();
+    const bool blend = pop.blend_tm();
+    for (int m = pair; m < kt * 27; m += npairs) {
+      const int cfg = m % 27, pk = m / 27;
       float q[2][4];
-      tm_generator_rows(P, pCa, m, h, q);
+      if (blend) {
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) q[i][j] = 0.f;
+        for (int k = 0; k < pop.K; ++k) {
+          float qk[2][4];
+          tm_generator_rows(Pk + k * kNParams, pCa, cfg, h, qk);
+          blend_acc(q, qk, fk[k]);
+        }
+      } else {
+        tm_generator_rows(kt > 1 ? Pk + pk * kNParams : P, pCa, cfg, h, q);
+      }
 #pragma unroll
       for (int i = 0; i < 2; ++i)
 #pragma unroll
@@ -191,14 +236,29 @@ static __device__ __noinline__ void build_tables_block(const float* P, const flo
       for (int i = 0; i < 2; ++i) cum4(q[i], cum_tm + m * 16 + 4 * (2 * h + i));
     }
   }
-  const int nwork = keys ? nkeys : (sampling ? 2 * nb : 0) + (absorbing ? 2 * nb : 0);
+  const int kx = pop.kx(), nset = 2 * nb;  // keys of one population's set
+  const bool blend = pop.blend_xb();
+  const int nwork = keys ? nkeys : (sampling ? kx * nset : 0) + (absorbing ? kx * nset : 0);
   for (int w = pair; w < nwork; w += npairs) {
-    const bool is_abs = keys ? absorbing : (!sampling || w >= 2 * nb);
-    const int key = keys ? (int)keys[w] : (is_abs && sampling ? w - 2 * nb : w);
-    const int bin = key % nb;
-    const float perm = key >= nb ? 1.0f : 0.0f;
+    const bool is_abs = keys ? absorbing : (!sampling || w >= kx * nset);
+    const int key = keys ? (int)keys[w] : (is_abs && sampling ? w - kx * nset : w);
+    const int pk = key / nset, k2 = key - pk * nset;
+    const int bin = k2 % nb;
+    const float perm = k2 >= nb ? 1.0f : 0.0f;
     float q[3][6];
-    xb_generator_rows(P, pCa, centers[bin], d, perm, h, q);
+    if (blend) {
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 6; ++j) q[i][j] = 0.f;
+      for (int k = 0; k < pop.K; ++k) {
+        float qk[3][6];
+        xb_generator_rows(Pk + k * kNParams, pCa, centers[bin], d, perm, h, qk);
+        blend_acc(q, qk, fk[k]);
+      }
+    } else {
+      xb_generator_rows(kx > 1 ? Pk + pk * kNParams : P, pCa, centers[bin], d, perm, h, q);
+    }
     if (is_abs) {  // the absorbing chain: rows 0 and 4 zeroed
 #pragma unroll
       for (int j = 0; j < 6; ++j) q[h == 0 ? 0 : 1][j] = 0.f;
@@ -1509,13 +1569,13 @@ struct Sim : SimDyn<DY> {
   __device__ void build_tables(float pCa, float d, bool sampling, bool absorbing) {
     build_tables_block(s.P, T.centers, T.n_bins, pCa, d, dtm, A.sq64_from, s.cum_tm,
                        reinterpret_cast<float*>(ws + L.cum_xb), s.pabs, sampling, sampling,
-                       absorbing, nullptr, 0, tid, NT);
+                       absorbing, nullptr, 0, tid, NT, A.pop, s.Pk, s.fk);
   }
   // the tropomyosin tables alone (they do not depend on the spacing)
   __device__ void build_tm_tables(float pCa) {
     build_tables_block(s.P, T.centers, T.n_bins, pCa, 0.f, dtm, A.sq64_from, s.cum_tm,
                        reinterpret_cast<float*>(ws + L.cum_xb), s.pabs, true, false, false, nullptr, 0,
-                       tid, NT);
+                       tid, NT, A.pop, s.Pk, s.fk);
   }
 
   // Dynamic spacing rebuilds the crossbridge tables every step.  Only the
@@ -1524,11 +1584,11 @@ struct Sim : SimDyn<DY> {
   // heads the metrics read (old state 2 or 3).  Flags and the sorted key list
   // live in the CG vector pv, which is free outside the solve.
   __device__ bool lazy_tables_fit() const {
-    const int nk = 2 * T.n_bins, nwords = (nk + 31) >> 5;
+    const int nk = A.pop.kx() * 2 * T.n_bins, nwords = (nk + 31) >> 5;
     return 4 * (nwords + 1) + 2 * nk <= 4 * T.n_dof;
   }
   __device__ void build_needed_tables(float pCa, float d, bool absorbing) {
-    const int nk = 2 * T.n_bins, nwords = (nk + 31) >> 5, X = T.total_xbs;
+    const int nk = A.pop.kx() * 2 * T.n_bins, nwords = (nk + 31) >> 5, X = T.total_xbs;
     uint32_t* bits = reinterpret_cast<uint32_t*>(s.pv);
     int* count = reinterpret_cast<int*>(bits + nwords);
     int16_t* list = reinterpret_cast<int16_t*>(count + 1);
@@ -1571,7 +1631,7 @@ struct Sim : SimDyn<DY> {
     const int nkeys = *count;
     build_tables_block(s.P, T.centers, T.n_bins, pCa, d, dtm, A.sq64_from, s.cum_tm,
                        reinterpret_cast<float*>(ws + L.cum_xb), s.pabs, false, !absorbing, absorbing, list,
-                       nkeys, tid, NT);
+                       nkeys, tid, NT, A.pop, s.Pk, s.fk);
     __syncthreads();
   }
 
@@ -1704,7 +1764,8 @@ struct Sim : SimDyn<DY> {
         // locked row [0,0,0,1]: first cumsum entry above u is index 3
         ns = u < 0.f ? 0 : (u < 1.0f ? 3 : 0);
       } else {
-        const float* c = s.cum_tm + cfg * 16 + st * 4;
+        const int row = A.pop.kt() > 1 ? s.tlab[g] * 27 + cfg : cfg;
+        const float* c = s.cum_tm + row * 16 + st * 4;
         ns = u < c[0] ? 0 : (u < c[1] ? 1 : (u < c[2] ? 2 : (u < c[3] ? 3 : 0)));
       }
       s.tm_new[g] = (int8_t)ns;
@@ -1740,7 +1801,11 @@ struct Sim : SimDyn<DY> {
     const int near = s.xb_near[i];
     const int site = near < 0 ? 0 : (near > nsi - 1 ? nsi - 1 : near);
     const bool perm = (s.tm[thin * nsi + site] == 3) && T.xb_valid[i];
-    return (perm ? T.n_bins : 0) + bin_of(s.xb_ax[i]);
+    return pop_key(i) + (perm ? T.n_bins : 0) + bin_of(s.xb_ax[i]);
+  }
+  // first table key of head i's population (0 without per-population tables)
+  __device__ __forceinline__ int pop_key(int i) const {
+    return A.pop.kx() > 1 ? (int)s.xlab[i] * 2 * T.n_bins : 0;
   }
 
   __device__ void thick_step(const uint32_t* sub, size_t inj_off) {
@@ -1757,7 +1822,7 @@ struct Sim : SimDyn<DY> {
       const int site = near < 0 ? 0 : (near > nsi - 1 ? nsi - 1 : near);
       const int tgt = thin * nsi + site;
       const bool perm = (s.tm[tgt] == 3) && T.xb_valid[i];
-      const int key = (perm ? nbins : 0) + bin_of(s.xb_ax[i]);
+      const int key = pop_key(i) + (perm ? nbins : 0) + bin_of(s.xb_ax[i]);
       s.xb_key[i] = (int16_t)key;
       const int old = s.xb_state[i];
       const float* c = cum_xb + key * 36 + old * 6;

@@ -24,6 +24,10 @@ MF_FLAG_ORIGINAL_PRNG = 4
 MF_FLAG_PLAIN = 8
 MF_FLAG_NO_GRAPH = 16
 
+MF_POP_EXPLICIT = 1
+MF_POP_XB = 2
+MF_POP_TM = 4
+
 MF_STATUS_NONFINITE = 1
 MF_STATUS_NOT_CONVERGED = 2
 MF_STATUS_MULTIBIND = 8
@@ -67,6 +71,9 @@ class mf_batch(ctypes.Structure):
         ('keys_out', ctypes.c_void_p), ('u_thin', ctypes.c_void_p), ('u_xb', ctypes.c_void_p),
         ('x_trace', ctypes.c_void_p), ('state_trace', ctypes.c_void_p),
         ('bound_trace', ctypes.c_void_p),
+        ('n_pops', ctypes.c_int32), ('pop_flags', ctypes.c_int32), ('label_stride', ctypes.c_int32),
+        ('pop_params', ctypes.c_void_p), ('pop_frac', ctypes.c_void_p), ('xb_label', ctypes.c_void_p),
+        ('tm_label', ctypes.c_void_p),
     ]
 
 
@@ -141,6 +148,16 @@ def prng_split(key, n: int, partitionable: bool = True) -> np.ndarray:
     rc = lib.mf_prng_split(int(key[0]), int(key[1]), n, 1 if partitionable else 0, out.ctypes.data)
     if rc:
         raise EngineError(f"mf_prng_split failed ({rc})")
+    return out
+
+
+def prng_uniform(key, n: int, partitionable: bool = True) -> np.ndarray:
+    """``jax.random.uniform(key, (n,))`` (float32) computed by the library's host Threefry."""
+    lib = load_library()
+    out = np.zeros(n, dtype=np.float32)
+    rc = lib.mf_prng_uniform(int(key[0]), int(key[1]), n, 1 if partitionable else 0, out.ctypes.data)
+    if rc:
+        raise EngineError(f"mf_prng_uniform failed ({rc})")
     return out
 
 
@@ -266,11 +283,16 @@ class Engine:
     # ------------------------------------------------------------------
     def run_batch(self, topos, params, z, pCa, ls, n_steps, keys, K_lat=None, nu=None, dt=None,
                   n_newton=4, n_cg=6, flags=0, chunk_steps=0, residual_warn=1.5, stream=None,
-                  u_thin=None, u_xb=None, want_x_trace=False, want_state_trace=False, keys_out=None):
+                  u_thin=None, u_xb=None, want_x_trace=False, want_state_trace=False, keys_out=None,
+                  pops=None):
         """Run B conditions through the fused kernel; every array is a torch CUDA tensor.
 
         ``topos`` is a list of B SarcTopology objects (or one shared).  Returns
         a dict with ``metrics`` [B, 52, T], ``status`` [B] and optional traces.
+        ``pops``: subpopulations as a dict ``K``, ``flags`` (MF_POP_*),
+        ``rows`` [B, K, 44] float32, ``fractions`` [B, K] float32 and, for
+        explicit populations, ``xb_label`` / ``tm_label`` [B, stride] int8
+        device tensors.
         """
         torch = _torch()
         dev = torch.device('cuda', self.device)
@@ -324,6 +346,19 @@ class Engine:
         bat.x_trace = xt.data_ptr() if xt is not None else None
         bat.state_trace = st.data_ptr() if st is not None else None
         bat.bound_trace = bt.data_ptr() if bt is not None else None
+        if pops is not None and int(pops['K']) > 1:
+            bat.n_pops, bat.pop_flags = int(pops['K']), int(pops['flags'])
+            bat.pop_params = f32(pops['rows']).data_ptr()
+            bat.pop_frac = f32(pops['fractions']).data_ptr()
+            stride = 0
+            for name in ('xb_label', 'tm_label'):
+                lab = pops.get(name)
+                if lab is not None:
+                    assert lab.is_cuda and lab.dtype == torch.int8 and lab.is_contiguous() and lab.shape[0] == B
+                    stride = lab.shape[1] if stride == 0 else stride
+                    assert lab.shape[1] == stride
+                    setattr(bat, name, lab.data_ptr())
+            bat.label_stride = int(stride)
         s = stream if stream is not None else torch.cuda.current_stream(dev)
         self._check(self.lib.mf_run_batch(self.h, ctypes.byref(bat), ctypes.c_void_p(s.cuda_stream)),
                     'mf_run_batch')
@@ -371,6 +406,24 @@ def upload(dev, *arrays):
     return [d[o:o + a.nbytes].view(tdt[a.dtype]).view(a.shape) for a, o in zip(arrays, offs)]
 
 
+def device_pops(sp, dev):
+    """A :class:`~multifil_jax_b200.subpopulation.ResolvedSubpop` as the device
+    tensors ``Engine.run_batch(pops=...)`` takes."""
+    torch = _torch()
+    flags = (MF_POP_EXPLICIT if sp.explicit else 0) | (MF_POP_XB if sp.xb else 0) | (MF_POP_TM if sp.tm else 0)
+    rows, frac = upload(dev, np.ascontiguousarray(sp.rows, np.float32), np.ascontiguousarray(sp.fractions, np.float32))
+    out = dict(K=sp.K, flags=flags, rows=rows, fractions=frac)
+    if sp.explicit:
+        B = sp.rows.shape[0]
+        stride = max(sp.xb_label.shape[1], sp.tm_label.shape[1])
+        for name in ('xb_label', 'tm_label'):
+            lab = np.zeros((B, stride), np.int8)
+            src = getattr(sp, name)
+            lab[:, :src.shape[1]] = src
+            out[name] = torch.as_tensor(lab).to(dev)
+    return out
+
+
 def to_host(t):
     """Copy a device tensor into page-locked host memory and return it as numpy.
 
@@ -414,13 +467,14 @@ def execute_plan(topology, plan, static_params, precision: str = 'float32', devi
             P, Z, PC, L, K, KL, NU = upload(dev, plan.params[s:e], plan.z[s:e], plan.pCa[s:e], plan.ls[s:e],
                                             plan.keys[s:e].astype(np.uint32).view(np.int32), plan.K_lat[s:e],
                                             plan.nu[s:e])
+            pops = device_pops(plan.subpop.take(s, e), dev) if plan.subpop is not None else None
             res = eng.run_batch([topology] * n, P, Z, PC, L,
                                 torch.full((n,), T, dtype=torch.int32, device=dev), K,
                                 K_lat=KL, nu=NU,
                                 dt=torch.full((n,), plan.dt, dtype=torch.float32, device=dev),
                                 n_newton=static_params.n_newton_steps, n_cg=static_params.n_cg_steps,
                                 flags=flags, chunk_steps=chunk_steps,
-                                residual_warn=static_params.solver_residual_tol, stream=stream)
+                                residual_warn=static_params.solver_residual_tol, stream=stream, pops=pops)
             m = res['metrics'].permute(1, 0, 2).contiguous() if key_major else res['metrics']
             if status_out is not None:
                 status_out[s:e] = res['status'].cpu().numpy()

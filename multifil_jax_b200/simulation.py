@@ -23,6 +23,7 @@ import numpy as np
 from .params import DYNAMIC_FIELDS, DynamicParams, StaticParams, N_PARAMS
 from .topology import SarcTopology
 from .result import MetricsDict, SimulationResult
+from .subpopulation import ResolvedSubpop, Subpopulation  # noqa: F401
 
 METRIC_KEYS = (
     'axial_force', 'solver_residual', 'z_line', 'pCa', 'lattice_spacing',
@@ -79,6 +80,7 @@ class BatchPlan:
     coords: Dict[str, list]
     rng_key: np.ndarray
     topology_config: Dict = field(default_factory=dict)
+    subpop: Optional['ResolvedSubpop'] = None  # per-condition populations (None: one population)
 
     @property
     def total(self) -> int:
@@ -97,8 +99,6 @@ def plan_batch(topology: SarcTopology, duration_ms: float = 1000.0, dt: float = 
                static_params: Optional[StaticParams] = None, replicates: int = 1, rng_seed: int = 0,
                subpopulation=None) -> BatchPlan:
     """Expand run()'s arguments into per-condition arrays (no device work)."""
-    if subpopulation is not None:
-        raise NotImplementedError("subpopulations are not supported by multifil_jax_b200")
     if replicates < 1:
         raise ValueError("replicates must be >= 1")
     n_steps = int(duration_ms / dt)
@@ -167,6 +167,14 @@ def plan_batch(topology: SarcTopology, duration_ms: float = 1000.0, dt: float = 
                 axes.append((name, list(arr.tolist())))
                 ptables[name] = arr.astype(np.float32)
                 paxis[name] = name
+    # a list of Subpopulations is a candidate-style sweep axis (simulation.py:945-953)
+    if isinstance(subpopulation, list):
+        if isinstance(dynamic_params, list):
+            raise ValueError("Cannot sweep a dynamic_params list and a subpopulation list simultaneously "
+                             "(both are candidate-style axes).")
+        if not subpopulation:
+            raise ValueError("subpopulation list is empty")
+        axes.append(('subpopulation', list(range(len(subpopulation)))))
 
     if axes:
         grids = np.meshgrid(*[np.arange(len(c)) for _, c in axes], indexing='ij')
@@ -216,6 +224,9 @@ def plan_batch(topology: SarcTopology, duration_ms: float = 1000.0, dt: float = 
         return np.full(total, float(np.asarray(getattr(base, name)).reshape(-1)[0]), np.float32)
     params = np.stack([param(n) for n in DYNAMIC_FIELDS], axis=1).astype(np.float32)
     assert params.shape == (total, N_PARAMS)
+    from .subpopulation import resolve_subpopulation
+    subpop = resolve_subpopulation(subpopulation, topology, params,
+                                   flat['subpopulation'] if isinstance(subpopulation, list) else None)
     keys = _split_keys(rng_seed, total)
     padded = get_bucket_size(total)
     if padded > total:
@@ -232,7 +243,8 @@ def plan_batch(topology: SarcTopology, duration_ms: float = 1000.0, dt: float = 
         tcfg['nu'] = nu
     return BatchPlan(n_steps=n_steps, dt=float(dt), params=params, z=z_b, pCa=p_b, ls=l_b, keys=keys,
                      K_lat=K_b, nu=nu_b, dynamic_ls=is_dyn, grid_shape=grid_shape, replicates=replicates,
-                     axis_names=axis_names, coords=coords, rng_key=last_key, topology_config=tcfg)
+                     axis_names=axis_names, coords=coords, rng_key=last_key, topology_config=tcfg,
+                     subpop=subpop)
 
 
 def assemble_result(plan: BatchPlan, metrics: np.ndarray, static_params: StaticParams, rng_seed: int,

@@ -319,11 +319,14 @@ def tm_config(tm, prev, nxt):
     return (n2 * 9 + n3 * 3 + nc).reshape(-1)
 
 
-def thin_transitions(tm, thin_bound, P_tm, topo, u):
-    """New tm_states (transitions.py:516-625), with the bound-and-open lock."""
+def thin_transitions(tm, thin_bound, P_tm, topo, u, labels=None):
+    """New tm_states (transitions.py:516-625), with the bound-and-open lock.
+
+    ``labels`` (per site): ``P_tm`` holds one 27-table set per population and
+    each site reads its own population's set (transitions.py:586-596)."""
     cfg = tm_config(tm, topo.tm_prev_neighbor, topo.tm_next_neighbor)
     s = tm.reshape(-1).astype(np.int32)
-    prob = P_tm[cfg, s]
+    prob = P_tm[cfg, s] if labels is None else P_tm[np.asarray(labels), cfg, s]
     locked = (s == 3) & (thin_bound.reshape(-1) >= 0)
     lock_row = np.array([0.0, 0.0, 0.0, 1.0], dtype=prob.dtype)
     prob = np.where(locked[:, None], lock_row, prob)
@@ -336,8 +339,11 @@ def permissiveness(tm, nearest, topo):
     return (st == 3).astype(np.float32) * topo.xb_valid.astype(np.float32)
 
 
-def thick_transitions(xb_state, xb_bound, thin_bound, nearest, x_axial, tm, P_bins, topo, u):
+def thick_transitions(xb_state, xb_bound, thin_bound, nearest, x_axial, tm, P_bins, topo, u, labels=None):
     """Sample crossbridge states and update the binding bookkeeping.
+
+    ``labels`` (per head): ``P_bins`` holds one bin grid per population and a
+    head reads its own population's grid (transitions.py:925-994).
 
     Restates thick_transitions (transitions.py:1081-1245).  The two scatters
     into ``thin.bound_to`` are applied in crossbridge-index order with the last
@@ -347,7 +353,7 @@ def thick_transitions(xb_state, xb_bound, thin_bound, nearest, x_axial, tm, P_bi
     perm = permissiveness(tm, nearest, topo)
     key = xb_bin_key(x_axial, perm, topo)
     old = xb_state.astype(np.int32)
-    prob = P_bins[key, old]
+    prob = P_bins[key, old] if labels is None else P_bins[np.asarray(labels), key, old]
     new = sample(prob, u)
     old_b = (old >= 1) & (old <= 3)
     new_b = (new >= 1) & (new <= 3)

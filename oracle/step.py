@@ -58,14 +58,58 @@ class Tables:
     s_xb: np.ndarray = field(default=None)
 
 
-def tables(topo, p, pCa, d, dt_ms, dt):
-    P_tm, s_tm = ph.expm_pade6(ph.tm_Q27(p, dt(pCa), dt) * dt(dt_ms), with_s=True)
-    P_xb, s_xb = ph.expm_pade6(ph.xb_Q_bins(topo, p, dt(pCa), dt(d), dt) * dt(dt_ms), with_s=True)
+def _pop_generators(gen, p, sp, family, dt):
+    """Generators of one rate family with subpopulations (transitions.py:580-596,
+    :957-976): the wild-type set when no population scales the family, the
+    fraction-weighted sum sum_k f_k Q_k (mean field, Python ``sum`` order), or
+    the K sets stacked on a leading axis (explicit labels)."""
+    if sp is None or not sp[family]:
+        return gen(p)
+    Qk = [gen(ph.param_dict(r, dt)) for r in sp['rows']]
+    if not sp['explicit']:
+        f = np.asarray(sp['frac'], dtype=np.float32).astype(dt)
+        return sum(f[k] * Qk[k] for k in range(len(Qk)))
+    return np.stack(Qk)
+
+
+def _expm_any(Q, with_s=False):
+    """expm_pade6 over any leading shape (K stacked sets included)."""
+    n = Q.shape[-1]
+    r = ph.expm_pade6(Q.reshape(-1, n, n), with_s=with_s)
+    if with_s:
+        return r[0].reshape(Q.shape), r[1].reshape(Q.shape[:-2])
+    return r.reshape(Q.shape)
+
+
+def tables(topo, p, pCa, d, dt_ms, dt, sp=None):
+    """Sampling tables at (pCa, d); with a subpopulation ``sp`` (see
+    ``subpop_spec``) the blended or per-population sets."""
+    Qt = _pop_generators(lambda q: ph.tm_Q27(q, dt(pCa), dt), p, sp, 'tm', dt)
+    Qx = _pop_generators(lambda q: ph.xb_Q_bins(topo, q, dt(pCa), dt(d), dt), p, sp, 'xb', dt)
+    P_tm, s_tm = _expm_any(Qt * dt(dt_ms), with_s=True)
+    P_xb, s_xb = _expm_any(Qx * dt(dt_ms), with_s=True)
     return Tables(P_tm, P_xb, s_tm, s_xb)
 
 
-def absorbing_table(topo, p, pCa, d, dt_ms, dt):
-    return ph.expm_pade6(ph.absorbing(ph.xb_Q_bins(topo, p, dt(pCa), dt(d), dt)) * dt(dt_ms))
+def absorbing_table(topo, p, pCa, d, dt_ms, dt, sp=None):
+    Qx = _pop_generators(lambda q: ph.xb_Q_bins(topo, q, dt(pCa), dt(d), dt), p, sp, 'xb', dt)
+    return _expm_any(ph.absorbing(Qx) * dt(dt_ms))
+
+
+def subpop_spec(rows, fractions, explicit, xb, tm, xb_label=None, tm_label=None):
+    """One condition's subpopulation for the oracle: K parameter rows, the K
+    fractions, which rate families the populations change, and the labels of
+    the explicit modes."""
+    return dict(rows=np.asarray(rows, np.float32), frac=np.asarray(fractions, np.float32), explicit=bool(explicit),
+                xb=bool(xb), tm=bool(tm),
+                xb_label=None if xb_label is None else np.asarray(xb_label, np.int64),
+                tm_label=None if tm_label is None else np.asarray(tm_label, np.int64))
+
+
+def _labels(sp, family):
+    if sp is None or not sp['explicit'] or not sp[family]:
+        return None
+    return sp[family + '_label']
 
 
 # ---------------------------------------------------------------------------
@@ -177,7 +221,7 @@ def initial_condition(topo, p, z0, n_newton, n_cg, dt, precond):
 # ---------------------------------------------------------------------------
 
 def metrics(topo, p, old: Condition, new: Condition, z, pCa, ls, pre_thick, force, resid, iters,
-            P_abs, dt, thin_rest_cum):
+            P_abs, dt, thin_rest_cum, xb_labels=None):
     f32 = dt
     nx = f32(new.xb_state.size)
     nt = f32(new.tm.size)
@@ -215,7 +259,7 @@ def metrics(topo, p, old: Condition, new: Condition, z, pCa, ls, pre_thick, forc
     # expected exits from the absorbing generator, on the pre-step geometry
     perm = ph.permissiveness(old.tm, old.xb_nearest, topo)
     key = ph.xb_bin_key(old.xb_dist[:, 0], perm, topo)
-    Pk = P_abs[key]
+    Pk = P_abs[key] if xb_labels is None else P_abs[xb_labels, key]
     s_old = xb_old.astype(np.int32)
     atp_p = np.sum((s_old == 3).astype(dt) * Pk[:, 3, 4])
     tear = np.sum(((s_old == 2) | (s_old == 3)).astype(dt) * Pk[np.arange(s_old.size), s_old, 0])
@@ -237,7 +281,7 @@ def metrics(topo, p, old: Condition, new: Condition, z, pCa, ls, pre_thick, forc
 
 def timestep(topo, p, c: Condition, z, pCa, ls_drv, dz, u_thin, u_xb, tab: Tables, n_newton, n_cg,
              dt, precond, dt_ms, K_lat=None, d_ref=None, P_abs=None, thin_rest_cum=None,
-             want_metrics=True, tab_abs_fn=None):
+             want_metrics=True, tab_abs_fn=None, sp=None):
     """Advance one condition by one step; returns (new condition, metrics row, extras)."""
     old = c.copy()
     old.thin_x = (old.thin_x + dt(dz)).astype(dt)
@@ -245,9 +289,10 @@ def timestep(topo, p, c: Condition, z, pCa, ls_drv, dz, u_thin, u_xb, tab: Table
     s = old.copy()
     # kinetics (timestep.py:97-129)
     s.xb_nearest, s.xb_dist = ph.nearest_sites(s.thick_x, s.thin_x, topo, dt(ls_drv), dt)
-    s.tm = ph.thin_transitions(s.tm, s.thin_bound, tab.P_tm, topo, u_thin)
+    s.tm = ph.thin_transitions(s.tm, s.thin_bound, tab.P_tm, topo, u_thin, labels=_labels(sp, 'tm'))
     s.xb_state, s.xb_bound, s.thin_bound = ph.thick_transitions(
-        s.xb_state, s.xb_bound, s.thin_bound, s.xb_nearest, s.xb_dist[:, 0], s.tm, tab.P_xb, topo, u_xb)
+        s.xb_state, s.xb_bound, s.thin_bound, s.xb_nearest, s.xb_dist[:, 0], s.tm, tab.P_xb, topo, u_xb,
+        labels=_labels(sp, 'xb'))
     # mechanics
     if K_lat is None:
         xt, xn, res, it, new_ls = solve_fixed(topo, p, s, z, ls_drv, n_newton, n_cg, dt, precond)
@@ -261,7 +306,7 @@ def timestep(topo, p, c: Condition, z, pCa, ls_drv, dz, u_thin, u_xb, tab: Table
         if P_abs is None:
             P_abs = tab_abs_fn(new_ls)
         row = metrics(topo, p, old, s, dt(z), dt(pCa), dt(new_ls), pre_thick, force, res, it, P_abs, dt,
-                      thin_rest_cum)
+                      thin_rest_cum, xb_labels=_labels(sp, 'xb'))
     return s, row, dict(force=force, residual=res, iters=it, ls=new_ls)
 
 
@@ -271,12 +316,14 @@ def thin_rest_cumsum(topo, dt):
 
 def run_condition(topo, prow, z_tr, pCa_tr, ls_tr, key, dt_ms=1.0, n_newton=4, n_cg=6, dt=np.float32,
                   K_lat=None, nu=0.0, uniforms=None, record_states=False, partitionable=None,
-                  hoist_tables=True, udtype=np.float32):
+                  hoist_tables=True, udtype=np.float32, subpop=None):
     """The per-condition body of ``_run_sim_kernel`` (simulation.py:633-729).
 
     Returns ``(metrics [52, T], info)``; ``info['uniforms']`` holds the draws
     used, ``info['states']`` per-step snapshots when ``record_states``.
     ``uniforms`` (list of (u_thin, u_xb)) replaces the PRNG draws.
+    ``subpop`` (``subpop_spec``) runs the condition with mixed populations
+    (simulation.py:658-676).
     """
     dt = np.dtype(dt).type
     p = ph.param_dict(prow, dt)
@@ -299,7 +346,7 @@ def run_condition(topo, prow, z_tr, pCa_tr, ls_tr, key, dt_ms=1.0, n_newton=4, n
         k = (float(pCa), float(d))
         if not hoist_tables or k not in cache:
             cache.clear()
-            cache[k] = tables(topo, p, pCa, d, dt_ms, dt)
+            cache[k] = tables(topo, p, pCa, d, dt_ms, dt, sp=subpop)
         return cache[k]
     abs_cache = {}
 
@@ -307,7 +354,7 @@ def run_condition(topo, prow, z_tr, pCa_tr, ls_tr, key, dt_ms=1.0, n_newton=4, n
         k = (float(pCa), float(d))
         if not hoist_tables or k not in abs_cache:
             abs_cache.clear()
-            abs_cache[k] = absorbing_table(topo, p, pCa, d, dt_ms, dt)
+            abs_cache[k] = absorbing_table(topo, p, pCa, d, dt_ms, dt, sp=subpop)
         return abs_cache[k]
 
     for t in range(T):
@@ -327,7 +374,7 @@ def run_condition(topo, prow, z_tr, pCa_tr, ls_tr, key, dt_ms=1.0, n_newton=4, n
         c, row, ex = timestep(topo, p, c, z_tr[t], pCa_tr[t], ls_drv, dz[t], u_thin.astype(dt),
                               u_xb.astype(dt), tab, n_newton, n_cg, dt, precond, dt_ms, K_lat=K_lat,
                               d_ref=d_ref, thin_rest_cum=thin_cum,
-                              tab_abs_fn=lambda d_new, t_=t: get_abs(pCa_tr[t_], d_new))
+                              tab_abs_fn=lambda d_new, t_=t: get_abs(pCa_tr[t_], d_new), sp=subpop)
         out[:, t] = row
         cur_ls = ex['ls']
         if record_states:

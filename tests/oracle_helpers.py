@@ -4,6 +4,16 @@ import numpy as np
 from oracle import step as OS
 
 
+def plan_subpop(plan, b):
+    """The oracle's subpopulation spec of condition b of a BatchPlan (None without one)."""
+    sp = plan.subpop
+    if sp is None:
+        return None
+    return OS.subpop_spec(sp.rows[b], sp.fractions[b], sp.explicit, sp.xb, sp.tm,
+                          None if sp.xb_label is None else sp.xb_label[b],
+                          None if sp.tm_label is None else sp.tm_label[b])
+
+
 def oracle_plan(topo, plan, static, dtype=np.float32, udtype=np.float32, params=None, **kw):
     """Metrics [B, 52, T] of every condition of a BatchPlan, computed by the oracle."""
     B, T = plan.total, plan.n_steps
@@ -14,7 +24,8 @@ def oracle_plan(topo, plan, static, dtype=np.float32, udtype=np.float32, params=
         K = float(plan.K_lat[b]) if plan.dynamic_ls else None
         m, info = OS.run_condition(topo, row, plan.z[b], plan.pCa[b], plan.ls[b], plan.keys[b],
                                    dt_ms=plan.dt, n_newton=static.n_newton_steps, n_cg=static.n_cg_steps,
-                                   dt=dtype, K_lat=K, nu=float(plan.nu[b]), udtype=udtype, **kw)
+                                   dt=dtype, K_lat=K, nu=float(plan.nu[b]), udtype=udtype,
+                                   subpop=plan_subpop(plan, b), **kw)
         out[b] = m
         infos.append(info)
     return out, infos

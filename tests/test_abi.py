@@ -25,7 +25,7 @@ def test_library_exports_every_declared_symbol():
     assert len(syms) >= 15
     for s in syms:
         assert hasattr(lib, s), s
-    assert lib.mf_abi_version() == 1
+    assert lib.mf_abi_version() == 2
 
 
 def test_ctypes_struct_layout_matches_c():
@@ -35,8 +35,11 @@ def test_ctypes_struct_layout_matches_c():
 #include <stddef.h>
 #include "multifil_b200.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu\n", sizeof(mf_topo_desc), sizeof(mf_batch), sizeof(mf_request),
-         offsetof(mf_batch, metrics_out), offsetof(mf_batch, bound_trace), offsetof(mf_request, pCa));
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(mf_topo_desc), sizeof(mf_batch), sizeof(mf_request),
+         offsetof(mf_batch, metrics_out), offsetof(mf_batch, bound_trace), offsetof(mf_request, pCa),
+         offsetof(mf_batch, n_pops), offsetof(mf_batch, tm_label));
+  printf("%zu %zu %zu %zu\n", sizeof(mf_state_batch), offsetof(mf_state_batch, thick_axial),
+         offsetof(mf_state_batch, status_out), offsetof(mf_state_batch, u_xb));
   return 0;
 }'''
     tmp = os.path.join(REPO, '_build')
@@ -46,8 +49,14 @@ int main(void) {
     open(c, 'w').write(src)
     subprocess.run(['gcc', '-I', os.path.join(REPO, 'include'), c, '-o', exe], check=True)
     out = list(map(int, subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()))
+    from multifil_jax_b200.timestep import mf_state_batch
+    sb = [ctypes.sizeof(mf_state_batch), mf_state_batch.thick_axial.offset, mf_state_batch.status_out.offset,
+          mf_state_batch.u_xb.offset]
+    assert out[-4:] == sb
+    out = out[:-4]
     py = [ctypes.sizeof(engine.mf_topo_desc), ctypes.sizeof(engine.mf_batch), ctypes.sizeof(engine.mf_request),
-          engine.mf_batch.metrics_out.offset, engine.mf_batch.bound_trace.offset, engine.mf_request.pCa.offset]
+          engine.mf_batch.metrics_out.offset, engine.mf_batch.bound_trace.offset, engine.mf_request.pCa.offset,
+          engine.mf_batch.n_pops.offset, engine.mf_batch.tm_label.offset]
     assert out == py
 
 
@@ -64,3 +73,5 @@ def test_invalid_arguments_are_rejected_without_a_device():
     assert lib.mf_prng_split(0, 0, -1, 1, None) < 0
     assert lib.mf_create(0, None) < 0
     assert lib.mf_destroy(None) < 0
+    from multifil_jax_b200.timestep import _bind
+    assert _bind(lib)(None, None, None) < 0

@@ -76,7 +76,7 @@ def test_errors(topo):
         plan_batch(topo, duration_ms=3, dynamic_params=[])
     with pytest.raises(ValueError):
         plan_batch(topo, duration_ms=3, dynamic_params=42)
-    with pytest.raises(NotImplementedError):
+    with pytest.raises(TypeError):
         plan_batch(topo, duration_ms=3, subpopulation=object())
 
 
