@@ -15,7 +15,7 @@ The time loop runs in hand-written CUDA kernels (``csrc/``) behind a C ABI
 __version__ = '0.1.0'
 
 from .params import (StaticParams, DynamicParams, DYNAMIC_FIELDS, get_skeletal_params,  # noqa: F401
-                     get_cardiac_params)
+                     get_cardiac_params, get_lethocerus_params, get_drosophila_params)
 from .topology import SarcTopology  # noqa: F401
 from .simulation import run, run_conditions, SimulationResult, MetricsDict, METRIC_KEYS  # noqa: F401
 from .subpopulation import Subpopulation  # noqa: F401
@@ -28,5 +28,5 @@ def get_ca_concentration(pCa: float) -> float:
 
 
 __all__ = ['run', 'run_conditions', 'SimulationResult', 'SarcTopology', 'Subpopulation', 'timestep', 'StaticParams', 'DynamicParams', 'DYNAMIC_FIELDS',
-           'get_skeletal_params', 'get_cardiac_params', 'get_ca_concentration', 'MetricsDict',
+           'get_skeletal_params', 'get_cardiac_params', 'get_lethocerus_params', 'get_drosophila_params', 'get_ca_concentration', 'MetricsDict',
            'METRIC_KEYS']

@@ -211,7 +211,8 @@ int mf_upload_topology(mf_ctx* ctx, const mf_topo_desc* d, int32_t* topo_id) {
   const int nxb = d->n_xb_per_crown, width = d->max_sites_per_face, nb = d->n_xb_bins;
   if (nth < 1 || ncr < 2 || nthin < 1 || ns < 2 || nxb < 1 || width < 1 || nb < 1)
     return fail(ctx, MF_ERR_INVALID, "bad lattice sizes");
-  if (ncr > 128 || ns > 128) return fail(ctx, MF_ERR_INVALID, "filaments longer than 128 nodes");
+  if (ncr > kMaxFilament || ns > kMaxFilament)
+    return fail(ctx, MF_ERR_INVALID, "filaments longer than %d nodes", kMaxFilament);
   const long X = (long)nth * ncr * nxb, S = (long)nthin * ns;
   if (X > 32767 || S > 32767) return fail(ctx, MF_ERR_INVALID, "lattice too large for int16 indices");
   auto t = std::make_unique<TopoHost>();

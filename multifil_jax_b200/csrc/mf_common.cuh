@@ -108,6 +108,14 @@ struct TopoDev {
   const float* thin_c;       // [S]: off[j]-off[j+1]-rest[j], last: off-rest
 };
 
+// Longest filament the kernels take (nodes), and the per-warp scan reversal
+// buffer of a lattice: 128 floats up to 128 nodes, else 256.
+constexpr int kMaxFilament = 256;
+MF_HD int scan_cap(const TopoDev& t) {
+  const int n = t.n_crowns > t.n_sites ? t.n_crowns : t.n_sites;
+  return n <= 128 ? 128 : 256;
+}
+
 // Byte layout of one condition's resident workspace (global memory).
 struct SlotLayout {
   size_t x, xb_state, xb_bound, xb_near, xb_ax, xb_key, tm, thin_bound, misc, cum_xb, pabs, cum_tm,

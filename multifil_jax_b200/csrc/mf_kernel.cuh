@@ -67,7 +67,7 @@ __host__ __device__ inline size_t smem_bytes(const TopoDev& t, int nt, int layou
   add(sizeof(float) * pop.kt() * 27 * 16);  // cum_tm
   add(sizeof(float) * pop.kx() * 6 * t.n_bins);  // pabs
   add(sizeof(float) * cl.total);           // coef
-  if (!precise) add(sizeof(float) * nw * 128);  // scan reversal buffer per warp (filaments <= 128)
+  if (!precise) add(sizeof(float) * nw * scan_cap(t));  // scan reversal buffer per warp
   add(sizeof(float) * kNParams);           // P
   add(sizeof(float) * 4 * t.n_thick);      // tvec
   add(sizeof(int16_t) * X);                // blist
@@ -136,7 +136,7 @@ __device__ void carve(Sim<NT, PR, DY>& m, char* base, int layout) {
   m.s.cum_tm = (float*)take(sizeof(float) * pop.kt() * 27 * 16);
   m.s.pabs = (float*)take(sizeof(float) * pop.kx() * 6 * t.n_bins);
   m.s.coef = (float*)take(sizeof(float) * m.cl.total);
-  m.s.scan = PR ? nullptr : (float*)take(sizeof(float) * NT / 32 * 128);
+  m.s.scan = PR ? nullptr : (float*)take(sizeof(float) * NT / 32 * scan_cap(t));
   m.s.P = (float*)take(sizeof(float) * kNParams);
   m.s.tvec = (float*)take(sizeof(float) * 4 * t.n_thick);
   m.s.blist = (int16_t*)take(sizeof(int16_t) * X);

@@ -380,15 +380,19 @@ struct Sim : SimDyn<DY> {
   // The reference's lax.associative_scan dataflow (JAX's odd/even
   // recursion) for the b-components of an affine-map scan whose a-components
   // per tree node are precomputed (Acoef, ScanPlan level offsets), evaluated
-  // in registers for one filament of n <= 128 nodes.  Lane L holds level-0
-  // elements [4L, 4L+4) in e[], level-1 elements [2L, 2L+2), and for every
-  // level >= 2 element L.  Up-sweep: level l+1 element k = fmaf(A_l[2k+1],
-  // E_l[2k], E_l[2k+1]).  Down-sweep, from the scanned level l+1 S:
-  // E_l[2k+1] = S[k], E_l[2k] = fmaf(A_l[2k], S[k-1], E_l[2k]) for k >= 1.
-  // Level changes move data by warp shuffles.
+  // in registers for one filament of n <= 32 E nodes (E = 4 or 8).  Lane L
+  // holds level-l elements [L E/2^l, (L+1) E/2^l) for every level l below
+  // log2(E) + 1 (w[l][]), and element L of every level above.  Up-sweep:
+  // level l+1 element k = fmaf(A_l[2k+1], E_l[2k], E_l[2k+1]).  Down-sweep,
+  // from the scanned level l+1 S: E_l[2k+1] = S[k],
+  // E_l[2k] = fmaf(A_l[2k], S[k-1], E_l[2k]) for k >= 1.  The in-lane levels
+  // need no data movement; the higher ones move by warp shuffles.
+  template <int E>
   __device__ __forceinline__ void scan_regs(const ScanPlan& pl, const float* __restrict__ Acoef,
-                                            float (&e)[4]) const {
-    constexpr int ML = 8;  // levels of a 128-element scan
+                                            float (&e)[E]) const {
+    constexpr int LE = E == 8 ? 3 : 2;  // levels held inside a lane, above level 0
+    constexpr int ML = LE + 6;          // levels of a 32 E-element scan
+    static_assert(E == 4 || E == 8, "4 or 8 nodes per lane");
     int len[ML], off[ML];
     const int levels = pl.levels;
 #pragma unroll
@@ -397,25 +401,32 @@ struct Sim : SimDyn<DY> {
       off[l] = l < levels ? pl.off[l] : 0;
     }
     const int L = lane;
-    float l1[2];
+    float w[LE + 1][E];
 #pragma unroll
-    for (int c = 0; c < 2; ++c) {
-      const int k = 2 * L + c;
-      l1[c] = k < len[1] ? fmaf(Acoef[off[0] + 2 * k + 1], e[2 * c], e[2 * c + 1]) : 0.f;
+    for (int i = 0; i < E; ++i) w[0][i] = e[i];
+#pragma unroll
+    for (int l = 0; l < LE; ++l) {
+      const int C = E >> (l + 1);
+#pragma unroll
+      for (int j = 0; j < E / 2; ++j)
+        if (j < C) {
+          const int k = L * C + j;
+          w[l + 1][j] = k < len[l + 1] ? fmaf(Acoef[off[l] + 2 * k + 1], w[l][2 * j], w[l][2 * j + 1]) : 0.f;
+        }
     }
     float v[ML];
 #pragma unroll
     for (int l = 0; l < ML; ++l) v[l] = 0.f;
-    v[2] = L < len[2] ? fmaf(Acoef[off[1] + 2 * L + 1], l1[0], l1[1]) : 0.f;
+    v[LE] = w[LE][0];
 #pragma unroll
-    for (int l = 2; l + 1 < ML; ++l) {
+    for (int l = LE; l + 1 < ML; ++l) {
       const float a = __shfl_sync(0xffffffffu, v[l], (2 * L) & 31);
       const float b = __shfl_sync(0xffffffffu, v[l], (2 * L + 1) & 31);
       if (L < len[l + 1]) v[l + 1] = fmaf(Acoef[off[l] + 2 * L + 1], a, b);
     }
     // down-sweep from the top: level l from the scanned level l + 1
 #pragma unroll
-    for (int l = ML - 2; l >= 2; --l) {
+    for (int l = ML - 2; l >= LE; --l) {
       const int src = (L & 1) ? (L - 1) >> 1 : (L >> 1) - 1;
       const float sv = __shfl_sync(0xffffffffu, v[l + 1], src & 31);
       if (l + 1 < levels && L < len[l]) {
@@ -423,23 +434,29 @@ struct Sim : SimDyn<DY> {
         else if (L >= 2) v[l] = fmaf(Acoef[off[l] + L], sv, v[l]);         // E[2k] += A[2k] S[k-1]
       }
     }
-    {
-      const float sp = __shfl_up_sync(0xffffffffu, v[2], 1);
-      if (2 < levels) {
-        if (2 * L + 1 < len[1]) l1[1] = v[2];
-        if (2 * L < len[1] && L >= 1) l1[0] = fmaf(Acoef[off[1] + 2 * L], sp, l1[0]);
+    w[LE][0] = v[LE];
+    // in-lane levels: S[k-1] of the lane's first k is the previous lane's last
+#pragma unroll
+    for (int l = LE - 1; l >= 0; --l) {
+      const int C = E >> (l + 1);  // level l+1 elements per lane
+      float last = w[l + 1][0];
+#pragma unroll
+      for (int j = 1; j < E / 2; ++j)
+        if (j < C) last = w[l + 1][j];
+      const float sp = __shfl_up_sync(0xffffffffu, last, 1);
+      if (l + 1 < levels) {
+#pragma unroll
+        for (int j = 0; j < E / 2; ++j)
+          if (j < C) {
+            const int k = L * C + j;
+            const float prev = j == 0 ? sp : w[l + 1][j > 0 ? j - 1 : 0];
+            if (2 * k < len[l] && k >= 1) w[l][2 * j] = fmaf(Acoef[off[l] + 2 * k], prev, w[l][2 * j]);
+            if (2 * k + 1 < len[l]) w[l][2 * j + 1] = w[l + 1][j];
+          }
       }
     }
-    {
-      const float sp = __shfl_up_sync(0xffffffffu, l1[1], 1);
-      if (1 < levels) {
-        const int n0 = len[0];
-        if (4 * L < n0 && L >= 1) e[0] = fmaf(Acoef[off[0] + 4 * L], sp, e[0]);
-        if (4 * L + 1 < n0) e[1] = l1[0];
-        if (4 * L + 2 < n0) e[2] = fmaf(Acoef[off[0] + 4 * L + 2], l1[0], e[2]);
-        if (4 * L + 3 < n0) e[3] = l1[1];
-      }
-    }
+#pragma unroll
+    for (int i = 0; i < E; ++i) e[i] = w[0][i];
   }
 
   // Node ownership: warp w owns filaments w, w + NW, ...; lane l handles
@@ -546,12 +563,13 @@ struct Sim : SimDyn<DY> {
         const float* inv = s.coef + (thick ? cl.thick_inv : cl.thin_inv);
         if (n <= 64) thomas_shfl<2>(in + base, out + base, n, Af, Ab, inv);
         else if (n <= 96) thomas_shfl<3>(in + base, out + base, n, Af, Ab, inv);
-        else thomas_shfl<4>(in + base, out + base, n, Af, Ab, inv);
+        else if (n <= 128) thomas_shfl<4>(in + base, out + base, n, Af, Ab, inv);
+        else thomas_shfl<8>(in + base, out + base, n, Af, Ab, inv);
       }
       __syncwarp();
       return;
     }
-    float* buf = s.scan + warp * 128;  // this warp's reversal buffer (filaments <= 128 nodes)
+    float* buf = s.scan + warp * scan_cap(T);  // this warp's reversal buffer
     __syncwarp();
     for (int f = warp; f < nf; f += NW) {
       const bool thick = f < T.n_thick;
@@ -561,35 +579,43 @@ struct Sim : SimDyn<DY> {
       const float* Af = s.coef + (thick ? cl.thick_fwd : cl.thin_fwd);
       const float* Ab = s.coef + (thick ? cl.thick_back : cl.thin_back);
       const float* inv = s.coef + (thick ? cl.thick_inv : cl.thin_inv);
-      // forward scan in registers, (y * inv) reversed through this warp's
-      // scratch, backward scan, reversed store
-      float e[4];
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        const int i = 4 * lane + c;
-        e[c] = i < n ? in[base + i] : 0.f;
-      }
-      scan_regs(pl, Af, e);
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        const int i = 4 * lane + c;
-        if (i < n) buf[n - 1 - i] = e[c] * inv[i];
-      }
-      __syncwarp();
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        const int i = 4 * lane + c;
-        e[c] = i < n ? buf[i] : 0.f;
-      }
-      __syncwarp();
-      scan_regs(pl, Ab, e);
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        const int i = 4 * lane + c;
-        if (i < n) out[base + n - 1 - i] = e[c];
-      }
+      if (n <= 128) thomas_tree<4>(in, out, base, n, pl, Af, Ab, inv, buf);
+      else thomas_tree<8>(in, out, base, n, pl, Af, Ab, inv, buf);
     }
     __syncwarp();
+  }
+
+  // float32 Thomas solve of one filament in the reference's tree order:
+  // forward scan in registers, (y * inv) reversed through this warp's
+  // scratch, backward scan, reversed store.
+  template <int E>
+  __device__ __forceinline__ void thomas_tree(const float* in, float* out, int base, int n, const ScanPlan& pl,
+                                              const float* Af, const float* Ab, const float* inv, float* buf) {
+    float e[E];
+#pragma unroll
+    for (int c = 0; c < E; ++c) {
+      const int i = E * lane + c;
+      e[c] = i < n ? in[base + i] : 0.f;
+    }
+    scan_regs<E>(pl, Af, e);
+#pragma unroll
+    for (int c = 0; c < E; ++c) {
+      const int i = E * lane + c;
+      if (i < n) buf[n - 1 - i] = e[c] * inv[i];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int c = 0; c < E; ++c) {
+      const int i = E * lane + c;
+      e[c] = i < n ? buf[i] : 0.f;
+    }
+    __syncwarp();
+    scan_regs<E>(pl, Ab, e);
+#pragma unroll
+    for (int c = 0; c < E; ++c) {
+      const int i = E * lane + c;
+      if (i < n) out[base + n - 1 - i] = e[c];
+    }
   }
 
   // One-barrier block reduction of K floats (sum) with an optional max in
@@ -1138,7 +1164,8 @@ struct Sim : SimDyn<DY> {
       const float* inv = s.coef + (thick ? cl.thick_inv : cl.thin_inv);
       if (n <= 64) g += cg_filament<2>(base, n, Af, Ab, inv, alpha, beta, update, first, last, bad);
       else if (n <= 96) g += cg_filament<3>(base, n, Af, Ab, inv, alpha, beta, update, first, last, bad);
-      else g += cg_filament<4>(base, n, Af, Ab, inv, alpha, beta, update, first, last, bad);
+      else if (n <= 128) g += cg_filament<4>(base, n, Af, Ab, inv, alpha, beta, update, first, last, bad);
+      else g += cg_filament<8>(base, n, Af, Ab, inv, alpha, beta, update, first, last, bad);
     }
     __syncwarp();
     return g;

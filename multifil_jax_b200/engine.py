@@ -184,12 +184,20 @@ def topo_desc_arrays(topo) -> Dict[str, np.ndarray]:
     """Host arrays of a SarcTopology in the layout ``mf_topo_desc`` expects."""
     from .topology import thin_rest_cumsum
     c = np.ascontiguousarray
+    # the device lattice has three faces per thin filament; a two-face
+    # (invertebrate) lattice gets an empty third face that no head targets
+    f2s = np.asarray(topo.face_to_sites, np.int32)
+    npf = np.asarray(topo.n_sites_per_face, np.int32)
+    if f2s.shape[1] < 3:
+        pad = 3 - f2s.shape[1]
+        f2s = np.concatenate([f2s, np.full((f2s.shape[0], pad, f2s.shape[2]), -1, np.int32)], axis=1)
+        npf = np.concatenate([npf, np.zeros((npf.shape[0], pad), np.int32)], axis=1)
     return dict(
         xb_to_thin_id=c(topo.xb_to_thin_id, dtype=np.int32),
         xb_to_thin_face=c(topo.xb_to_thin_face, dtype=np.int32),
         xb_valid=c(topo.xb_valid, dtype=np.uint8),
-        face_to_sites=c(topo.face_to_sites, dtype=np.int32),
-        n_sites_per_face=c(topo.n_sites_per_face, dtype=np.int32),
+        face_to_sites=c(f2s, dtype=np.int32),
+        n_sites_per_face=c(npf, dtype=np.int32),
         tm_prev_neighbor=c(topo.tm_prev_neighbor, dtype=np.int32),
         tm_next_neighbor=c(topo.tm_next_neighbor, dtype=np.int32),
         crown_offsets=c(topo.crown_offsets, dtype=np.float32),

@@ -94,9 +94,11 @@ STATIC_FIELDS = frozenset({
 class StaticParams:
     """Structural configuration (reference ``core/params.py:563-733``).
 
-    Only the vertebrate lattice (``actin_geometry='vertebrate'``, three heads
-    per crown, no superlattice) is built by this package; the topology builder
-    rejects the invertebrate branches with a ``NotImplementedError``.
+    ``actin_geometry`` is ``'vertebrate'`` (1 thick : 2 thin, three faces per
+    thin filament) or ``'invertebrate'`` (1 thick : 3 thin, two faces);
+    ``n_superlattice_classes`` 3 staggers the thick filaments of the insect
+    myosin superlattice; ``legacy_crown_geometry`` uses the fixed crown-face
+    table.
     """
     n_crowns: int = 52
     n_polymers_per_thin: int = 15
@@ -234,10 +236,42 @@ def get_cardiac_params() -> Tuple[StaticParams, DynamicParams]:
     return StaticParams(), DynamicParams(**_CARDIAC_OVERRIDES)
 
 
+# Insect indirect flight muscle geometry shared by the two insect presets
+# (reference core/params.py:1185-1196 and :1264-1275); the Drosophila preset
+# adds the 3-class myosin superlattice.
+_IFM_STATIC = {
+    'actin_geometry': 'invertebrate',
+    'thick_crown_spacing': 14.5,
+    'actin_half_pitch': 38.7,
+    'mono_per_poly': 28,
+    'polymer_base_turns': 13,
+    'n_xb_per_crown': 4,
+    'crown_rotation_deg': 33.75,
+    'target_zone_wiggle': float(np.radians(26.0)),
+    'n_crowns': 100,
+    'n_polymers_per_thin': 20,
+}
+_IFM_DYNAMIC = {'titin_a': 40.0, 'titin_b': 0.025, 'titin_rest': 50.0}
+
+
+def get_lethocerus_params() -> Tuple[StaticParams, DynamicParams]:
+    """Lethocerus indirect flight muscle (reference ``core/params.py:982-1202``):
+    invertebrate lattice, four heads per crown, 100 crowns, no superlattice."""
+    return StaticParams(**_IFM_STATIC), DynamicParams(**_IFM_DYNAMIC)
+
+
+def get_drosophila_params() -> Tuple[StaticParams, DynamicParams]:
+    """Drosophila indirect flight muscle (reference ``core/params.py:1205-1281``):
+    the Lethocerus geometry with the 3-class myosin superlattice (lattices need
+    an even ``nrows`` and ``ncols`` a multiple of 3)."""
+    return StaticParams(**_IFM_STATIC, n_superlattice_classes=3), DynamicParams(**_IFM_DYNAMIC)
+
+
 def params_table(rows) -> np.ndarray:
     """Stack DynamicParams (all-scalar) into a float32 [B, 44] table."""
     return np.stack([dp.param_row() for dp in rows]).astype(np.float32)
 
 
 __all__ = ['StaticParams', 'DynamicParams', 'DYNAMIC_FIELDS', 'STATIC_FIELDS', 'N_PARAMS',
-           'PARAM_INDEX', 'get_skeletal_params', 'get_cardiac_params', 'params_table']
+           'PARAM_INDEX', 'get_skeletal_params', 'get_cardiac_params', 'get_lethocerus_params',
+           'get_drosophila_params', 'params_table']

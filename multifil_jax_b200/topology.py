@@ -1,13 +1,23 @@
-"""Vertebrate half-sarcomere lattice: which filament faces which, once per size.
+"""Half-sarcomere lattice: which filament faces which, once per size.
 
 :meth:`SarcTopology.create` reproduces the reference builder
-(``multifil_jax/core/sarc_geometry.py:379-645``) for the vertebrate lattice
-(1 thick : 2 thin, thin filaments at trigonal interstices, three heads per
-crown).  Every array it produces must be bit-identical to the reference's, so
-the arithmetic below keeps the reference's float32/float64 dtype flow step by
+(``multifil_jax/core/sarc_geometry.py:379-645``) for both lattices:
+
+* vertebrate: 1 thick : 2 thin, thin filaments at trigonal interstices with
+  three faces, three heads per crown;
+* invertebrate (insect flight muscle): 1 thick : 3 thin, thin filaments at the
+  midpoints of thick-thick edges with two faces (sarc_geometry.py:915-1005),
+  each thin filament's binding-site grid turned and shifted by its 3-fold
+  registration class (:1134-1170, :1230-1262), optionally with the 3-class
+  myosin superlattice of the thick filaments (:1118-1131) and any number of
+  heads per crown (four in the insect presets, about half of them without a
+  partner: ``xb_valid``);
+* the legacy fixed crown-face table (:1357-1367, :1443-1447).
+
+Every array it produces must be bit-identical to the reference's, so the
+arithmetic below keeps the reference's float32/float64 dtype flow step by
 step (numpy promotion rules included); the golden fixtures in
-``tests/golden`` pin that.  The invertebrate / superlattice / legacy-face
-branches are not part of this package and raise ``NotImplementedError``.
+``tests/golden`` pin that.
 
 Beyond the reference's arrays, :meth:`SarcTopology.device_arrays` derives the
 compact layout the CUDA kernels read (per-XB target thin and face, per-face
@@ -23,6 +33,13 @@ from .params import StaticParams, DynamicParams
 
 SQRT3 = np.float32(np.sqrt(3))
 THICK_THIN_DISTANCE = np.float32(1.0 / np.sqrt(3))
+# invertebrate: thin filaments half way along thick-thick edges, thick faces
+# pointing along the edges (sarc_geometry.py:80, :101)
+THICK_THIN_DISTANCE_INVERTEBRATE = np.float32(0.5)
+THICK_FACE_ANGLES_INVERTEBRATE = np.array([0, 60, 120, 180, 240, 300], dtype=np.float32) * np.pi / 180
+N_REGISTRATION_CLASSES = 3
+# legacy crown levels 1..3 -> the three thick faces their heads use (sarc_geometry.py:1357)
+LEGACY_FACE_TABLE = np.array([[0, 2, 4], [1, 3, 5], [0, 2, 4]])
 # thin-face direction vectors, index = orientation code (sarc_geometry.py:88-95)
 ORIENTATION_VECTORS = np.array([
     [0.866, -0.5], [0.0, -1.0], [-0.866, -0.5],
@@ -136,6 +153,123 @@ def _thin_positions(thick_pos, box_x, box_y, periodic):
     return np.array(positions, dtype=np.float32), orientations
 
 
+def _thin_positions_on_edges(thick_pos, box_x, box_y, periodic):
+    """Invertebrate thin filaments at edge midpoints (sarc_geometry.py:915-1005).
+
+    For every thick filament and each of its six neighbour directions with a
+    thick filament one lattice unit away, one thin filament half way along
+    the edge (each edge once); its two faces look back at the two thick
+    filaments.  Returned sorted top row first, then by x, with the thick pair
+    of every edge.
+    """
+    tol = 0.1
+    dirs = np.array([0, 60, 120, 180, 240, 300], dtype=np.float32) * np.pi / 180
+    face_dirs = np.array([np.arctan2(v[1], v[0]) for v in ORIENTATION_VECTORS])
+
+    def nearest_code(a):
+        d = np.abs(face_dirs - a)
+        d = np.minimum(d, 2 * np.pi - d)
+        return int(np.argmin(d))
+
+    def thick_at(x, y):
+        for idx, q in enumerate(thick_pos):
+            if periodic:
+                dx = x - q[0]
+                dy = y - q[1]
+                dx = dx - box_x * np.round(dx / box_x)
+                dy = dy - box_y * np.round(dy / box_y)
+                dist = np.sqrt(dx ** 2 + dy ** 2)
+            else:
+                dist = np.sqrt((x - q[0]) ** 2 + (y - q[1]) ** 2)
+            if dist < tol:
+                return idx
+        return None
+
+    edges, seen = [], set()
+    for i, p in enumerate(thick_pos):
+        for a in dirs:
+            nx = p[0] + 1.0 * np.cos(a)
+            ny = p[1] + 1.0 * np.sin(a)
+            if periodic:
+                nx = _wrap_x(nx, box_x)
+                ny = _wrap_y(ny, box_y)
+            j = thick_at(nx, ny)
+            if j is None:
+                continue
+            mx = p[0] + 0.5 * 1.0 * np.cos(a)
+            my = p[1] + 0.5 * 1.0 * np.sin(a)
+            if periodic:
+                mx = _wrap_x(mx, box_x)
+                my = _wrap_y(my, box_y)
+            k = (round(round(mx, 4) % box_x, 3), round(round(my, 4) % box_y, 3))
+            if k in seen:
+                continue
+            seen.add(k)
+            back = a + np.pi
+            if back > np.pi:
+                back -= 2 * np.pi
+            oi, oj = nearest_code(back), nearest_code(a)
+            if oi == oj:
+                oj = (oi + 3) % 6
+            edges.append((np.float32(mx), np.float32(my), (oi, oj), (i, j)))
+    edges.sort(key=lambda e: (-e[1], e[0]))
+    if not edges:
+        return np.zeros((0, 2), dtype=np.float32), [], []
+    return (np.array([[e[0], e[1]] for e in edges], dtype=np.float32), [e[2] for e in edges],
+            [e[3] for e in edges])
+
+
+def _edge_connectivity(thick_pos, thin_pos, pairs, box_x, box_y, periodic):
+    """thick_to_thin / thin_to_thick of the edge lattice (sarc_geometry.py:1037-1055):
+    thin face 0 faces the first thick filament of its edge, face 1 the second; on
+    the thick side the face whose direction is closest to the thin filament."""
+    n_thick, n_thin = len(thick_pos), len(thin_pos)
+    t2n = [[None] * 6 for _ in range(n_thick)]
+    n2t = [[None] * 2 for _ in range(n_thin)]
+    for k in range(n_thin):
+        q = thin_pos[k]
+        for face, t in enumerate(pairs[k]):
+            p = thick_pos[t]
+            dx = q[0] - p[0]
+            dy = q[1] - p[1]
+            if periodic:
+                dx = dx - box_x * np.round(dx / box_x)
+                dy = dy - box_y * np.round(dy / box_y)
+            ang = np.arctan2(dy, dx)
+            best, best_d = 0, np.inf
+            for f in range(6):
+                d = abs((ang - THICK_FACE_ANGLES_INVERTEBRATE[f] + np.pi) % (2 * np.pi) - np.pi)
+                if d < best_d:
+                    best_d, best = d, f
+            n2t[k][face] = (t, best)
+            t2n[t][best] = (k, face)
+    return t2n, n2t
+
+
+def _registration_classes(thick_pos, pairs, box_x, box_y, periodic):
+    """3-fold actin registration class of every edge thin filament: the edge's
+    direction modulo 180 degrees in steps of 60 (sarc_geometry.py:1134-1170)."""
+    cls = np.empty(len(pairs), dtype=np.int32)
+    for k, (i, j) in enumerate(pairs):
+        dx = thick_pos[j][0] - thick_pos[i][0]
+        dy = thick_pos[j][1] - thick_pos[i][1]
+        if periodic:
+            dx = dx - box_x * np.round(dx / box_x)
+            dy = dy - box_y * np.round(dy / box_y)
+        deg = np.degrees(np.arctan2(dy, dx)) % 180.0
+        cls[k] = int(np.round(deg / 60.0)) % N_REGISTRATION_CLASSES
+    return cls
+
+
+def _superlattice_classes(n_thick, ncols, n_classes):
+    """Thick-filament class of the myosin superlattice: (q - r) mod n over the
+    axial coordinates of the row-major grid (sarc_geometry.py:1118-1131)."""
+    idx = np.arange(n_thick)
+    row, col = idx // ncols, idx % ncols
+    q = col - (row - (row & 1)) // 2
+    return ((q - row) % n_classes).astype(np.int32)
+
+
 def _thin_index_at(thin_pos, x, y, box_x, box_y, periodic, tol=0.01):
     for i, q in enumerate(thin_pos):
         d = (_min_image_dist([x, y], q, box_x, box_y) if periodic
@@ -228,13 +362,20 @@ def _crown_offsets(n_crowns, bare_zone, spacing):
 
 
 def _binding_sites(orients, thin_starts, n_thin, n_polymers, half_pitch, mono_per_poly,
-                   base_turns, wiggle):
+                   base_turns, wiggle, reg_class=None):
     """Actin-helix binding sites per thin filament, sorted M-line-far first.
 
     Same monomer grid, azimuth test, site ordering, chain parity and chain
-    neighbour rules as sarc_geometry.py:1194-1352 (vertebrate: registration
-    class 0 for every filament).
+    neighbour rules as sarc_geometry.py:1194-1352.  A thin filament of
+    registration class c has its helix start advanced by
+    c * round(mono_per_poly / 3) monomers and its grid shifted by
+    c * half_pitch / 3 towards the Z-line (class 0, every vertebrate filament:
+    no change).
     """
+    if reg_class is None:
+        reg_class = np.zeros(n_thin, dtype=np.int32)
+    ang_step = int(round(mono_per_poly / N_REGISTRATION_CLASSES))
+    ax_step = np.float32(half_pitch / N_REGISTRATION_CLASSES)
     base_len = np.float32(2 * half_pitch)
     base_turns = np.float32(base_turns)
     rev = np.float32(2 * np.pi)
@@ -246,7 +387,9 @@ def _binding_sites(orients, thin_starts, n_thin, n_polymers, half_pitch, mono_pe
                           (-0.866, 0.5), (0, 1.0), (0.866, 0.5)], dtype=np.float32)
     out = dict(offsets=[], rests=[], faces=[], chains=[], prev=[], next=[])
     for i in range(n_thin):
-        start = thin_starts[i] + 0
+        c = int(reg_class[i])
+        start = thin_starts[i] + c * ang_step
+        grid = mono_off + c * ax_step
         ang = np.array([((m + start + 1) % mono_per_poly) * pitch % rev for m in range(n_mono)],
                        dtype=np.float32)
         fv = face_vecs[list(orients[i])]
@@ -254,14 +397,14 @@ def _binding_sites(orients, thin_starts, n_thin, n_polymers, half_pitch, mono_pe
         fang = np.where(fang < 0, fang + rev, fang)
         w = np.float32(wiggle)
         hits = [np.where(np.abs(ang - a) < w)[0] for a in fang]
-        by_face = [mono_off[h] for h in hits]
+        by_face = [grid[h] for h in hits]
         if by_face and any(len(f) > 0 for f in by_face):
             flat = np.sort(np.hstack(by_face))[::-1]
         else:
-            flat = mono_off[::-1]
+            flat = grid[::-1]
         chain = []
         for o in flat:
-            m = np.where(np.abs(mono_off - o) < 1e-6)[0]
+            m = np.where(np.abs(grid - o) < 1e-6)[0]
             chain.append((m[0] if len(m) else 0) % 2)
         chain = np.array(chain, dtype=np.int32)
         n = len(flat)
@@ -293,9 +436,10 @@ def _binding_sites(orients, thin_starts, n_thin, n_polymers, half_pitch, mono_pe
 
 
 def _xb_maps(t2n, face_sites, n_per_face, thick_starts, n_thick, n_crowns, width,
-             n_xb, rot_deg, wiggle_deg):
-    """Fixed-width crossbridge -> candidate-site maps (sarc_geometry.py:1370-1492,
-    continuous-azimuth branch)."""
+             n_xb, rot_deg, wiggle_deg, legacy=False):
+    """Fixed-width crossbridge -> candidate-site maps (sarc_geometry.py:1370-1492):
+    a head's thick face from its azimuth (accepted within ``wiggle_deg`` of a
+    hexagonal direction, else no partner), or from the legacy crown-level table."""
     total = n_thick * n_crowns * n_xb
     thin_id = np.zeros(total, dtype=np.int32)
     thin_face = np.zeros(total, dtype=np.int32)
@@ -305,12 +449,17 @@ def _xb_maps(t2n, face_sites, n_per_face, thick_starts, n_thick, n_crowns, width
         t = x // (n_crowns * n_xb)
         local = x % (n_crowns * n_xb)
         crown, k = local // n_xb, local % n_xb
-        eff = crown + (thick_starts[t] - 1)
-        az = (k * (360.0 / n_xb) + eff * rot_deg) % 360.0
-        face = int(round(az / 60.0)) % 6
-        res = abs(az - face * 60.0)
-        res = min(res, 360.0 - res)
-        if res < wiggle_deg:
+        if legacy:
+            face = LEGACY_FACE_TABLE[(crown + thick_starts[t] - 1) % 3, k]
+            hit = True
+        else:
+            eff = crown + (thick_starts[t] - 1)
+            az = (k * (360.0 / n_xb) + eff * rot_deg) % 360.0
+            face = int(round(az / 60.0)) % 6
+            res = abs(az - face * 60.0)
+            res = min(res, 360.0 - res)
+            hit = res < wiggle_deg
+        if hit:
             ti, tf = t2n[t, face, 0], t2n[t, face, 1]
         else:
             ti, tf = -1, 0
@@ -359,14 +508,10 @@ class SarcTopology:
                thick_starts: Optional[List[int]] = None) -> 'SarcTopology':
         """Build the lattice on the CPU (reference ``sarc_geometry.py:379-645``)."""
         sp = static_params if static_params is not None else StaticParams()
-        if sp.actin_geometry != 'vertebrate':
-            raise NotImplementedError("only the vertebrate lattice is built by multifil_jax_b200")
-        if sp.legacy_crown_geometry:
-            raise NotImplementedError("legacy_crown_geometry is not supported")
-        if sp.n_superlattice_classes != 1:
-            raise NotImplementedError("myosin superlattice is not supported")
         if nrows < 1 or ncols < 1:
             raise ValueError("nrows and ncols must be >= 1")
+        vert = sp.actin_geometry == 'vertebrate'
+        n_faces = 3 if vert else 2
         n_xb = sp.n_xb_per_crown
         thick_pos, box_x, box_y = _thick_positions(nrows, ncols)
         n_thick = len(thick_pos)
@@ -376,22 +521,31 @@ class SarcTopology:
             if len(thick_starts) != n_thick:
                 raise ValueError(f"thick_starts must have length n_thick={n_thick}, got {len(thick_starts)}")
             ts = np.array(thick_starts, dtype=np.int32)
-        thin_pos, orients = _thin_positions(thick_pos, box_x, box_y, periodic)
+        if vert:
+            thin_pos, orients = _thin_positions(thick_pos, box_x, box_y, periodic)
+            pairs, reg = None, None
+        else:
+            thin_pos, orients, pairs = _thin_positions_on_edges(thick_pos, box_x, box_y, periodic)
+            reg = _registration_classes(thick_pos, pairs, box_x, box_y, periodic)
         n_thin = len(thin_pos)
         if thin_starts is None:
-            tn = _spread_starts(n_thin, 0, 26)
+            # invertebrate: the registration class is the only phase variation
+            tn = _spread_starts(n_thin, 0, 26) if vert else np.zeros(n_thin, dtype=np.int32)
         else:
             if len(thin_starts) != n_thin:
                 raise ValueError(f"thin_starts must have length n_thin={n_thin}, got {len(thin_starts)}")
             tn = np.array(thin_starts, dtype=np.int32)
 
-        t2n_list, n2t_list = _connectivity(thick_pos, thin_pos, orients, box_x, box_y, periodic)
+        if vert:
+            t2n_list, n2t_list = _connectivity(thick_pos, thin_pos, orients, box_x, box_y, periodic)
+        else:
+            t2n_list, n2t_list = _edge_connectivity(thick_pos, thin_pos, pairs, box_x, box_y, periodic)
         t2n = np.full((n_thick, 6, 2), -1, dtype=np.int32)
         for t, faces in enumerate(t2n_list):
             for f, c in enumerate(faces):
                 if c is not None:
                     t2n[t, f] = [c[0], c[1]]
-        n2t = np.full((n_thin, 3, 2), -1, dtype=np.int32)
+        n2t = np.full((n_thin, n_faces, 2), -1, dtype=np.int32)
         for i, faces in enumerate(n2t_list):
             for f, c in enumerate(faces):
                 if c is not None:
@@ -400,17 +554,22 @@ class SarcTopology:
             missing = np.argwhere(t2n[:, :, 0] < 0)
             if len(missing):
                 raise ValueError(f"thick_to_thin has {len(missing)} unconnected (thick, face) pair(s) "
-                                 f"under periodic=True for nrows={nrows}, ncols={ncols}")
+                                 f"under periodic=True for nrows={nrows}, ncols={ncols}, "
+                                 f"actin_geometry='{sp.actin_geometry}'; the invertebrate lattice needs "
+                                 f"an even nrows")
+        if periodic and sp.n_superlattice_classes == 3 and (nrows % 2 != 0 or ncols % 3 != 0):
+            raise ValueError(f"n_superlattice_classes=3 requires nrows even and ncols a multiple of 3 "
+                             f"under periodic=True (got nrows={nrows}, ncols={ncols})")
         titin = [(t, f, c[0], c[1]) for t in range(n_thick) for f in range(6)
                  if (c := t2n_list[t][f]) is not None]
         titin_arr = (np.array(titin, dtype=np.int32) if titin else np.zeros((0, 4), dtype=np.int32))
 
-        bare = (sp.thick_bare_zone + np.zeros(n_thick, dtype=np.int32).astype(np.float32)
-                * (sp.thick_crown_spacing / sp.n_superlattice_classes))
+        sl = _superlattice_classes(n_thick, ncols, sp.n_superlattice_classes)
+        bare = (sp.thick_bare_zone + sl.astype(np.float32) * (sp.thick_crown_spacing / sp.n_superlattice_classes))
         crown_off, crown_rests = _crown_offsets(sp.n_crowns, bare, sp.thick_crown_spacing)
 
         bs = _binding_sites(orients, tn, n_thin, sp.n_polymers_per_thin, sp.actin_half_pitch,
-                            sp.mono_per_poly, sp.polymer_base_turns, sp.target_zone_wiggle)
+                            sp.mono_per_poly, sp.polymer_base_turns, sp.target_zone_wiggle, reg)
         max_sites = max(len(o) for o in bs['offsets'])
         b_off = np.zeros((n_thin, max_sites), dtype=np.float32)
         b_rest = np.full((n_thin, max_sites), 2.77, dtype=np.float32)
@@ -425,8 +584,8 @@ class SarcTopology:
             prv[i, :n] = bs['prev'][i]
             nxt[i, :n] = bs['next'][i]
         width = max((len(s) for faces in bs['faces'] for s in faces), default=0)
-        f2s = np.full((n_thin, 3, width), -1, dtype=np.int32)
-        npf = np.zeros((n_thin, 3), dtype=np.int32)
+        f2s = np.full((n_thin, n_faces, width), -1, dtype=np.int32)
+        npf = np.zeros((n_thin, n_faces), dtype=np.int32)
         for i in range(n_thin):
             for j, s in enumerate(bs['faces'][i]):
                 f2s[i, j, :len(s)] = s
@@ -434,14 +593,14 @@ class SarcTopology:
 
         thin_id, thin_face, sites, valid = _xb_maps(
             t2n, f2s, npf, ts, n_thick, sp.n_crowns, width, n_xb,
-            sp.crown_rotation_deg, sp.crown_face_wiggle_deg)
+            sp.crown_rotation_deg, sp.crown_face_wiggle_deg, sp.legacy_crown_geometry)
 
         edges = f32_linspace(sp.xb_bin_lo, sp.xb_bin_hi, sp.n_xb_bins + 1)
         centers = (np.float32(0.5) * (edges[:-1] + edges[1:])).astype(np.float32)
 
         return cls(
             n_thick=n_thick, n_crowns=sp.n_crowns, n_thin=n_thin, n_sites=max_sites,
-            n_titin=len(titin_arr), n_xb_per_crown=n_xb, n_faces_per_thin=3,
+            n_titin=len(titin_arr), n_xb_per_crown=n_xb, n_faces_per_thin=n_faces,
             max_sites_per_face=width, total_xbs=n_thick * sp.n_crowns * n_xb,
             n_xb_bins=sp.n_xb_bins,
             xb_to_thin_id=thin_id, xb_to_thin_face=thin_face, xb_to_site_indices=sites,

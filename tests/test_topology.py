@@ -41,9 +41,7 @@ def test_known_sizes():
         assert t.n_sites == 90 and t.max_sites_per_face == 30
 
 
-def test_unsupported_geometry_raises():
-    with pytest.raises(NotImplementedError):
-        SarcTopology.create(2, 2, StaticParams(actin_geometry='invertebrate'))
+def test_bad_lattice_arguments_raise():
     with pytest.raises(ValueError):
         SarcTopology.create(2, 2, thick_starts=[1, 2])
     with pytest.raises(ValueError):
