@@ -116,6 +116,7 @@ static cudaError_t launch(int nt, const StepArgs& a, int grid, int base, size_t 
 // per warp), else 256 (two per warp).  512 up to 4000 nodes, else 1024.  The
 // autotuner measures and overrides.
 static int default_threads(const TopoDev& t, bool precise) {
+  if (max_filament(t) > 128) return t.n_dof <= 4000 ? 512 : 1024;
   if (t.n_dof <= 1200) return (!precise || t.n_thick + t.n_thin <= 12) ? 384 : 256;
   if (t.n_dof <= 4000) return 512;
   return 1024;
@@ -128,6 +129,7 @@ static int default_threads(const TopoDev& t, bool precise) {
 static bool make_cfg(const TopoDev& t, int nt, bool precise, bool allow_regs, bool dyn, int smem_optin, Cfg& c,
                      PopShape ps = PopShape()) {
   c.threads = nt;
+  if (max_filament(t) > 128 && nt < kWideThreads) return false;  // no code for long filaments below 512
   if (precise && allow_regs && regcg_fits(t, nt)) {
     const size_t sm = smem_bytes(t, nt, LAYOUT_REGS, true, dyn, ps);
     if (sm + kStaticSmem <= (size_t)smem_optin) {
@@ -689,10 +691,22 @@ namespace {
 __global__ void tables_probe_kernel(const float* params, const float* centers, int nb, float pCa, float d,
                                     float dt, int sq64, float* cum_tm, float* cum_xb, float* pabs) {
   __shared__ float P[kNParams];
+  __shared__ TableCtx tc;
   for (int i = threadIdx.x; i < kNParams; i += blockDim.x) P[i] = params[i];
+  if (threadIdx.x == 0) {
+    tc.P = P;
+    tc.centers = centers;
+    tc.nb = nb;
+    tc.dtm = dt;
+    tc.sq64 = sq64;
+    tc.cum_tm = cum_tm;
+    tc.cum_xb = cum_xb;
+    tc.pabs = pabs;
+    tc.pop = PopShape();
+    tc.Pk = tc.fk = nullptr;
+  }
   __syncthreads();
-  build_tables_block(P, centers, nb, pCa, d, dt, sq64, cum_tm, cum_xb, pabs, true, true, true, nullptr, 0,
-                     (int)threadIdx.x, (int)blockDim.x, PopShape(), nullptr, nullptr);
+  build_tables_block(tc, pCa, d, true, true, true, nullptr, 0, (int)threadIdx.x, (int)blockDim.x);
 }
 
 }  // namespace

@@ -111,10 +111,9 @@ struct TopoDev {
 // Longest filament the kernels take (nodes), and the per-warp scan reversal
 // buffer of a lattice: 128 floats up to 128 nodes, else 256.
 constexpr int kMaxFilament = 256;
-MF_HD int scan_cap(const TopoDev& t) {
-  const int n = t.n_crowns > t.n_sites ? t.n_crowns : t.n_sites;
-  return n <= 128 ? 128 : 256;
-}
+constexpr int kWideThreads = 512;  // smallest CTA size for filaments of more than 128 nodes
+MF_HD int max_filament(const TopoDev& t) { return t.n_crowns > t.n_sites ? t.n_crowns : t.n_sites; }
+MF_HD int scan_cap(const TopoDev& t) { return max_filament(t) <= 128 ? 128 : 256; }
 
 // Byte layout of one condition's resident workspace (global memory).
 struct SlotLayout {

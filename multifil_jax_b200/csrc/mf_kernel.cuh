@@ -166,6 +166,18 @@ __device__ void carve(Sim<NT, PR, DY>& m, char* base, int layout) {
     if (pop.kx() > 1) m.s.xlab = (int8_t*)take(X);
     if (pop.kt() > 1) m.s.tlab = (int8_t*)take(S);
   }
+  // the table builder's inputs (the timestep is set by the caller)
+  TableCtx& tc = m.s.tab;
+  tc.P = m.s.P;
+  tc.centers = t.centers;
+  tc.nb = t.n_bins;
+  tc.sq64 = m.A.sq64_from;
+  tc.cum_tm = m.s.cum_tm;
+  tc.cum_xb = reinterpret_cast<float*>(m.ws + m.L.cum_xb);
+  tc.pabs = m.s.pabs;
+  tc.pop = pop;
+  tc.Pk = m.s.Pk;
+  tc.fk = m.s.fk;
 }
 
 // ---------------------------------------------------------------------------
@@ -454,7 +466,10 @@ __device__ void run_condition(const StepArgs& A, int ci) {
   m.status = 0;
   m.Tstride = cd.T;
   const int layout = (A.flags & FLAG_VEC_GLOBAL) ? LAYOUT_GLOBAL : ((A.flags & FLAG_REGS) ? LAYOUT_REGS : LAYOUT_SMEM);
-  if (m.tid == 0) carve(m, smem_raw, layout);
+  if (m.tid == 0) {
+    carve(m, smem_raw, layout);
+    m.s.tab.dtm = cd.dt;
+  }
   __syncthreads();
   m.lazy_tab = DY && m.lazy_tables_fit();
   // the host sets FLAG_REGS exactly when regcg_fits, n_cg > 0 and the

@@ -83,7 +83,10 @@ __device__ void run_state(const StepArgs& A, const StateIO& io, int b) {
   m.regcg = false;
   m.lazy_tab = false;
   const int layout = (A.flags & FLAG_VEC_GLOBAL) ? LAYOUT_GLOBAL : LAYOUT_SMEM;
-  if (m.tid == 0) carve(m, smem_raw, layout);
+  if (m.tid == 0) {
+    carve(m, smem_raw, layout);
+    m.s.tab.dtm = io.dt;
+  }
   __syncthreads();
   const int N = T.n_dof, X = T.total_xbs, S = T.n_sites_total, NTN = T.n_thick_nodes;
   const float* prow = io.params + (size_t)b * kNParams;

@@ -101,6 +101,22 @@ __device__ __forceinline__ float warp_max(float v) {
   return v;
 }
 
+// Per-condition inputs of the table builder, kept in the CTA's shared memory
+// (Smem::tab) so that a call passes one address and the per-call values.
+struct TableCtx {
+  const float* P;        // [44] wild-type parameter row
+  const float* centers;  // [n_bins] bin centres
+  int nb;                // n_bins
+  float dtm;             // timestep (ms)
+  int sq64;              // float64 squaring from this s on
+  float* cum_tm;         // [kt*27*16]
+  float* cum_xb;         // [kx*2*n_bins*36]
+  float* pabs;           // [kx*2*n_bins*3]
+  PopShape pop;
+  const float* Pk;       // [K*44] population rows
+  const float* fk;       // [K] fractions
+};
+
 // Shared-memory carve of one condition.
 struct Smem {
   float* x;       // [N] node positions (precise mode: displacements)
@@ -155,6 +171,7 @@ struct Smem {
   float* fk;         // [K]
   int8_t* xlab;      // [X] when the crossbridge tables are per population
   int8_t* tlab;      // [S] when the tropomyosin tables are per population
+  TableCtx tab;      // the table builder's per-condition inputs
 };
 
 // Thomas coefficient block layout inside coef (floats).
@@ -200,11 +217,18 @@ static __device__ __forceinline__ void blend_acc(float (&acc)[R][C], const float
     for (int j = 0; j < C; ++j) acc[i][j] = __fadd_rn(acc[i][j], __fmul_rn(f, q[i][j]));
 }
 
-static __device__ __noinline__ void build_tables_block(const float* P, const float* centers, int nb, float pCa, float d,
-                                                float dtm, int sq64, float* cum_tm, float* cum_xb, float* pabs,
-                                                bool tm, bool sampling, bool absorbing, const int16_t* keys,
-                                                int nkeys, int tid, int nt, PopShape pop, const float* Pk,
-                                                const float* fk) {
+static __device__ __noinline__ void build_tables_block(const TableCtx& c, float pCa, float d, bool tm, bool sampling,
+                                                bool absorbing, const int16_t* keys, int nkeys, int tid, int nt) {
+  const float* P = c.P;
+  const float* centers = c.centers;
+  const int nb = c.nb, sq64 = c.sq64;
+  const float dtm = c.dtm;
+  float* cum_tm = c.cum_tm;
+  float* cum_xb = c.cum_xb;
+  float* pabs = c.pabs;
+  const PopShape pop = c.pop;
+  const float* Pk = c.Pk;
+  const float* fk = c.fk;
   const int h = tid & 1;                                  // which half of the rows
   const int pair = tid >> 1, npairs = nt >> 1;
   const unsigned pmask = 3u << (tid & 30);
@@ -300,6 +324,10 @@ template <int NT, bool PR, bool DY>
 struct Sim : SimDyn<DY> {
   using SimDyn<DY>::dyn;
   static constexpr int NW = NT / 32;
+  // Filaments longer than 128 nodes (8 per lane in the scans and CG passes)
+  // run only in CTAs of 512 or more threads, which the host picks for them;
+  // the smaller instances carry no code for them.
+  static constexpr bool kWide = NT >= kWideThreads;
   // The lattice, the shared-memory carve and the layouts live in CTA-shared
   // structs at fixed addresses: reading a field is one shared load, and none
   // of the ~50 pointers and sizes occupies a register across the step loop.
@@ -459,6 +487,65 @@ struct Sim : SimDyn<DY> {
     for (int i = 0; i < E; ++i) e[i] = w[0][i];
   }
 
+  // The same dataflow for 4 nodes per lane, written out level by level (the
+  // form of the 128-node instances, which keeps fewer values live than the
+  // general template).
+  __device__ __forceinline__ void scan_regs4(const ScanPlan& pl, const float* __restrict__ Acoef,
+                                            float (&e)[4]) const {
+    constexpr int ML = 8;  // levels of a 128-element scan
+    int len[ML], off[ML];
+    const int levels = pl.levels;
+#pragma unroll
+    for (int l = 0; l < ML; ++l) {
+      len[l] = l < levels ? pl.len[l] : 0;
+      off[l] = l < levels ? pl.off[l] : 0;
+    }
+    const int L = lane;
+    float l1[2];
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const int k = 2 * L + c;
+      l1[c] = k < len[1] ? fmaf(Acoef[off[0] + 2 * k + 1], e[2 * c], e[2 * c + 1]) : 0.f;
+    }
+    float v[ML];
+#pragma unroll
+    for (int l = 0; l < ML; ++l) v[l] = 0.f;
+    v[2] = L < len[2] ? fmaf(Acoef[off[1] + 2 * L + 1], l1[0], l1[1]) : 0.f;
+#pragma unroll
+    for (int l = 2; l + 1 < ML; ++l) {
+      const float a = __shfl_sync(0xffffffffu, v[l], (2 * L) & 31);
+      const float b = __shfl_sync(0xffffffffu, v[l], (2 * L + 1) & 31);
+      if (L < len[l + 1]) v[l + 1] = fmaf(Acoef[off[l] + 2 * L + 1], a, b);
+    }
+    // down-sweep from the top: level l from the scanned level l + 1
+#pragma unroll
+    for (int l = ML - 2; l >= 2; --l) {
+      const int src = (L & 1) ? (L - 1) >> 1 : (L >> 1) - 1;
+      const float sv = __shfl_sync(0xffffffffu, v[l + 1], src & 31);
+      if (l + 1 < levels && L < len[l]) {
+        if (L & 1) v[l] = sv;                                              // E[2k+1] = S[k]
+        else if (L >= 2) v[l] = fmaf(Acoef[off[l] + L], sv, v[l]);         // E[2k] += A[2k] S[k-1]
+      }
+    }
+    {
+      const float sp = __shfl_up_sync(0xffffffffu, v[2], 1);
+      if (2 < levels) {
+        if (2 * L + 1 < len[1]) l1[1] = v[2];
+        if (2 * L < len[1] && L >= 1) l1[0] = fmaf(Acoef[off[1] + 2 * L], sp, l1[0]);
+      }
+    }
+    {
+      const float sp = __shfl_up_sync(0xffffffffu, l1[1], 1);
+      if (1 < levels) {
+        const int n0 = len[0];
+        if (4 * L < n0 && L >= 1) e[0] = fmaf(Acoef[off[0] + 4 * L], sp, e[0]);
+        if (4 * L + 1 < n0) e[1] = l1[0];
+        if (4 * L + 2 < n0) e[2] = fmaf(Acoef[off[0] + 4 * L + 2], l1[0], e[2]);
+        if (4 * L + 3 < n0) e[3] = l1[1];
+      }
+    }
+  }
+
   // Node ownership: warp w owns filaments w, w + NW, ...; lane l handles
   // nodes l, l + 32, ... of each.  Every elementwise vector update and the
   // Thomas solves stay inside a warp, so only the crossbridge coupling and
@@ -563,13 +650,13 @@ struct Sim : SimDyn<DY> {
         const float* inv = s.coef + (thick ? cl.thick_inv : cl.thin_inv);
         if (n <= 64) thomas_shfl<2>(in + base, out + base, n, Af, Ab, inv);
         else if (n <= 96) thomas_shfl<3>(in + base, out + base, n, Af, Ab, inv);
-        else if (n <= 128) thomas_shfl<4>(in + base, out + base, n, Af, Ab, inv);
-        else thomas_shfl<8>(in + base, out + base, n, Af, Ab, inv);
+        else if (!kWide || n <= 128) thomas_shfl<4>(in + base, out + base, n, Af, Ab, inv);
+        else if constexpr (kWide) thomas_shfl<8>(in + base, out + base, n, Af, Ab, inv);
       }
       __syncwarp();
       return;
     }
-    float* buf = s.scan + warp * scan_cap(T);  // this warp's reversal buffer
+    float* buf = s.scan + warp * (kWide ? scan_cap(T) : 128);  // this warp's reversal buffer
     __syncwarp();
     for (int f = warp; f < nf; f += NW) {
       const bool thick = f < T.n_thick;
@@ -579,8 +666,8 @@ struct Sim : SimDyn<DY> {
       const float* Af = s.coef + (thick ? cl.thick_fwd : cl.thin_fwd);
       const float* Ab = s.coef + (thick ? cl.thick_back : cl.thin_back);
       const float* inv = s.coef + (thick ? cl.thick_inv : cl.thin_inv);
-      if (n <= 128) thomas_tree<4>(in, out, base, n, pl, Af, Ab, inv, buf);
-      else thomas_tree<8>(in, out, base, n, pl, Af, Ab, inv, buf);
+      if (!kWide || n <= 128) thomas_tree<4>(in, out, base, n, pl, Af, Ab, inv, buf);
+      else if constexpr (kWide) thomas_tree<8>(in, out, base, n, pl, Af, Ab, inv, buf);
     }
     __syncwarp();
   }
@@ -597,7 +684,8 @@ struct Sim : SimDyn<DY> {
       const int i = E * lane + c;
       e[c] = i < n ? in[base + i] : 0.f;
     }
-    scan_regs<E>(pl, Af, e);
+    if constexpr (E == 4) scan_regs4(pl, Af, e);
+    else scan_regs<E>(pl, Af, e);
 #pragma unroll
     for (int c = 0; c < E; ++c) {
       const int i = E * lane + c;
@@ -610,7 +698,8 @@ struct Sim : SimDyn<DY> {
       e[c] = i < n ? buf[i] : 0.f;
     }
     __syncwarp();
-    scan_regs<E>(pl, Ab, e);
+    if constexpr (E == 4) scan_regs4(pl, Ab, e);
+    else scan_regs<E>(pl, Ab, e);
 #pragma unroll
     for (int c = 0; c < E; ++c) {
       const int i = E * lane + c;
@@ -1164,8 +1253,8 @@ struct Sim : SimDyn<DY> {
       const float* inv = s.coef + (thick ? cl.thick_inv : cl.thin_inv);
       if (n <= 64) g += cg_filament<2>(base, n, Af, Ab, inv, alpha, beta, update, first, last, bad);
       else if (n <= 96) g += cg_filament<3>(base, n, Af, Ab, inv, alpha, beta, update, first, last, bad);
-      else if (n <= 128) g += cg_filament<4>(base, n, Af, Ab, inv, alpha, beta, update, first, last, bad);
-      else g += cg_filament<8>(base, n, Af, Ab, inv, alpha, beta, update, first, last, bad);
+      else if (!kWide || n <= 128) g += cg_filament<4>(base, n, Af, Ab, inv, alpha, beta, update, first, last, bad);
+      else if constexpr (kWide) g += cg_filament<8>(base, n, Af, Ab, inv, alpha, beta, update, first, last, bad);
     }
     __syncwarp();
     return g;
@@ -1594,15 +1683,11 @@ struct Sim : SimDyn<DY> {
   // probability tables (built when (pCa, d) differ from the cached key)
   // ------------------------------------------------------------------
   __device__ void build_tables(float pCa, float d, bool sampling, bool absorbing) {
-    build_tables_block(s.P, T.centers, T.n_bins, pCa, d, dtm, A.sq64_from, s.cum_tm,
-                       reinterpret_cast<float*>(ws + L.cum_xb), s.pabs, sampling, sampling,
-                       absorbing, nullptr, 0, tid, NT, A.pop, s.Pk, s.fk);
+    build_tables_block(s.tab, pCa, d, sampling, sampling, absorbing, nullptr, 0, tid, NT);
   }
   // the tropomyosin tables alone (they do not depend on the spacing)
   __device__ void build_tm_tables(float pCa) {
-    build_tables_block(s.P, T.centers, T.n_bins, pCa, 0.f, dtm, A.sq64_from, s.cum_tm,
-                       reinterpret_cast<float*>(ws + L.cum_xb), s.pabs, true, false, false, nullptr, 0,
-                       tid, NT, A.pop, s.Pk, s.fk);
+    build_tables_block(s.tab, pCa, 0.f, true, false, false, nullptr, 0, tid, NT);
   }
 
   // Dynamic spacing rebuilds the crossbridge tables every step.  Only the
@@ -1656,9 +1741,7 @@ struct Sim : SimDyn<DY> {
     }
     __syncthreads();
     const int nkeys = *count;
-    build_tables_block(s.P, T.centers, T.n_bins, pCa, d, dtm, A.sq64_from, s.cum_tm,
-                       reinterpret_cast<float*>(ws + L.cum_xb), s.pabs, false, !absorbing, absorbing, list,
-                       nkeys, tid, NT, A.pop, s.Pk, s.fk);
+    build_tables_block(s.tab, pCa, d, false, !absorbing, absorbing, list, nkeys, tid, NT);
     __syncthreads();
   }
 
