@@ -402,6 +402,14 @@ __device__ void metrics(Sim<NT, PR, DY>& m, int t, float zl, float pCa, float ne
     put(M_WORK_THICK_MEAN, work / (float)NTN);
     put(M_WORK_PER_ATP, r25 > 0.01f ? work / r25 : 0.0f);
   }
+  // the next step's pre-step snapshot: every read of this one (the partial
+  // sums above) ended at the barrier, and the step's closing barrier orders
+  // these copies before the next kinetics changes the state
+  for (int i = tid; i < NTN; i += NT) m.s.old_thick[i] = m.s.x[i];
+  for (int i = tid; i < X; i += NT) {
+    m.s.old_xbs[i] = m.s.xb_state[i];
+    m.s.old_key[i] = m.s.xb_key[i];
+  }
   MF_MT(5);
 #undef MF_MT
 }
@@ -650,11 +658,15 @@ __device__ void run_condition(const StepArgs& A, int ci) {
       }
       MF_PH(2);
       // old_state snapshot for the metrics (metrics_fn.py reads the pre-step
-      // geometry)
-      for (int i = m.tid; i < NTN; i += NT) m.s.old_thick[i] = m.s.x[i];
-      for (int i = m.tid; i < X; i += NT) {
-        m.s.old_xbs[i] = m.s.xb_state[i];
-        m.s.old_key[i] = m.s.xb_key[i];
+      // geometry): taken here at the first step of a launch, afterwards by the
+      // previous step's metrics epilogue
+      const bool first = t == (t0 > 0 ? t0 : 0);
+      if (first) {
+        for (int i = m.tid; i < NTN; i += NT) m.s.old_thick[i] = m.s.x[i];
+        for (int i = m.tid; i < X; i += NT) {
+          m.s.old_xbs[i] = m.s.xb_state[i];
+          m.s.old_key[i] = m.s.xb_key[i];
+        }
       }
       if (m.tid == 0) {
         if (!keys_ready) {
@@ -665,7 +677,9 @@ __device__ void run_condition(const StepArgs& A, int ci) {
         }
         keys_ready = 0;
       }
-      __syncthreads();
+      // the shifted thin positions (float32 mode) must be complete before the
+      // nearest-site staging reads them; the keys are read after its barriers
+      if (first || !m.precise) __syncthreads();
       MF_PH(3);
     }
     // 2-4. kinetics

@@ -838,38 +838,43 @@ struct Sim : SimDyn<DY> {
     __syncthreads();
     for (int g = tid; g < S; g += NT) cnt[g] = 0;
     __syncthreads();
-    int base = 0;
-    for (int c = 0; c < X; c += NT) {
-      const int i = c + tid;
-      bool f = false;
-      if (i < X) {
-        s.fxb[i] = 0.f;
-        const int st = s.xb_state[i];
-        const int bnd = s.xb_bound[i];
-        f = st >= 1 && st <= 3 && bnd >= 0;
-        int gs = -1;
-        if (f) {
-          gs = thin_of(i) * nsi + bnd;
-          const int k = atomicAdd(&cnt[gs], 1);
-          if (k < 2) site_h[2 * gs + k] = (int16_t)i;
-          else if (k == 2) status |= MF_MULTIBIND_BIT;
-        }
-        s.hsite[i] = gs;
+    // each thread takes a run of consecutive heads, so one block-wide scan of
+    // the per-thread counts places every head in increasing index order
+    const int per = (X + NT - 1) / NT, i0 = tid * per;
+    const int i1 = i0 + per < X ? i0 + per : X;
+    int nf = 0;
+    for (int i = i0; i < i1; ++i) {
+      s.fxb[i] = 0.f;
+      const int st = s.xb_state[i];
+      const int bnd = s.xb_bound[i];
+      const bool f = st >= 1 && st <= 3 && bnd >= 0;
+      int gs = -1;
+      if (f) {
+        gs = thin_of(i) * nsi + bnd;
+        const int k = atomicAdd(&cnt[gs], 1);
+        if (k < 2) site_h[2 * gs + k] = (int16_t)i;
+        else if (k == 2) status |= MF_MULTIBIND_BIT;
+        ++nf;
       }
-      const unsigned m = __ballot_sync(0xffffffffu, f);
-      if (lane == 0) s.wsum[warp] = __popc(m);
-      __syncthreads();
-      int off = base, tot = 0;
-      for (int w = 0; w < NW; ++w) {
-        const int v = s.wsum[w];
-        off += w < warp ? v : 0;
-        tot += v;
-      }
-      if (f) s.blist[off + __popc(m & ((1u << lane) - 1u))] = (int16_t)i;
-      base += tot;
-      __syncthreads();
+      s.hsite[i] = gs;
     }
-    if (tid == 0) *s.nbound = base;
+    int incl = nf;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane == 31) s.wsum[warp] = incl;
+    __syncthreads();
+    int off = incl - nf, tot = 0;
+    for (int w = 0; w < NW; ++w) {
+      const int v = s.wsum[w];
+      off += w < warp ? v : 0;
+      tot += v;
+    }
+    for (int i = i0; i < i1; ++i)
+      if (s.hsite[i] >= 0) s.blist[off++] = (int16_t)i;
+    if (tid == 0) *s.nbound = tot;
     // the two heads of a site in head order (their slots came from the
     // atomic counter; a contracted multiply-add of the second term is not
     // symmetric, so the sums over them need one fixed order)
