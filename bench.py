@@ -388,17 +388,17 @@ def _oracle_sample(args_tuple):
     return time.perf_counter() - t0
 
 
-def cpu_baseline(args, cores=1, n_cond=8, T=150):
+def cpu_baseline(args, cores=1, n_cond=8, T=150, pool=None):
     """The oracle (NumPy restatement of the reference timestep) on host cores:
-    n_cond conditions spread over the sweep's pCa range (its keys), T steps each."""
+    n_cond conditions spread over the sweep's pCa range (their keys), T steps
+    each.  With ``pool`` (worker processes already started and warmed) the
+    conditions run in parallel and only their work is timed."""
     os.environ.setdefault('OMP_NUM_THREADS', '1')
     idx = np.linspace(0, 255, n_cond).round().astype(int)
     jobs = [(2, 2, T, float(np.linspace(4.0, 7.0, 256)[i]), int(i)) for i in idx]
     t0 = time.perf_counter()
-    if cores > 1:
-        import multiprocessing as mp
-        with mp.get_context('spawn').Pool(cores) as pool:
-            pool.map(_oracle_sample, jobs)
+    if pool is not None:
+        pool.map(_oracle_sample, jobs, chunksize=1)
     else:
         for j in jobs:
             _oracle_sample(j)
@@ -409,16 +409,24 @@ def cpu_baseline(args, cores=1, n_cond=8, T=150):
 
 
 def bench_reference(args):
-    """--impl reference: the reference algorithm on the host CPU (JAX is not installable here)."""
+    """--impl reference: the reference algorithm on the host CPU (JAX is not installable here).
+
+    One worker process per host core, started and warmed before timing; each
+    timed step runs two conditions per core for 60 timesteps."""
     rank, world, local = _dist()
     if rank != 0:
         return
+    import multiprocessing as mp
+    os.environ.setdefault('OMP_NUM_THREADS', '1')
     cores = len(os.sched_getaffinity(0))
+    n_cond, T = 2 * cores, 60
     vals = []
-    for _ in range(args.warmup):
-        cpu_baseline(args, cores=cores, n_cond=cores, T=5)
-    for _ in range(args.steps):
-        vals.append(cpu_baseline(args, cores=cores, n_cond=cores, T=10)['value'])
+    with mp.get_context('spawn').Pool(cores) as pool:
+        pool.map(_oracle_sample, [(2, 2, 2, 4.5, 0)] * cores, chunksize=1)  # start and import in every worker
+        for _ in range(args.warmup):
+            cpu_baseline(args, cores=cores, n_cond=cores, T=5, pool=pool)
+        for _ in range(args.steps):
+            vals.append(cpu_baseline(args, cores=cores, n_cond=n_cond, T=T, pool=pool)['value'])
     v = float(np.mean(vals))
     print(json.dumps({
         'impl': 'reference', 'metric': METRIC, 'value': v, 'unit': METRIC, 'n_gpus': world,
@@ -426,9 +434,10 @@ def bench_reference(args):
         'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
         'config': {'workload': '256-condition pCa sweep, 2x2 skeletal lattice, 500 ms (sampled)',
                    'note': 'reference JAX path not installable (no jax wheel offline); its NumPy restatement '
-                           '(oracle) runs instead, one condition per host core'},
+                           '(oracle) runs instead, one worker process per host core'},
         'cpu_baseline': {'value': v, 'unit': METRIC, 'cores': cores, 'kind': 'port',
-                         'sample': f'{cores} conditions x 10 timesteps per step, 2x2 lattice'},
+                         'sample': f'{n_cond} conditions x {T} timesteps per step (each from its initial '
+                                   f'equilibrium), 2x2 lattice, pool started before timing'},
         'e2e': {'value': v, 'unit': METRIC, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
     }), flush=True)
 
