@@ -91,10 +91,29 @@ def test_ifm_mixed_precision_vs_fp64_oracle(engine):
     assert err <= 1e-5, err
 
 
-def test_ifm_dynamic_spacing_runs():
-    """Dynamic lattice spacing on the insect lattice: finite, spacing moves."""
+def test_ifm_dynamic_spacing_matches_oracle(engine):
+    """Dynamic lattice spacing on the insect lattice (float32, injected
+    uniforms): states identical to the oracle's, spacing and positions within
+    1e-5, over the Newton path shared with the oracle."""
+    from multifil_jax_b200.engine import MF_FLAG_DYNAMIC_LS
     topo, s, d = lattice('leth_2x2')
-    r = run(topo, duration_ms=15, pCa=4.5, z_line=1550.0, K_lat=5.0, nu=0.5, dynamic_params=d, static_params=s,
-            precision='mixed')
-    assert np.all(np.isfinite(r.axial_force)) and np.all(np.isfinite(r.lattice_spacing))
-    assert np.ptp(r.metrics['lattice_spacing']) > 0
+    T = 10
+    key = prng.split(prng.PRNGKey(6), 1)[0]
+    K = 5.0 * topo.n_thick
+    zt = 1550.0 + 0.5 * np.arange(T)
+    m_o, info = OS.run_condition(topo, d.param_row(), zt, np.full(T, 4.5), np.full(T, 14.0), key, K_lat=K, nu=0.5,
+                                 record_states=True)
+    ut = np.stack([u[0] for u in info['uniforms']])[None]
+    ux = np.stack([u[1] for u in info['uniforms']])[None]
+    res = run_engine(engine, topo, d.param_row()[None], zt[None], np.full((1, T), 4.5), np.full((1, T), 14.0),
+                     key[None], K_lat=[K], nu=[0.5], flags=MF_FLAG_DYNAMIC_LS, u_thin=ut, u_xb=ux, traces=True)
+    sdiv = state_divergence(res, 0, info, topo, T)
+    div = first_divergence(res['metrics'], m_o[None], KEYS)
+    win = min(v for v in (sdiv, div, T) if v is not None)
+    print(f'\nIFM dynamic spacing: window {win} of {T}')
+    assert win >= 5
+    ls_o, ls_g = m_o[4, :win], res['metrics'][0, 4, :win]
+    assert np.max(np.abs(ls_g - ls_o) / ls_o) < 1e-5
+    xo = oracle_positions(info, topo)[:win]
+    xg = res['x_trace'][0, :win, :topo.n_dof]
+    assert np.max(np.abs(xg - xo) / np.maximum(np.abs(xo), 10.0)) < 1e-5

@@ -74,3 +74,20 @@ def test_cancel_and_busy(engine):
         srv.cancel(ids[1])
         srv.drain()
         assert srv.poll(ids[0]) is not None and srv.poll(ids[2]) is not None
+
+
+def test_served_insect_lattice_equals_alone(engine):
+    """An insect flight muscle request (160-site thin filaments, four heads
+    per crown, 512-thread CTAs) served beside vertebrate ones equals it alone."""
+    from multifil_jax_b200 import get_lethocerus_params
+    s, d = get_lethocerus_params()
+    ifm = dict(topo=SarcTopology.create(2, 2, s, d), params=d, pCa=4.5, z=1550.0, dur=20.0,
+               key=prng.split(prng.PRNGKey(77), 1)[0])
+    reqs = _requests(3, seed=5) + [ifm]
+    with SimulationServer(mem_budget=256 << 20, chunk_steps=6, precision='mixed') as srv:
+        ids = [srv.submit(q['topo'], q['params'], q['pCa'], q['z'], q['dur'], q['key']) for q in reqs]
+        srv.drain()
+        for rid, q in zip(ids, reqs):
+            r = srv.poll(rid)
+            got = np.stack([r.metrics[k].astype(np.float32) for k in METRIC_KEYS])
+            assert np.array_equal(got, _alone(engine, q)), q['topo']
