@@ -447,10 +447,11 @@ def profile_case(args):
     import torch
     from multifil_jax_b200 import SarcTopology, get_skeletal_params
     from multifil_jax_b200.simulation import plan_batch
-    from multifil_jax_b200.engine import get_engine, MF_FLAG_PRECISE
+    from multifil_jax_b200.engine import get_engine, MF_FLAG_PRECISE, MF_FLAG_DYNAMIC_LS
     parts = [int(v) for v in args.profile_case.split(',')]
     B, T = parts[0], parts[1]
     n = parts[2] if len(parts) > 2 else 2
+    dyn = len(parts) > 3 and parts[3] != 0  # lattice spacing solved as an unknown (K_lat 5, nu 0.5)
     s, d = get_skeletal_params()
     topo = SarcTopology.create(n, n, s, d)
     plan = plan_batch(topo, duration_ms=T, pCa=list(np.linspace(4.0, 7.0, B)), dynamic_params=d, static_params=s)
@@ -460,10 +461,16 @@ def profile_case(args):
     keys = torch.as_tensor(plan.keys.astype(np.int64), device=dev).to(torch.int32)
     NS = torch.full((B,), T, dtype=torch.int32, device=dev)
     flags = MF_FLAG_PRECISE if args.precision == 'mixed' else 0
+    kw = {}
+    if dyn:
+        flags |= MF_FLAG_DYNAMIC_LS
+        kw = dict(K_lat=torch.full((B,), 5.0 * topo.n_thick, device=dev), nu=torch.full((B,), 0.5, device=dev))
     for _ in range(2):
-        out = eng.run_batch(topo, dv(plan.params), dv(plan.z), dv(plan.pCa), dv(plan.ls), NS, keys, flags=flags)
+        out = eng.run_batch(topo, dv(plan.params), dv(plan.z), dv(plan.pCa), dv(plan.ls), NS, keys, flags=flags,
+                            **kw)
     torch.cuda.synchronize()
-    print(json.dumps({'profile_case': [B, T, n], 'force_last_mean': float(out['metrics'][:, 0, -1].mean())}))
+    print(json.dumps({'profile_case': [B, T, n, int(dyn)],
+                      'force_last_mean': float(out['metrics'][:, 0, -1].mean())}))
 
 
 # ---------------------------------------------------------------------------
@@ -749,7 +756,8 @@ def main():
                     help='run one workload study instead of the bench line')
     ap.add_argument('--study-capacity-requests', type=int, default=2000)
     ap.add_argument('--profile-case', default=None,
-                    help='B,T[,lattice]: run the fused kernel once on B conditions x T steps (for ncu)')
+                    help='B,T[,lattice[,dyn]]: run the fused kernel once on B conditions x T steps (for ncu); '
+                         'dyn=1 solves the lattice spacing (K_lat 5 per thick filament, nu 0.5)')
     args = ap.parse_args()
     if args.study == 'uneven':
         study_uneven(args)

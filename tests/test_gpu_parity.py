@@ -15,7 +15,8 @@ KEYS = list(METRIC_KEYS)
 
 
 @pytest.mark.parametrize('nr,nc,T,pCa,z', [(1, 1, 30, 4.5, 900.0), (2, 2, 40, 4.5, 900.0),
-                                           (2, 2, 25, 6.0, 950.0), (3, 3, 12, 5.0, 1000.0)])
+                                           (2, 2, 25, 6.0, 950.0), (3, 3, 12, 5.0, 1000.0),
+                                           (5, 5, 12, 4.5, 900.0), (6, 6, 10, 5.5, 950.0)])
 def test_kernel_matches_oracle_per_step(engine, nr, nc, T, pCa, z):
     """Injected identical uniforms: integer states bit-identical, positions/forces within 1e-5."""
     s, d = get_skeletal_params()
@@ -161,14 +162,16 @@ def test_dynamic_lattice_spacing_matches_oracle(engine, nr, nc):
     assert not bad, bad
 
 
-@pytest.mark.parametrize('pCa', [4.5, 5.5, 6.5])
-def test_mixed_precision_force_error_vs_fp64_oracle(engine, pCa):
+@pytest.mark.parametrize('nr,nc,pCa,T', [(2, 2, 4.5, 200), (2, 2, 5.5, 200), (2, 2, 6.5, 200),
+                                         (5, 5, 5.0, 30), (6, 6, 4.5, 30)])
+def test_mixed_precision_force_error_vs_fp64_oracle(engine, nr, nc, pCa, T):
     """'mixed' precision: <= 1e-5 relative force error against the FP64 oracle
-    (same uniforms) over 200 steps; the states follow the oracle's throughout
-    unless a draw falls within 1e-5 of a table threshold."""
+    (same uniforms) over 200 steps at 2x2, and over 30 steps on the lattices
+    whose solver vectors live in the workspace (5x5, 6x6); the states follow
+    the oracle's throughout unless a draw falls within 1e-5 of a table
+    threshold."""
     s, d = get_skeletal_params()
-    topo = SarcTopology.create(2, 2, s, d)
-    T = 200
+    topo = SarcTopology.create(nr, nc, s, d)
     key = prng.split(prng.PRNGKey(0), 1)[0]
     zt, pt, lt = np.full(T, 900.0), np.full(T, pCa), np.full(T, 14.0)
     m32, info32 = OS.run_condition(topo, d.param_row(), zt, pt, lt, key)
