@@ -25,20 +25,33 @@ constexpr int kPair = 2;  // lanes per matrix
 
 // This lane's rows of C = A B, from its rows of A (a) and the rows of B held
 // by the pair (b): C[i][k] = A[i][0] B[0][k] + ... in increasing j, one fused
-// multiply-add per further term.
+// multiply-add per further term.  A lane already holds its own rows of B;
+// the partner's rows are swapped in once with an xor shuffle (R N values per
+// product, half of what a broadcast of every row moves: the shuffle unit
+// issues one warp instruction per clock per SM and bounds this code).  Done
+// in blocks of R columns so that only R x R swapped values are live.
 template <int N, class F>
-__device__ __forceinline__ void mm_pair(unsigned pmask, const F (&a)[N / 2][N], const F (&b)[N / 2][N],
+__device__ __forceinline__ void mm_pair(unsigned pmask, int h, const F (&a)[N / 2][N], const F (&b)[N / 2][N],
                                         F (&c)[N / 2][N]) {
   constexpr int R = N / 2;
 #pragma unroll
-  for (int j = 0; j < N; ++j) {
-    F bj[N];
+  for (int k0 = 0; k0 < N; k0 += R) {
+    F o[R][R];  // the partner's rows of B, columns k0 .. k0 + R - 1
 #pragma unroll
-    for (int k = 0; k < N; ++k) bj[k] = __shfl_sync(pmask, b[j % R][k], j / R, kPair);
+    for (int r = 0; r < R; ++r)
 #pragma unroll
-    for (int i = 0; i < R; ++i)
+      for (int kk = 0; kk < R; ++kk) o[r][kk] = __shfl_xor_sync(pmask, b[r][k0 + kk], 1, kPair);
 #pragma unroll
-      for (int k = 0; k < N; ++k) c[i][k] = j == 0 ? a[i][0] * bj[k] : fma(a[i][j], bj[k], c[i][k]);
+    for (int j = 0; j < N; ++j) {
+      const bool own = j / R == h;
+#pragma unroll
+      for (int kk = 0; kk < R; ++kk) {
+        const F bj = own ? b[j % R][k0 + kk] : o[j % R][kk];
+#pragma unroll
+        for (int i = 0; i < R; ++i)
+          c[i][k0 + kk] = j == 0 ? a[i][0] * bj : fma(a[i][j], bj, c[i][k0 + kk]);
+      }
+    }
   }
 }
 
@@ -83,15 +96,15 @@ __device__ int expm_pair(unsigned pmask, int h, float (&a)[N / 2][N], int sq64_f
   // V = b0 I + b2 A2 + b4 A4 + b6 A6 ;  U = A (b1 I + b3 A2 + b5 A4), in an
   // order that keeps at most four half-matrices live
   float a2[R][N], a4[R][N], t[R][N], u[R][N];
-  mm_pair<N>(pmask, a, a, a2);
-  mm_pair<N>(pmask, a2, a2, a4);
+  mm_pair<N>(pmask, h, a, a, a2);
+  mm_pair<N>(pmask, h, a2, a2, a4);
 #pragma unroll
   for (int i = 0; i < R; ++i)
 #pragma unroll
     for (int j = 0; j < N; ++j)
       t[i][j] = (j == h * R + i ? kPade6B[1] : 0.f) + kPade6B[3] * a2[i][j] + kPade6B[5] * a4[i][j];
-  mm_pair<N>(pmask, a, t, u);
-  mm_pair<N>(pmask, a4, a2, t);  // A6
+  mm_pair<N>(pmask, h, a, t, u);
+  mm_pair<N>(pmask, h, a4, a2, t);  // A6
   // Solve (V - U) X = (V + U) by LU with partial pivoting (the first row of
   // largest magnitude in the column is the pivot).  L reuses a2, R reuses a4.
 #pragma unroll
@@ -105,6 +118,10 @@ __device__ int expm_pair(unsigned pmask, int h, float (&a)[N / 2][N], int sq64_f
     }
   float (&L)[R][N] = a2;
   float (&Rm)[R][N] = a4;
+  // Rows k .. N-1 of the last R columns are lane 1's alone, so those steps
+  // (and the first R steps of the back substitution, lane 0's alone) need no
+  // shuffles; a pivot that stays on the diagonal (the usual case: the scaled
+  // V - U is close to I) needs one broadcast of the pivot row and no exchange.
 #pragma unroll
   for (int k = 0; k < N; ++k) {
     // pivot: largest |L[i][k]| over rows i >= k, lowest index on ties
@@ -117,29 +134,64 @@ __device__ int expm_pair(unsigned pmask, int h, float (&a)[N / 2][N], int sq64_f
       if (v != v) v = -1.f;
       if (gi >= k && v > best) { best = v; piv = gi; }
     }
-    const float ob = __shfl_xor_sync(pmask, best, 1, kPair);
-    const int op = __shfl_xor_sync(pmask, piv, 1, kPair);
-    if (ob > best || (ob == best && op < piv)) { best = ob; piv = op; }
+    if (k < R) {  // candidates in both lanes
+      const float ob = __shfl_xor_sync(pmask, best, 1, kPair);
+      const int op = __shfl_xor_sync(pmask, piv, 1, kPair);
+      if (ob > best || (ob == best && op < piv)) { best = ob; piv = op; }
+    }
     if (piv >= N) piv = k;
-    // exchange rows k and piv
-    float Lp[N], Rp[N], Lk[N], Rk[N];
-    fetch_row<N>(pmask, L, piv, Lp);
-    fetch_row<N>(pmask, Rm, piv, Rp);
+    // exchange rows k and piv; Lp, Rp: the pivot row
+    float Lp[N], Rp[N];
+    if (k >= R) {  // both rows are lane 1's (lane 0 has no row >= k and changes nothing)
+      const int li = piv % R;
 #pragma unroll
-    for (int j = 0; j < N; ++j) {
-      Lk[j] = __shfl_sync(pmask, L[k % R][j], k / R, kPair);
-      Rk[j] = __shfl_sync(pmask, Rm[k % R][j], k / R, kPair);
-    }
+      for (int j = 0; j < N; ++j) {
+        float vl = L[0][j], vr = Rm[0][j];
 #pragma unroll
-    for (int i = 0; i < R; ++i) {
-      if (h * R + i == piv) {
-#pragma unroll
-        for (int j = 0; j < N; ++j) { L[i][j] = Lk[j]; Rm[i][j] = Rk[j]; }
+        for (int i = 1; i < R; ++i) {
+          vl = li == i ? L[i][j] : vl;
+          vr = li == i ? Rm[i][j] : vr;
+        }
+        Lp[j] = vl;
+        Rp[j] = vr;
       }
-    }
-    if (h == k / R) {
+      if (h == k / R && piv != k) {
 #pragma unroll
-      for (int j = 0; j < N; ++j) { L[k % R][j] = Lp[j]; Rm[k % R][j] = Rp[j]; }
+        for (int i = 0; i < R; ++i) {
+          if (h * R + i == piv) {
+#pragma unroll
+            for (int j = 0; j < N; ++j) { L[i][j] = L[k % R][j]; Rm[i][j] = Rm[k % R][j]; }
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < N; ++j) { L[k % R][j] = Lp[j]; Rm[k % R][j] = Rp[j]; }
+      }
+    } else if (piv == k) {  // pair-uniform: row k stays, lane 0 broadcasts it
+#pragma unroll
+      for (int j = 0; j < N; ++j) {
+        Lp[j] = __shfl_sync(pmask, L[k % R][j], k / R, kPair);
+        Rp[j] = __shfl_sync(pmask, Rm[k % R][j], k / R, kPair);
+      }
+    } else {
+      float Lk[N], Rk[N];
+      fetch_row<N>(pmask, L, piv, Lp);
+      fetch_row<N>(pmask, Rm, piv, Rp);
+#pragma unroll
+      for (int j = 0; j < N; ++j) {
+        Lk[j] = __shfl_sync(pmask, L[k % R][j], k / R, kPair);
+        Rk[j] = __shfl_sync(pmask, Rm[k % R][j], k / R, kPair);
+      }
+#pragma unroll
+      for (int i = 0; i < R; ++i) {
+        if (h * R + i == piv) {
+#pragma unroll
+          for (int j = 0; j < N; ++j) { L[i][j] = Lk[j]; Rm[i][j] = Rk[j]; }
+        }
+      }
+      if (h == k / R) {
+#pragma unroll
+        for (int j = 0; j < N; ++j) { L[k % R][j] = Lp[j]; Rm[k % R][j] = Rp[j]; }
+      }
     }
     // eliminate below the pivot with the pivot row (now Lp, Rp)
 #pragma unroll
@@ -161,8 +213,13 @@ __device__ int expm_pair(unsigned pmask, int h, float (&a)[N / 2][N], int sq64_f
       for (int j = 0; j < N; ++j) a[g % R][j] = Rm[g % R][j] / L[g % R][g];
     }
     float xg[N];
+    if (g >= R) {  // lane 0's rows (all < g) need lane 1's row g
 #pragma unroll
-    for (int j = 0; j < N; ++j) xg[j] = __shfl_sync(pmask, a[g % R][j], g / R, kPair);
+      for (int j = 0; j < N; ++j) xg[j] = __shfl_sync(pmask, a[g % R][j], g / R, kPair);
+    } else {       // rows < g are lane 0's, which holds row g
+#pragma unroll
+      for (int j = 0; j < N; ++j) xg[j] = a[g % R][j];
+    }
 #pragma unroll
     for (int i = 0; i < R; ++i) {
       if (h * R + i < g) {
@@ -188,7 +245,7 @@ __device__ int expm_pair(unsigned pmask, int h, float (&a)[N / 2][N], int sq64_f
       for (int j = 0; j < N; ++j) D[i][j] = (double)a[i][j] / sum;
     }
     for (int q = 0; q < nsq; ++q) {
-      mm_pair<N>(pmask, D, D, E);
+      mm_pair<N>(pmask, h, D, D, E);
 #pragma unroll
       for (int i = 0; i < R; ++i)
 #pragma unroll
@@ -205,7 +262,7 @@ __device__ int expm_pair(unsigned pmask, int h, float (&a)[N / 2][N], int sq64_f
   } else {
     float c[R][N];
     for (int q = 0; q < nsq; ++q) {
-      mm_pair<N>(pmask, a, a, c);
+      mm_pair<N>(pmask, h, a, a, c);
 #pragma unroll
       for (int i = 0; i < R; ++i)
 #pragma unroll

@@ -518,6 +518,7 @@ __device__ void run_condition(const StepArgs& A, int ci) {
   // (pCa, d) of the sampling and absorbing tables in the workspace and the
   // initial z: read from shared memory every step, persisted at launch end
   __shared__ double tab_key[5];
+  __shared__ int samp_est;  // key count of the last sampling build (dynamic spacing)
   if (t0 == 0) {
     // ---- realize_state + initial equilibrium with the constants (A1) ----
     m.zref = (double)zt[0];
@@ -579,7 +580,10 @@ __device__ void run_condition(const StepArgs& A, int ci) {
   // the start of the step; otherwise thread 0 derives them there.
   __shared__ uint32_t sub_thin[2][2], sub_thick[2][2];
   __shared__ int keys_ready;
-  if (m.tid == 0) keys_ready = 0;
+  if (m.tid == 0) {
+    keys_ready = 0;
+    samp_est = A.pop.kx() * 2 * T.n_bins;
+  }
   // Drivers (z, pCa, ls) of step t in drv[t & 1].  Thread 0 copies those of
   // step t + 1 with cp.async during step t: their latency overlaps a whole
   // step, and no register holds them (or the driver pointers) across the
@@ -633,11 +637,17 @@ __device__ void run_condition(const StepArgs& A, int ci) {
       // probability tables for (pCa, d_kin); with a dynamic spacing the
       // crossbridge rows are built after the tropomyosin update instead
       if (DY && m.lazy_tab) {
+        // tab_key[1]: the spacing at which every sampling row was built
+        // (together with the absorbing rows of the step before), NaN when
+        // the rows are of mixed keys
         if ((double)pCa != tab_key[0]) {
           __syncthreads();
           m.build_tm_tables(pCa);
           __syncthreads();
-          if (m.tid == 0) tab_key[0] = pCa;
+          if (m.tid == 0) {
+            tab_key[0] = pCa;
+            tab_key[1] = NAN;
+          }
           __syncthreads();
         }
       } else if (!((double)pCa == tab_key[0] && (double)d_kin == tab_key[1])) {
@@ -701,7 +711,13 @@ __device__ void run_condition(const StepArgs& A, int ci) {
           keys_ready = 1;
         }
       });
-      if (DY && m.lazy_tab) m.build_needed_tables(pCa, d_kin, false);
+      if (DY && m.lazy_tab && !((double)d_kin == tab_key[1])) {
+        const int nk = m.build_needed_tables(pCa, d_kin, false);
+        if (m.tid == 0) {
+          samp_est = nk;
+          tab_key[1] = NAN;
+        }
+      }
       MF_PH(5);
       m.thick_step(sub_thick[t & 1], inj_x);
       MF_PH(6);
@@ -740,7 +756,12 @@ __device__ void run_condition(const StepArgs& A, int ci) {
     if (m.tid == 0) ls_s = new_ls;
     // absorbing table for the metrics at (pCa, new_ls)
     if (DY && m.lazy_tab) {
-      m.build_needed_tables(pCa, new_ls, true);
+      // with pCa unchanged at step t + 1 its sampling rows may be built here
+      if (m.tid == 0 && t + 1 < t1) cp_async_wait_all();  // step t + 1's drivers
+      __syncthreads();
+      const bool same_next = t + 1 < t1 && drv[(t + 1) & 1][1] == pCa;
+      const int all = m.build_needed_tables(pCa, new_ls, true, same_next, samp_est);
+      if (all && m.tid == 0) tab_key[1] = new_ls;
     } else if (!((double)pCa == tab_key[2] && (double)new_ls == tab_key[3])) {
       __syncthreads();
       m.build_tables(pCa, new_ls, false, true);

@@ -200,7 +200,12 @@ __host__ __device__ inline CoefLayout coef_layout(const TopoDev& t) {
 // spacing changes, and its Pade arithmetic would otherwise sit in the step
 // loop's code.  tm: the 27 tropomyosin tables; sampling / absorbing: the
 // crossbridge tables of every key, or with `keys` only the nkeys listed ones
-// (of the one kind selected).
+// (of the one kind selected), or with `keys` and both kinds selected every
+// sampling key followed by the listed absorbing keys.  Work goes to the
+// pairs in rounds of nt/2 matrices; every-key sampling work runs in
+// descending bin order (table_key_of_order): the far bins, whose stiff
+// generators take the most squarings, share the first round and the cheap
+// central bins the last one.
 //
 // Subpopulations (pop, with the K population rows Pk and fractions fk):
 // a blended family uses sum_k f_k Q_k, products and sums rounded one by one
@@ -215,6 +220,19 @@ static __device__ __forceinline__ void blend_acc(float (&acc)[R][C], const float
   for (int i = 0; i < R; ++i)
 #pragma unroll
     for (int j = 0; j < C; ++j) acc[i][j] = __fadd_rn(acc[i][j], __fmul_rn(f, q[i][j]));
+}
+
+// Bin-major order of the crossbridge table keys: ord = (bin * kx + population)
+// * 2 + permissiveness, and its inverse (key = population * 2 n_bins +
+// permissiveness * n_bins + bin).
+__device__ __forceinline__ int table_order_of_key(int key, int kx, int nb) {
+  const int nset = 2 * nb, pk = key / nset, k2 = key - pk * nset;
+  const int perm = k2 >= nb ? 1 : 0, bin = k2 - perm * nb;
+  return (bin * kx + pk) * 2 + perm;
+}
+__device__ __forceinline__ int table_key_of_order(int ord, int kx, int nb) {
+  const int perm = ord & 1, q = ord >> 1, pk = q % kx, bin = q / kx;
+  return pk * 2 * nb + perm * nb + bin;
 }
 
 static __device__ __noinline__ void build_tables_block(const TableCtx& c, float pCa, float d, bool tm, bool sampling,
@@ -261,11 +279,23 @@ static __device__ __noinline__ void build_tables_block(const TableCtx& c, float 
     }
   }
   const int kx = pop.kx(), nset = 2 * nb;  // keys of one population's set
+  const int nall = kx * nset;
   const bool blend = pop.blend_xb();
-  const int nwork = keys ? nkeys : (sampling ? kx * nset : 0) + (absorbing ? kx * nset : 0);
+  const bool all_then_list = keys && sampling && absorbing;
+  const int nwork = keys ? nkeys + (all_then_list ? nall : 0) : (sampling ? nall : 0) + (absorbing ? nall : 0);
   for (int w = pair; w < nwork; w += npairs) {
-    const bool is_abs = keys ? absorbing : (!sampling || w >= kx * nset);
-    const int key = keys ? (int)keys[w] : (is_abs && sampling ? w - kx * nset : w);
+    bool is_abs;
+    int key;
+    if (all_then_list) {
+      is_abs = w >= nall;
+      key = is_abs ? (int)keys[w - nall] : table_key_of_order(nall - 1 - w, kx, nb);
+    } else if (keys) {
+      is_abs = absorbing;
+      key = keys[w];
+    } else {
+      is_abs = !sampling || w >= nall;
+      key = is_abs && sampling ? w - nall : w;
+    }
     const int pk = key / nset, k2 = key - pk * nset;
     const int bin = k2 % nb;
     const float perm = k2 >= nb ? 1.0f : 0.0f;
@@ -1698,14 +1728,26 @@ struct Sim : SimDyn<DY> {
   // Dynamic spacing rebuilds the crossbridge tables every step.  Only the
   // rows some head reads are built: the sampling keys of all heads (after
   // the tropomyosin update, thick_step's keys) or the absorbing keys of the
-  // heads the metrics read (old state 2 or 3).  Flags and the sorted key list
-  // live in the CG vector pv, which is free outside the solve.
+  // heads the metrics read (old state 2 or 3).  Flags and the key list
+  // live in the CG vector pv, which is free outside the solve; the flags are
+  // indexed in bin-major order and the list runs from the highest bin down
+  // (the stiff far bins first, the cheap central ones in the last round).
+  //
+  // The absorbing rows of step t and the sampling rows of step t + 1 have
+  // the same spacing (the one step t solved for) and, with pCa unchanged,
+  // the same key: with merge_ok the absorbing build also builds every
+  // sampling row when that takes fewer rounds of npairs matrices than the
+  // absorbing rows now plus the sampling rows of the next step (estimated by
+  // samp_est, the key count of the last sampling build).  Returns the key
+  // count of a sampling build, or for an absorbing build 1 if every sampling
+  // row was built with it, else 0.
   __device__ bool lazy_tables_fit() const {
     const int nk = A.pop.kx() * 2 * T.n_bins, nwords = (nk + 31) >> 5;
     return 4 * (nwords + 1) + 2 * nk <= 4 * T.n_dof;
   }
-  __device__ void build_needed_tables(float pCa, float d, bool absorbing) {
-    const int nk = A.pop.kx() * 2 * T.n_bins, nwords = (nk + 31) >> 5, X = T.total_xbs;
+  __device__ int build_needed_tables(float pCa, float d, bool absorbing, bool merge_ok = false, int samp_est = 0) {
+    const int kx = A.pop.kx(), nb = T.n_bins;
+    const int nk = kx * 2 * nb, nwords = (nk + 31) >> 5, X = T.total_xbs;
     uint32_t* bits = reinterpret_cast<uint32_t*>(s.pv);
     int* count = reinterpret_cast<int*>(bits + nwords);
     int16_t* list = reinterpret_cast<int16_t*>(count + 1);
@@ -1720,14 +1762,17 @@ struct Sim : SimDyn<DY> {
         const int so = s.old_xbs[i];
         if (so == 2 || so == 3) key = s.old_key[i];
       }
-      if (key >= 0) atomicOr(&bits[key >> 5], 1u << (key & 31));
+      if (key >= 0) {
+        const int o = table_order_of_key(key, kx, nb);
+        atomicOr(&bits[o >> 5], 1u << (o & 31));
+      }
     }
     __syncthreads();
     if (warp == 0) {
       int base = 0;
       for (int c = 0; c < nwords; c += 32) {
-        const int wi = c + lane;
-        uint32_t wb = wi < nwords ? bits[wi] : 0u;
+        const int wi = nwords - 1 - (c + lane);  // lane 0 takes the highest word
+        uint32_t wb = wi >= 0 ? bits[wi] : 0u;
         const int n = __popc(wb);
         int incl = n;
 #pragma unroll
@@ -1737,8 +1782,9 @@ struct Sim : SimDyn<DY> {
         }
         int off = base + incl - n;
         while (wb) {
-          list[off++] = (int16_t)(wi * 32 + __ffs(wb) - 1);
-          wb &= wb - 1u;
+          const int bit = 31 - __clz(wb);
+          list[off++] = (int16_t)table_key_of_order(wi * 32 + bit, kx, nb);
+          wb &= ~(1u << bit);
         }
         base += __shfl_sync(0xffffffffu, incl, 31);
       }
@@ -1746,8 +1792,12 @@ struct Sim : SimDyn<DY> {
     }
     __syncthreads();
     const int nkeys = *count;
-    build_tables_block(s.tab, pCa, d, false, !absorbing, absorbing, list, nkeys, tid, NT);
+    constexpr int npairs = NT / 2;
+    auto rounds = [](int n) { return (n + npairs - 1) / npairs; };
+    const bool merge = absorbing && merge_ok && rounds(nk + nkeys) < rounds(nkeys) + rounds(samp_est);
+    build_tables_block(s.tab, pCa, d, false, !absorbing || merge, absorbing, list, nkeys, tid, NT);
     __syncthreads();
+    return absorbing ? (merge ? 1 : 0) : nkeys;
   }
 
   // ------------------------------------------------------------------
