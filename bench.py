@@ -283,7 +283,9 @@ def bench_gpu(args):
                                       'float64 expm squaring (<=1e-5 force error vs the FP64 oracle); '
                                       'float32 = the reference\'s single-precision arithmetic'},
         'e2e': {'value': e2e_value, 'unit': METRIC, 'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': int(d2h),
-                'warmup_calls': E2E_WARMUP},
+                'warmup_calls': E2E_WARMUP,
+                'd2h_path': 'the kernel writes the metrics into page-locked host memory over the bus '
+                            '(inside the launch, no copy after it)'},
         'gpu_launches': args.steps,
         'roofline': {'bound': 'fp32', 'achieved': achieved_tf, 'peak': fp32_peak, 'unit': 'TFLOP/s',
                      'frac': achieved_tf / fp32_peak,

@@ -110,7 +110,10 @@ typedef struct {
     int32_t flags;          /* MF_FLAG_* */
     int32_t chunk_steps;    /* steps per launch in the batched path (0 = all) */
     float residual_warn;    /* StaticParams.solver_residual_tol (status bit only) */
-    float* metrics_out;     /* [B*52*T_max] device */
+    float* metrics_out;     /* [B*52*T_max] device, or page-locked host memory mapped at the
+                               same address (cudaHostAlloc under unified addressing): the
+                               kernels then write the metrics over the bus and no copy
+                               follows; pageable memory is refused (MF_ERR_INVALID) */
     int32_t* status_out;    /* [B] device */
     uint32_t* keys_out;     /* [B*2] device or NULL: key after the last step */
     /* test hooks (NULL in production) */

@@ -79,6 +79,25 @@ static int fail(mf_ctx* c, int code, const char* fmt, ...) {
   return code;
 }
 
+// Whether the kernels can store through p: device or managed memory, or
+// page-locked host memory mapped into the device address space at the same
+// address (cudaHostAlloc under unified addressing; the kernel then writes
+// over the bus and no copy is needed).  Pageable host memory is rejected.
+static int check_kernel_ptr(mf_ctx* ctx, const void* p, const char* name) {
+  cudaPointerAttributes a{};
+  const cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    return fail(ctx, MF_ERR_INVALID, "%s: not a CUDA-accessible pointer (%s)", name, cudaGetErrorString(e));
+  }
+  if (a.type == cudaMemoryTypeUnregistered)
+    return fail(ctx, MF_ERR_INVALID, "%s: pageable host memory (the kernels need device or page-locked memory)",
+                name);
+  if (a.type == cudaMemoryTypeHost && a.devicePointer != p)
+    return fail(ctx, MF_ERR_INVALID, "%s: page-locked memory not mapped at the same device address", name);
+  return MF_OK;
+}
+
 #define CK(call)                                                                        \
   do {                                                                                  \
     cudaError_t e_ = (call);                                                            \
@@ -472,6 +491,7 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
   int rc = batch_pops(ctx, bt, ps);
   if (rc) return rc;
   CK(cudaSetDevice(ctx->device));
+  if ((rc = check_kernel_ptr(ctx, bt->metrics_out, "metrics_out"))) return rc;
   cudaStream_t st = (cudaStream_t)stream_v;
   const int B = bt->B;
   // group conditions by CTA configuration; one launch per group
@@ -794,6 +814,10 @@ int mf_run_batch_static(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
     if (prc) return prc;
   }
   CK(cudaSetDevice(ctx->device));
+  {
+    const int prc = check_kernel_ptr(ctx, bt->metrics_out, "metrics_out");
+    if (prc) return prc;
+  }
   // one-time set-up on this device, with the device current
   const int dev = ctx->device;
   std::call_once(g_static_once[dev], [dev]() {

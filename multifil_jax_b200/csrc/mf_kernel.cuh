@@ -716,6 +716,10 @@ __device__ void run_condition(const StepArgs& A, int ci) {
         if (m.tid == 0) {
           samp_est = nk;
           tab_key[1] = NAN;
+#ifdef MF_PHASE_TIMING
+          m.sub_acc[5] += 1.0;  // sampling builds
+          m.sub_acc[7] += nk;   // their keys
+#endif
         }
       }
       MF_PH(5);
@@ -761,7 +765,12 @@ __device__ void run_condition(const StepArgs& A, int ci) {
       __syncthreads();
       const bool same_next = t + 1 < t1 && drv[(t + 1) & 1][1] == pCa;
       const int all = m.build_needed_tables(pCa, new_ls, true, same_next, samp_est);
-      if (all && m.tid == 0) tab_key[1] = new_ls;
+      if (all && m.tid == 0) {
+        tab_key[1] = new_ls;
+#ifdef MF_PHASE_TIMING
+        m.sub_acc[6] += 1.0;  // absorbing builds that built every sampling row too
+#endif
+      }
     } else if (!((double)pCa == tab_key[2] && (double)new_ls == tab_key[3])) {
       __syncthreads();
       m.build_tables(pCa, new_ls, false, true);

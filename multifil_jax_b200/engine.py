@@ -292,7 +292,7 @@ class Engine:
     def run_batch(self, topos, params, z, pCa, ls, n_steps, keys, K_lat=None, nu=None, dt=None,
                   n_newton=4, n_cg=6, flags=0, chunk_steps=0, residual_warn=1.5, stream=None,
                   u_thin=None, u_xb=None, want_x_trace=False, want_state_trace=False, keys_out=None,
-                  pops=None):
+                  pops=None, metrics_out=None):
         """Run B conditions through the fused kernel; every array is a torch CUDA tensor.
 
         ``topos`` is a list of B SarcTopology objects (or one shared).  Returns
@@ -318,7 +318,13 @@ class Engine:
             assert a.is_cuda and a.dtype == torch.float32 and a.is_contiguous()
             return a
 
-        metrics = torch.empty((B, N_METRICS, T), dtype=torch.float32, device=dev)
+        if metrics_out is None:
+            metrics = torch.empty((B, N_METRICS, T), dtype=torch.float32, device=dev)
+        else:  # device memory, or page-locked host memory the kernel writes over the bus
+            assert metrics_out.dtype == torch.float32 and metrics_out.is_contiguous()
+            assert tuple(metrics_out.shape) == (B, N_METRICS, T)
+            assert metrics_out.is_cuda or metrics_out.is_pinned()
+            metrics = metrics_out
         status = torch.zeros(B, dtype=torch.int32, device=dev)
         out = dict(metrics=metrics, status=status)
         xt = st = bt = None
@@ -432,41 +438,36 @@ def device_pops(sp, dev):
     return out
 
 
-def to_host(t):
-    """Copy a device tensor into page-locked host memory and return it as numpy.
-
-    The blocks come from torch's caching host allocator: a loop of calls that
-    drops each result before the next reuses the same blocks, so the copy
-    runs at full DMA speed and no fresh pages are faulted in (about 8 ms for
-    a 26 MB result when the destination is new pageable memory).
-    """
+def host_metrics(B: int, T: int):
+    """A page-locked host block for [B, 52, T] metrics that the kernels write
+    over the bus (``Engine.run_batch(metrics_out=...)``): the launch leaves
+    the result on the host, with no device buffer and no copy after it.
+    Blocks come from torch's caching host allocator, so a loop of calls that
+    drops each result before the next reuses the same pages."""
     torch = _torch()
-    h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
-    h.copy_(t, non_blocking=True)
-    torch.cuda.current_stream(t.device).synchronize()
-    return h.numpy()
+    return torch.empty((B, N_METRICS, T), dtype=torch.float32, pin_memory=True)
 
 
 def execute_plan(topology, plan, static_params, precision: str = 'float32', device: Optional[int] = None,
                  minibatch_size="auto", chunk_steps: int = 0, stream=None, key_major: bool = False,
                  status_out: Optional[np.ndarray] = None) -> np.ndarray:
     """Run every condition of a BatchPlan on the GPU; returns host metrics [B, 52, T]
-    (``key_major``: [52, B, T], transposed on the device so that every metric is
-    one contiguous block on the host).  ``status_out`` (int32 [B]) receives
-    every condition's MF_STATUS_* bits."""
+    (``key_major``: a [52, B, T] view of the same block, one metric per leading
+    index).  The kernels write the metrics straight into page-locked host
+    memory.  ``status_out`` (int32 [B]) receives every condition's MF_STATUS_*
+    bits."""
     torch = _torch()
     eng = get_engine(device)
     dev = torch.device('cuda', eng.device)
     B, T = plan.total, plan.n_steps
-    shape = (N_METRICS, B, T) if key_major else (B, N_METRICS, T)
     if B == 0 or T == 0:
-        return np.zeros(shape, dtype=np.float32)
+        return np.zeros((N_METRICS, B, T) if key_major else (B, N_METRICS, T), dtype=np.float32)
     if minibatch_size in (None, "auto"):
         chunk = B
     else:
         chunk = max(1, int(minibatch_size))
     flags = _flags_for(plan, precision)
-    out = None if chunk >= B else torch.empty(shape, dtype=torch.float32, pin_memory=True)
+    out = host_metrics(B, T)
     with torch.cuda.device(dev):
         for s in range(0, B, chunk):
             e = min(B, s + chunk)
@@ -482,15 +483,10 @@ def execute_plan(topology, plan, static_params, precision: str = 'float32', devi
                                 dt=torch.full((n,), plan.dt, dtype=torch.float32, device=dev),
                                 n_newton=static_params.n_newton_steps, n_cg=static_params.n_cg_steps,
                                 flags=flags, chunk_steps=chunk_steps,
-                                residual_warn=static_params.solver_residual_tol, stream=stream, pops=pops)
-            m = res['metrics'].permute(1, 0, 2).contiguous() if key_major else res['metrics']
+                                residual_warn=static_params.solver_residual_tol, stream=stream, pops=pops,
+                                metrics_out=out[s:e])
             if status_out is not None:
                 status_out[s:e] = res['status'].cpu().numpy()
-            if out is None:
-                return to_host(m)
-            if key_major:
-                out[:, s:e].copy_(m)
-            else:
-                out[s:e].copy_(m, non_blocking=True)
-        torch.cuda.current_stream(dev).synchronize()
-    return out.numpy()
+        (stream if stream is not None else torch.cuda.current_stream(dev)).synchronize()
+    m = out.numpy()
+    return m.transpose(1, 0, 2) if key_major else m

@@ -377,7 +377,7 @@ def run_conditions(conditions: List[dict], *, static_params: Optional[StaticPara
     eng = get_engine(device)
     dev = torch.device('cuda', eng.device)
     flags = (MF_FLAG_DYNAMIC_LS if all(dyn) else 0) | (MF_FLAG_PRECISE if precision == 'mixed' else 0)
-    from .engine import upload, to_host
+    from .engine import upload, host_metrics
     if autotune:
         from .autotune import autotune_many, choose_batch_sizes
         picks = autotune_many(topos, precision=precision, device=device, dynamic_ls=all(dyn))
@@ -398,10 +398,12 @@ def run_conditions(conditions: List[dict], *, static_params: Optional[StaticPara
     with torch.cuda.device(dev):
         dP, dZ, dPC, dL, dN, dKY, dK, dNU, dDT = upload(dev, P, Z, PC, L, np.asarray(steps, np.int32),
                                                         KEYS.view(np.int32), K, NU, DT)
-        res = eng.run_batch(topos, dP, dZ, dPC, dL, dN, dKY, K_lat=dK, nu=dNU, dt=dDT,
-                            n_newton=sp.n_newton_steps, n_cg=sp.n_cg_steps, flags=flags, chunk_steps=chunk_steps,
-                            residual_warn=sp.solver_residual_tol)
-        m = to_host(res['metrics'])
+        hm = host_metrics(len(conditions), T)  # written by the kernels over the bus
+        eng.run_batch(topos, dP, dZ, dPC, dL, dN, dKY, K_lat=dK, nu=dNU, dt=dDT,
+                      n_newton=sp.n_newton_steps, n_cg=sp.n_cg_steps, flags=flags, chunk_steps=chunk_steps,
+                      residual_warn=sp.solver_residual_tol, metrics_out=hm)
+        torch.cuda.current_stream(dev).synchronize()
+        m = hm.numpy()
     out = []
     for i, n in enumerate(steps):
         md = MetricsDict()
