@@ -374,8 +374,18 @@ class Engine:
                     setattr(bat, name, lab.data_ptr())
             bat.label_stride = int(stride)
         s = stream if stream is not None else torch.cuda.current_stream(dev)
-        self._check(self.lib.mf_run_batch(self.h, ctypes.byref(bat), ctypes.c_void_p(s.cuda_stream)),
-                    'mf_run_batch')
+        rc = self.lib.mf_run_batch(self.h, ctypes.byref(bat), ctypes.c_void_p(s.cuda_stream))
+        if rc == MF_ERR_INVALID and not metrics.is_cuda and b'not mapped' in (self.lib.mf_last_error(self.h) or b''):
+            # page-locked memory the device cannot address at the same pointer
+            # (a host allocator that registers pages without mapping them):
+            # run into device memory and copy, as for any other caller
+            dm = torch.empty((B, N_METRICS, T), dtype=torch.float32, device=dev)
+            bat.metrics_out = dm.data_ptr()
+            rc = self.lib.mf_run_batch(self.h, ctypes.byref(bat), ctypes.c_void_p(s.cuda_stream))
+            if rc == 0:
+                with torch.cuda.stream(s):
+                    metrics.copy_(dm, non_blocking=True)
+        self._check(rc, 'mf_run_batch')
         return out
 
 
