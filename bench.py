@@ -221,8 +221,9 @@ def bench_gpu(args):
             e2e_times.append(t1 - t0)
     t_e2e = _max_over_ranks(float(np.sum(e2e_times)), world, dev)
     e2e_value = B * T * len(e2e_times) * world / t_e2e
-    h2d = plan.params.nbytes + plan.z.nbytes + plan.pCa.nbytes + plan.ls.nbytes + plan.keys.nbytes + \
-        plan.K_lat.nbytes + plan.nu.nbytes + 2 * 4 * B
+    # drivers constant in time go up as one value per condition (MF_FLAG_CONST_DRIVERS)
+    drv_bytes = 3 * 4 * B if plan.const_drivers else plan.z.nbytes + plan.pCa.nbytes + plan.ls.nbytes
+    h2d = plan.params.nbytes + drv_bytes + plan.keys.nbytes + plan.K_lat.nbytes + plan.nu.nbytes + 2 * 4 * B
     d2h = B * 52 * T * 4
 
     # plain: one condition per launch, one launch per timestep, on a subset

@@ -56,6 +56,8 @@ extern "C" {
 #define MF_FLAG_ORIGINAL_PRNG 4    /* pre-0.5 jax.random counter layout */
 #define MF_FLAG_PLAIN 8            /* one condition per launch, one launch per step */
 #define MF_FLAG_NO_GRAPH 16        /* batched path without CUDA-graph capture */
+#define MF_FLAG_CONST_DRIVERS 32   /* z, pCa and ls are [B]: one value per condition for every
+                                      step (a scalar sweep), instead of [B*T_max] traces */
 
 #define MF_N_PARAMS 44
 #define MF_N_METRICS 52
@@ -97,9 +99,9 @@ typedef struct {
     int32_t T_max;          /* row stride of the per-step arrays */
     const int32_t* topo_id; /* [B] host: lattice of each condition (mf_upload_topology ids) */
     const float* params;    /* [B*44] device: DynamicParams rows, reference field order */
-    const float* z;         /* [B*T_max] device: z_line trace */
-    const float* pCa;       /* [B*T_max] device */
-    const float* ls;        /* [B*T_max] device: lattice_spacing trace (driver / d_ref basis) */
+    const float* z;         /* [B*T_max] device: z_line trace ([B] with MF_FLAG_CONST_DRIVERS) */
+    const float* pCa;       /* [B*T_max] device (same) */
+    const float* ls;        /* [B*T_max] device: lattice_spacing trace, driver / d_ref basis (same) */
     const int32_t* n_steps; /* [B] device: steps of each condition (<= T_max) */
     const uint32_t* keys;   /* [B*2] device: jax.random key of each condition */
     const float* K_lat;     /* [B] device: lattice stiffness already x n_thick (dynamic LS) */

@@ -543,9 +543,11 @@ int mf_run_batch(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
     hc[k].t0 = 0;
     hc[k].t1 = n_steps[i];
     hc[k].params = bt->params + (size_t)i * MF_N_PARAMS;
-    hc[k].z = bt->z + (size_t)i * bt->T_max;
-    hc[k].pCa = bt->pCa + (size_t)i * bt->T_max;
-    hc[k].ls = bt->ls + (size_t)i * bt->T_max;
+    const size_t dstride = (bt->flags & MF_FLAG_CONST_DRIVERS) ? 1 : (size_t)bt->T_max;
+    hc[k].drv_const = (bt->flags & MF_FLAG_CONST_DRIVERS) ? 1 : 0;
+    hc[k].z = bt->z + (size_t)i * dstride;
+    hc[k].pCa = bt->pCa + (size_t)i * dstride;
+    hc[k].ls = bt->ls + (size_t)i * dstride;
     hc[k].key = bt->keys + 2 * (size_t)i;
     hc[k].metrics = bt->metrics_out + (size_t)i * MF_N_METRICS * bt->T_max;
     hc[k].status = bt->status_out ? bt->status_out + i : nullptr;
@@ -884,9 +886,11 @@ int mf_run_batch_static(mf_ctx* ctx, const mf_batch* bt, void* stream_v) {
     c.t0 = 0;
     c.t1 = n_steps[i];
     c.params = bt->params + (size_t)i * MF_N_PARAMS;
-    c.z = bt->z + (size_t)i * bt->T_max;
-    c.pCa = bt->pCa + (size_t)i * bt->T_max;
-    c.ls = bt->ls + (size_t)i * bt->T_max;
+    const size_t dstride = (bt->flags & MF_FLAG_CONST_DRIVERS) ? 1 : (size_t)bt->T_max;
+    c.drv_const = (bt->flags & MF_FLAG_CONST_DRIVERS) ? 1 : 0;
+    c.z = bt->z + (size_t)i * dstride;
+    c.pCa = bt->pCa + (size_t)i * dstride;
+    c.ls = bt->ls + (size_t)i * dstride;
     c.key = bt->keys + 2 * (size_t)i;
     c.metrics = bt->metrics_out + (size_t)i * MF_N_METRICS * bt->T_max;
     c.status = bt->status_out ? bt->status_out + i : nullptr;

@@ -507,6 +507,7 @@ __device__ void run_condition(const StepArgs& A, int ci) {
   const float* zt = cd.z;
   const float* pt = cd.pCa;
   const float* lt = cd.ls;
+  const int ds = cd.drv_const ? 0 : 1;  // driver index step per timestep
   const int n_steps = cd.n_steps;
   const int t0 = cd.t0;
   const int t1 = cd.t1 < n_steps ? cd.t1 : n_steps;
@@ -592,11 +593,11 @@ __device__ void run_condition(const StepArgs& A, int ci) {
   __shared__ float prev_z_s;
   if (m.tid == 0) {
     if (t0 < t1) {
-      drv[t0 & 1][0] = zt[t0];
-      drv[t0 & 1][1] = pt[t0];
-      drv[t0 & 1][2] = lt[t0];
+      drv[t0 & 1][0] = zt[t0 * ds];
+      drv[t0 & 1][1] = pt[t0 * ds];
+      drv[t0 & 1][2] = lt[t0 * ds];
     }
-    prev_z_s = t0 > 0 ? zt[t0 - 1] : 0.0f;
+    prev_z_s = t0 > 0 ? zt[(t0 - 1) * ds] : 0.0f;
   }
   __syncthreads();
   // t = -1: the initial equilibrium with the constants (A1): nearest sites
@@ -615,9 +616,9 @@ __device__ void run_condition(const StepArgs& A, int ci) {
       const float dz = t > 0 ? zl - prev_z_s : 0.0f;
       if (m.tid == 0 && t + 1 < t1) {
         float* nx = drv[(t + 1) & 1];
-        cp_async4(nx + 0, cd.z + t + 1);
-        cp_async4(nx + 1, cd.pCa + t + 1);
-        cp_async4(nx + 2, cd.ls + t + 1);
+        cp_async4(nx + 0, cd.z + (t + 1) * ds);
+        cp_async4(nx + 1, cd.pCa + (t + 1) * ds);
+        cp_async4(nx + 2, cd.ls + (t + 1) * ds);
       }
       // 1. rigid shift of the thin filaments
       if (!m.precise) {

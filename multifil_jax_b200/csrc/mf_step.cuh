@@ -28,10 +28,11 @@ struct CondDesc {
   int index;              // row in the caller's arrays (test hooks)
   int t0, t1;             // step range of this launch
   int T;                  // stride of z/pCa/ls/metrics rows
+  int drv_const;          // 1: z/pCa/ls hold one value for every step (zero: per-step traces)
   const float* params;    // [44]
-  const float* z;         // [T]
-  const float* pCa;       // [T]
-  const float* ls;        // [T]
+  const float* z;         // [T], or [1] with drv_const
+  const float* pCa;       // [T], or [1] with drv_const
+  const float* ls;        // [T], or [1] with drv_const
   const uint32_t* key;    // [2] key at step 0
   float* metrics;         // [52*T]
   int* status;            // or NULL

@@ -23,6 +23,7 @@ MF_FLAG_PRECISE = 2
 MF_FLAG_ORIGINAL_PRNG = 4
 MF_FLAG_PLAIN = 8
 MF_FLAG_NO_GRAPH = 16
+MF_FLAG_CONST_DRIVERS = 32
 
 MF_POP_EXPLICIT = 1
 MF_POP_XB = 2
@@ -292,11 +293,13 @@ class Engine:
     def run_batch(self, topos, params, z, pCa, ls, n_steps, keys, K_lat=None, nu=None, dt=None,
                   n_newton=4, n_cg=6, flags=0, chunk_steps=0, residual_warn=1.5, stream=None,
                   u_thin=None, u_xb=None, want_x_trace=False, want_state_trace=False, keys_out=None,
-                  pops=None, metrics_out=None):
+                  pops=None, metrics_out=None, n_time=None):
         """Run B conditions through the fused kernel; every array is a torch CUDA tensor.
 
         ``topos`` is a list of B SarcTopology objects (or one shared).  Returns
         a dict with ``metrics`` [B, 52, T], ``status`` [B] and optional traces.
+        ``z``, ``pCa``, ``ls`` are [B, T] traces, or [B] values held for every
+        step (then ``n_time`` gives T; MF_FLAG_CONST_DRIVERS).
         ``pops``: subpopulations as a dict ``K``, ``flags`` (MF_POP_*),
         ``rows`` [B, K, 44] float32, ``fractions`` [B, K] float32 and, for
         explicit populations, ``xb_label`` / ``tm_label`` [B, stride] int8
@@ -304,7 +307,12 @@ class Engine:
         """
         torch = _torch()
         dev = torch.device('cuda', self.device)
-        B, T = z.shape
+        if z.dim() == 1:
+            assert pCa.dim() == 1 and ls.dim() == 1 and n_time is not None
+            B, T = z.shape[0], int(n_time)
+            flags = int(flags) | MF_FLAG_CONST_DRIVERS
+        else:
+            B, T = z.shape
         if not isinstance(topos, (list, tuple)):
             topos = [topos] * B
         by_obj = {}  # one lookup per distinct lattice object, not per condition
@@ -483,7 +491,9 @@ def execute_plan(topology, plan, static_params, precision: str = 'float32', devi
             e = min(B, s + chunk)
             n = e - s
 
-            P, Z, PC, L, K, KL, NU = upload(dev, plan.params[s:e], plan.z[s:e], plan.pCa[s:e], plan.ls[s:e],
+            drv = (plan.z[s:e, 0], plan.pCa[s:e, 0], plan.ls[s:e, 0]) if plan.const_drivers else \
+                (plan.z[s:e], plan.pCa[s:e], plan.ls[s:e])
+            P, Z, PC, L, K, KL, NU = upload(dev, plan.params[s:e], *drv,
                                             plan.keys[s:e].astype(np.uint32).view(np.int32), plan.K_lat[s:e],
                                             plan.nu[s:e])
             pops = device_pops(plan.subpop.take(s, e), dev) if plan.subpop is not None else None
@@ -494,7 +504,7 @@ def execute_plan(topology, plan, static_params, precision: str = 'float32', devi
                                 n_newton=static_params.n_newton_steps, n_cg=static_params.n_cg_steps,
                                 flags=flags, chunk_steps=chunk_steps,
                                 residual_warn=static_params.solver_residual_tol, stream=stream, pops=pops,
-                                metrics_out=out[s:e])
+                                metrics_out=out[s:e], n_time=T)
             if status_out is not None:
                 status_out[s:e] = res['status'].cpu().numpy()
         (stream if stream is not None else torch.cuda.current_stream(dev)).synchronize()

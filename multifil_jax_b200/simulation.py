@@ -86,6 +86,12 @@ class BatchPlan:
     def total(self) -> int:
         return self.params.shape[0]
 
+    @property
+    def const_drivers(self) -> bool:
+        """Whether z, pCa and ls each hold one value per condition for every
+        step (time stride 0), so that [B] values can replace the traces."""
+        return self.n_steps > 0 and all(a.ndim == 2 and a.strides[1] == 0 for a in (self.z, self.pCa, self.ls))
+
 
 def _split_keys(seed: int, n: int) -> np.ndarray:
     from .engine import prng_key, prng_split
@@ -140,7 +146,9 @@ def plan_batch(topology: SarcTopology, duration_ms: float = 1000.0, dt: float = 
             arr = np.asarray(value)
             if arr.ndim > 0 and arr.shape[0] != n_steps:
                 raise ValueError(f"{name} array length {arr.shape[0]} != n_steps {n_steps}")
-            wf_tables[name] = as_trace(value).astype(np.float32)[None, :]
+            # a scalar stays one value (a [1, 1] table): held for every step
+            wf_tables[name] = (np.full((1, 1), float(arr), np.float32) if arr.ndim == 0
+                               else as_trace(value).astype(np.float32)[None, :])
     if isinstance(K_lat, list):
         axes.append(('K_lat', list(K_lat)))
     if isinstance(nu, list):
@@ -195,9 +203,9 @@ def plan_batch(topology: SarcTopology, duration_ms: float = 1000.0, dt: float = 
         if name in wf_sweeps:
             return np.broadcast_to(tab[flat[name]], (total, n_steps))
         return np.broadcast_to(tab[0], (total, n_steps))
-    z_b = np.ascontiguousarray(wave('z_line'), dtype=np.float32)
-    p_b = np.ascontiguousarray(wave('pCa'), dtype=np.float32)
-    l_b = np.ascontiguousarray(wave('lattice_spacing'), dtype=np.float32)
+    # read-only broadcast views: a driver constant in time has time stride 0
+    # (BatchPlan.const_drivers), and nothing [B, T] is materialised for it
+    z_b, p_b, l_b = wave('z_line'), wave('pCa'), wave('lattice_spacing')
     if isinstance(K_lat, list):
         K_b = np.asarray(K_lat, np.float32)[flat['K_lat']]
     elif is_dyn:
@@ -356,9 +364,10 @@ def run_conditions(conditions: List[dict], *, static_params: Optional[StaticPara
         raise ValueError("every condition needs at least one timestep")
     T = max(steps)
     P = np.zeros((B, 44), np.float32)
-    Z = np.zeros((B, T), np.float32)
-    PC = np.zeros((B, T), np.float32)
-    L = np.zeros((B, T), np.float32)
+    # one driver value per condition, held for every step (MF_FLAG_CONST_DRIVERS)
+    Z = np.zeros(B, np.float32)
+    PC = np.zeros(B, np.float32)
+    L = np.zeros(B, np.float32)
     K = np.zeros(B, np.float32)
     NU = np.zeros(B, np.float32)
     DT = np.zeros(B, np.float32)
@@ -385,13 +394,13 @@ def run_conditions(conditions: List[dict], *, static_params: Optional[StaticPara
 
         def run_short():
             with torch.cuda.device(dev):
-                a = upload(dev, P, Z[:, :Ts], PC[:, :Ts], L[:, :Ts], np.minimum(np.asarray(steps, np.int32), Ts),
+                a = upload(dev, P, Z, PC, L, np.minimum(np.asarray(steps, np.int32), Ts),
                            KEYS.view(np.int32), K, NU, DT)
                 torch.cuda.synchronize(dev)
                 t0 = time.perf_counter()
                 eng.run_batch(topos, *a[:6], K_lat=a[6], nu=a[7], dt=a[8], n_newton=sp.n_newton_steps,
                               n_cg=sp.n_cg_steps, flags=flags, chunk_steps=chunk_steps,
-                              residual_warn=sp.solver_residual_tol)
+                              residual_warn=sp.solver_residual_tol, n_time=Ts)
                 torch.cuda.synchronize(dev)
                 return time.perf_counter() - t0
         choose_batch_sizes(topos, picks, run_short, precision=precision, device=device)
@@ -401,7 +410,7 @@ def run_conditions(conditions: List[dict], *, static_params: Optional[StaticPara
         hm = host_metrics(len(conditions), T)  # written by the kernels over the bus
         eng.run_batch(topos, dP, dZ, dPC, dL, dN, dKY, K_lat=dK, nu=dNU, dt=dDT,
                       n_newton=sp.n_newton_steps, n_cg=sp.n_cg_steps, flags=flags, chunk_steps=chunk_steps,
-                      residual_warn=sp.solver_residual_tol, metrics_out=hm)
+                      residual_warn=sp.solver_residual_tol, metrics_out=hm, n_time=T)
         torch.cuda.current_stream(dev).synchronize()
         m = hm.numpy()
     out = []

@@ -204,11 +204,15 @@ def test_choose_batch_sizes_keeps_the_faster_set(monkeypatch):
 
 def test_scalar_sweep_matches_constant_trace_sweep(topo):
     """plan_batch broadcasts a sweep of scalars; the driver arrays equal those
-    of the same sweep given as constant traces."""
+    of the same sweep given as constant traces.  Scalars stay one value per
+    condition (time stride 0, uploaded as [B] with MF_FLAG_CONST_DRIVERS);
+    traces are materialised."""
     pcas = [4.0, 5.25, 6.5]
     a = plan_batch(topo, duration_ms=7, pCa=pcas, z_line=[900.0, 950.0])
     b = plan_batch(topo, duration_ms=7, pCa=[np.full(7, v) for v in pcas],
                    z_line=[np.full(7, 900.0), np.full(7, 950.0)])
     for name in ('pCa', 'z', 'ls', 'params', 'keys'):
         assert np.array_equal(getattr(a, name), getattr(b, name)), name
-    assert a.pCa.flags['C_CONTIGUOUS'] and a.pCa.dtype == np.float32 and a.pCa.shape == (6, 7)
+    assert a.pCa.dtype == np.float32 and a.pCa.shape == (6, 7)
+    assert a.const_drivers and a.pCa.strides[1] == 0
+    assert not b.const_drivers and b.pCa.flags['C_CONTIGUOUS']
