@@ -300,3 +300,36 @@ def test_identical_conditions_identical_results():
             eng.tune_threads(topo, 0, 'mixed')
         for b in range(1, B):
             assert np.array_equal(m[b], m[0]), (nt, b)
+
+
+@pytest.mark.parametrize('flags', [0, MF_FLAG_PRECISE, MF_FLAG_PLAIN, MF_FLAG_PRECISE | MF_FLAG_DYNAMIC_LS])
+def test_constant_drivers_equal_traces(engine, flags):
+    """[B] drivers held for every step (MF_FLAG_CONST_DRIVERS, what run() sends
+    for scalar sweeps) give exactly the results of the same values as [B, T]
+    traces, in one launch, in CUDA-graph chunks and on the plain path."""
+    import torch
+    from tests.gpu_helpers import tt, keys_tensor
+    s, d = get_skeletal_params()
+    topo = SarcTopology.create(2, 2, s, d)
+    B, T = 5, 18
+    zc, pc, lc = np.linspace(880.0, 960.0, B), np.linspace(4.2, 6.8, B), np.full(B, 14.0)
+    P = np.tile(d.param_row(), (B, 1))
+    keys = prng.split(prng.PRNGKey(9), B)
+    dyn = bool(flags & MF_FLAG_DYNAMIC_LS)
+    kl = np.full(B, 5.0 * topo.n_thick) if dyn else np.zeros(B)
+    nu = np.full(B, 0.5) if dyn else np.zeros(B)
+    common = dict(K_lat=tt(kl, torch.float32), nu=tt(nu, torch.float32), dt=tt(np.ones(B), torch.float32),
+                  flags=flags)
+    for chunk in (0, 7):
+        if chunk and flags & MF_FLAG_PLAIN:
+            continue
+        ref = engine.run_batch(topo, tt(P, torch.float32), tt(np.repeat(zc[:, None], T, 1), torch.float32),
+                               tt(np.repeat(pc[:, None], T, 1), torch.float32),
+                               tt(np.repeat(lc[:, None], T, 1), torch.float32), tt(np.full(B, T, np.int32)),
+                               keys_tensor(keys), chunk_steps=chunk, **common)
+        got = engine.run_batch(topo, tt(P, torch.float32), tt(zc, torch.float32), tt(pc, torch.float32),
+                               tt(lc, torch.float32), tt(np.full(B, T, np.int32)), keys_tensor(keys),
+                               chunk_steps=chunk, n_time=T, **common)
+        torch.cuda.synchronize()
+        assert np.array_equal(got['metrics'].cpu().numpy(), ref['metrics'].cpu().numpy()), chunk
+        assert np.array_equal(got['status'].cpu().numpy(), ref['status'].cpu().numpy())
