@@ -224,13 +224,17 @@ def plan_batch(topology: SarcTopology, duration_ms: float = 1000.0, dt: float = 
         d0 = l_b[:, 0:1]
         l_b = (d0 * (z_b[:, 0:1] / z_b) ** nu_b[:, None]).astype(np.float32)
 
-    def param(name):
+    # one constant row, then the swept columns
+    row = np.empty(N_PARAMS, np.float32)
+    for j, name in enumerate(DYNAMIC_FIELDS):
+        if isinstance(dynamic_params, dict) and name in dynamic_params and name not in paxis:
+            row[j] = float(dynamic_params[name])
+        else:
+            row[j] = float(np.asarray(getattr(base, name)).reshape(-1)[0])
+    params = np.tile(row, (total, 1))
+    for j, name in enumerate(DYNAMIC_FIELDS):
         if name in paxis:
-            return ptables[name][flat[paxis[name]]]
-        if isinstance(dynamic_params, dict) and name in dynamic_params:
-            return np.full(total, float(dynamic_params[name]), np.float32)
-        return np.full(total, float(np.asarray(getattr(base, name)).reshape(-1)[0]), np.float32)
-    params = np.stack([param(n) for n in DYNAMIC_FIELDS], axis=1).astype(np.float32)
+            params[:, j] = ptables[name][flat[paxis[name]]]
     assert params.shape == (total, N_PARAMS)
     from .subpopulation import resolve_subpopulation
     subpop = resolve_subpopulation(subpopulation, topology, params,
