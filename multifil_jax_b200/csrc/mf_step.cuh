@@ -1822,18 +1822,20 @@ struct Sim : SimDyn<DY> {
     double* __restrict__ fp = s.face_pos;
     const int16_t* __restrict__ cands = T.face_sites;
     const uint8_t* __restrict__ fn = T.face_n;
-    for (int q = tid; q < nfaces * W; q += NT) {
-      const int face = q / W, k = q - face * W;
-      double pos = NAN;
-      if (k < fn[face]) {
-        const int g = (face / 3) * nsi + cands[q];
-        pos = precise ? site_pos_d(g) : (double)s.x[ntn + g];
-      }
-      fp[q] = pos > 0.0 ? pos : NAN;
-    }
-    __syncthreads();
+    // one warp per face: its lanes stage the candidate positions and, on a
+    // face of at most 32 candidates, classify the run from their own values
     for (int face = warp; face < nfaces; face += NW) {
-      const double pk = (W <= 32 && lane < W) ? fp[face * W + lane] : NAN;
+      double pk = NAN;
+      for (int k = lane; k < W; k += 32) {
+        double pos = NAN;
+        if (k < fn[face]) {
+          const int g = (face / 3) * nsi + cands[face * W + k];
+          pos = precise ? site_pos_d(g) : (double)s.x[ntn + g];
+        }
+        pos = pos > 0.0 ? pos : NAN;
+        fp[face * W + k] = pos;
+        if (W <= 32) pk = pos;
+      }
       const bool v = pk == pk;
       const unsigned vm = __ballot_sync(0xffffffffu, v);
       const double pn = __shfl_down_sync(0xffffffffu, pk, 1);
@@ -1942,7 +1944,14 @@ struct Sim : SimDyn<DY> {
     }
     after_loop();
     __syncthreads();
-    for (int g = tid; g < S; g += NT) s.tm[g] = s.tm_new[g];
+    // the new states, and thick_step's empty bids per site (win1 / win2, in
+    // the site region, which nothing reads between here and thick_step)
+    int* win1 = reinterpret_cast<int*>(s.site);
+    for (int g = tid; g < S; g += NT) {
+      s.tm[g] = s.tm_new[g];
+      win1[g] = -1;
+      s.win2[g] = -1;
+    }
     __syncthreads();
   }
 
@@ -1981,9 +1990,7 @@ struct Sim : SimDyn<DY> {
   __device__ void thick_step(const uint32_t* sub, size_t inj_off) {
     const int X = T.total_xbs, S = T.n_sites_total;
     const float* cum_xb = reinterpret_cast<const float*>(ws + L.cum_xb);
-    int* win1 = reinterpret_cast<int*>(s.site);
-    for (int g = tid; g < S; g += NT) { win1[g] = -1; s.win2[g] = -1; }
-    __syncthreads();
+    int* win1 = reinterpret_cast<int*>(s.site);  // emptied by thin_step
     // sample, decide binding, and bid for the two scatter targets
     const int nsi = T.n_sites, nbins = T.n_bins;
     for (int i = tid; i < X; i += NT) {
