@@ -693,9 +693,11 @@ __device__ void run_condition(const StepArgs& A, int ci) {
       if (first || !m.precise) __syncthreads();
       MF_PH(3);
     }
-    // 2-4. kinetics
+    // 2-4. kinetics.  No barrier after the nearest-site search: the
+    // tropomyosin sampling reads none of its outputs, the initial key loop
+    // reads only its own heads' offsets, and thin_step's first barrier
+    // precedes the bid arrays it writes over the staged face positions.
     m.nearest(d_kin);
-    __syncthreads();
     MF_PH(4);
     if (init) {
       // table rows of the initial geometry (every site starts in state 0: block 0)

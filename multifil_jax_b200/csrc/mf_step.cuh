@@ -866,7 +866,8 @@ struct Sim : SimDyn<DY> {
     const int X = T.total_xbs, S = T.n_sites_total, nsi = T.n_sites;
     int* __restrict__ cnt = s.win2;
     int16_t* __restrict__ site_h = s.site_h;
-    __syncthreads();
+    // every caller ends its previous phase with a barrier (thick_step's
+    // last scatter, the nearest-site search of the initial equilibrium)
     for (int g = tid; g < S; g += NT) cnt[g] = 0;
     __syncthreads();
     // each thread takes a run of consecutive heads, so one block-wide scan of
