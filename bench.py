@@ -32,7 +32,7 @@ sys.path.insert(0, REPO)
 B_SWEEP, T_SWEEP = 256, 500
 # DRAM bytes (read + write) of one launch of the mixed-precision sweep, from
 # ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum on this workload
-TRAFFIC_PER_LAUNCH = 2.70e6 + 45.25e6
+TRAFFIC_PER_LAUNCH = 2.69e6 + 45.97e6
 METRIC = 'condition-timesteps/s'
 
 
