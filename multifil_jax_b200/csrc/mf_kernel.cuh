@@ -519,7 +519,7 @@ __device__ void run_condition(const StepArgs& A, int ci) {
   // (pCa, d) of the sampling and absorbing tables in the workspace and the
   // initial z: read from shared memory every step, persisted at launch end
   __shared__ double tab_key[5];
-  __shared__ int samp_est;  // key count of the last sampling build (dynamic spacing)
+  __shared__ int samp_est;  // key count of the last sampling build (dynamic spacing; 0: none yet)
   if (t0 == 0) {
     // ---- realize_state + initial equilibrium with the constants (A1) ----
     m.zref = (double)zt[0];
@@ -583,7 +583,7 @@ __device__ void run_condition(const StepArgs& A, int ci) {
   __shared__ int keys_ready;
   if (m.tid == 0) {
     keys_ready = 0;
-    samp_est = A.pop.kx() * 2 * T.n_bins;
+    samp_est = 0;  // no merged build before a sampling build has counted the keys
   }
   // Drivers (z, pCa, ls) of step t in drv[t & 1].  Thread 0 copies those of
   // step t + 1 with cp.async during step t: their latency overlaps a whole
