@@ -308,7 +308,8 @@ class Engine:
         torch = _torch()
         dev = torch.device('cuda', self.device)
         if z.dim() == 1:
-            assert pCa.dim() == 1 and ls.dim() == 1 and n_time is not None
+            if pCa.dim() != 1 or ls.dim() != 1 or n_time is None:
+                raise EngineError("drivers held for every step: z, pCa and ls must all be [B] and n_time given")
             B, T = z.shape[0], int(n_time)
             flags = int(flags) | MF_FLAG_CONST_DRIVERS
         else:
