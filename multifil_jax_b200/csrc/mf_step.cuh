@@ -1743,7 +1743,7 @@ struct Sim : SimDyn<DY> {
   // samp_est, the key count of the last sampling build; while the builds
   // merge, no sampling build runs and the estimate keeps the count that
   // started them).  Measured on 2x2 to 4x4 solved-spacing sweeps this beats
-  // both separate builds of the read rows only (5-10 %) and a rule that
+  // both separate builds of the read rows only (7-12 %) and a rule that
   // merges only when nearly every row is read.  Returns the key count of a
   // sampling build, or for an absorbing build 1 if every sampling row was
   // built with it, else 0.
