@@ -223,14 +223,9 @@ static __device__ __forceinline__ void blend_acc(float (&acc)[R][C], const float
     for (int j = 0; j < C; ++j) acc[i][j] = __fadd_rn(acc[i][j], __fmul_rn(f, q[i][j]));
 }
 
-// Bin-major order of the crossbridge table keys: ord = (bin * kx + population)
-// * 2 + permissiveness, and its inverse (key = population * 2 n_bins +
-// permissiveness * n_bins + bin).
-__device__ __forceinline__ int table_order_of_key(int key, int kx, int nb) {
-  const int nset = 2 * nb, pk = key / nset, k2 = key - pk * nset;
-  const int perm = k2 >= nb ? 1 : 0, bin = k2 - perm * nb;
-  return (bin * kx + pk) * 2 + perm;
-}
+// The crossbridge table key (population * 2 n_bins + permissiveness * n_bins
+// + bin) at position ord of the bin-major order ord = (bin * kx + population)
+// * 2 + permissiveness.
 __device__ __forceinline__ int table_key_of_order(int ord, int kx, int nb) {
   const int perm = ord & 1, q = ord >> 1, pk = q % kx, bin = q / kx;
   return pk * 2 * nb + perm * nb + bin;
@@ -1731,9 +1726,10 @@ struct Sim : SimDyn<DY> {
   // rows some head reads are built: the sampling keys of all heads (after
   // the tropomyosin update, thick_step's keys) or the absorbing keys of the
   // heads the metrics read (old state 2 or 3).  Flags and the key list
-  // live in the CG vector pv, which is free outside the solve; the flags are
-  // indexed in bin-major order and the list runs from the highest bin down
-  // (the stiff far bins first, the cheap central ones in the last round).
+  // live in the CG vector pv, which is free outside the solve; the list is
+  // in key order (neighbouring bins of one permissiveness share a warp, and
+  // with them similar squaring counts: measured 0.5-1 % faster than a
+  // bin-major list from the highest bin down).
   //
   // The absorbing rows of step t and the sampling rows of step t + 1 have
   // the same spacing (the one step t solved for) and, with pCa unchanged,
@@ -1768,17 +1764,14 @@ struct Sim : SimDyn<DY> {
         const int so = s.old_xbs[i];
         if (so == 2 || so == 3) key = s.old_key[i];
       }
-      if (key >= 0) {
-        const int o = table_order_of_key(key, kx, nb);
-        atomicOr(&bits[o >> 5], 1u << (o & 31));
-      }
+      if (key >= 0) atomicOr(&bits[key >> 5], 1u << (key & 31));
     }
     __syncthreads();
     if (warp == 0) {
       int base = 0;
       for (int c = 0; c < nwords; c += 32) {
-        const int wi = nwords - 1 - (c + lane);  // lane 0 takes the highest word
-        uint32_t wb = wi >= 0 ? bits[wi] : 0u;
+        const int wi = c + lane;
+        uint32_t wb = wi < nwords ? bits[wi] : 0u;
         const int n = __popc(wb);
         int incl = n;
 #pragma unroll
@@ -1788,9 +1781,8 @@ struct Sim : SimDyn<DY> {
         }
         int off = base + incl - n;
         while (wb) {
-          const int bit = 31 - __clz(wb);
-          list[off++] = (int16_t)table_key_of_order(wi * 32 + bit, kx, nb);
-          wb &= ~(1u << bit);
+          list[off++] = (int16_t)(wi * 32 + __ffs(wb) - 1);
+          wb &= wb - 1u;
         }
         base += __shfl_sync(0xffffffffu, incl, 31);
       }
