@@ -216,3 +216,27 @@ def test_scalar_sweep_matches_constant_trace_sweep(topo):
     assert a.pCa.dtype == np.float32 and a.pCa.shape == (6, 7)
     assert a.const_drivers and a.pCa.strides[1] == 0
     assert not b.const_drivers and b.pCa.flags['C_CONTIGUOUS']
+
+
+def test_const_drivers_only_when_every_driver_is_held(topo):
+    """BatchPlan.const_drivers (the [B] upload with MF_FLAG_CONST_DRIVERS) holds
+    exactly when z, pCa and the spacing are each one value per condition."""
+    T = 6
+    ramp = np.linspace(900.0, 905.0, T)
+    cases = [
+        (dict(pCa=4.5, z_line=900.0), True),
+        (dict(pCa=[4.5, 5.5], z_line=[900.0, 950.0], lattice_spacing=[13.5, 14.0]), True),
+        (dict(pCa=4.5, z_line=ramp), False),                      # a z trace
+        (dict(pCa=[np.full(T, 4.5), np.full(T, 5.0)]), False),    # a sweep of traces
+        (dict(pCa=4.5, z_line=ramp, nu=0.5), False),              # Poisson spacing from the z trace
+        (dict(pCa=4.5, z_line=900.0, K_lat=5.0, nu=0.5), True),   # spacing solved: drivers still held
+    ]
+    for kw, expect in cases:
+        p = plan_batch(topo, duration_ms=T, **kw)
+        assert p.const_drivers is expect, kw
+        for a in (p.z, p.pCa, p.ls):
+            assert a.shape == (p.total, T) and a.dtype == np.float32
+        if expect:
+            for a in (p.z, p.pCa, p.ls):
+                assert np.array_equal(a, np.repeat(a[:, :1], T, axis=1))
+    assert not plan_batch(topo, duration_ms=0.5, pCa=4.5).const_drivers  # no steps
